@@ -1,0 +1,298 @@
+/*
+ * ag_capi.c -- the reference's algorithm entry points for the CSR data
+ * structure, backed by the B200 kernels.
+ *
+ * Mirrors 02_capi_graph/src/algorithms/capi/pageRank.c (newPageRankStatsGraphCSR
+ * :50-78, freePageRankStats :170-180, pageRankGraphCSR :874-939,
+ * pageRankPullGraphCSR :942-1109) and SPMV.c (newSPMVStatsGraphCSR :51-73,
+ * freeSPMVStats :145-158, SPMVGraphCSR :594-621, SPMVPullGraphCSR :622-751):
+ * same stats objects, same iteration and convergence semantics, same stdout
+ * tables.  The per-iteration table is printed after the device-resident loop
+ * finishes, from the per-pass record the device keeps.  The legacy symbols
+ * print one diagnostic line and exit on a device failure, as the reference's
+ * accelerator calls do (capienv.c:113-131); the *_ex forms return the status.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ag_internal.h"
+
+static int env_quiet(void)
+{
+    const char *q = getenv("AG_QUIET");
+    return q && q[0] && q[0] != '0';
+}
+
+static void fail_exit(const char *phase, ag_status_t st)
+{
+    fprintf(stderr, "Accelerator verification failed: phase=%s reason=%s detail=%s\n", phase, ag_status_string(st),
+            ag_last_error());
+    exit(EXIT_FAILURE);
+}
+
+/* ------------------------------------------------------------ PageRank */
+struct PageRankStats *newPageRankStatsGraphCSR(struct GraphCSR *graph)
+{
+    uint32_t v, n = graph ? graph->num_vertices : 0;
+    struct PageRankStats *stats = (struct PageRankStats *)calloc(1, sizeof(struct PageRankStats));
+    if (!stats)
+        return NULL;
+    stats->damp = Damp;
+    stats->base_pr = (1.0f - stats->damp);
+    stats->iterations = 0;
+    stats->num_vertices = n;
+    stats->time_total = 0.0;
+    stats->error_total = 0.0;
+    stats->realRanks = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+    stats->pageRanks = (float *)malloc((n ? n : 1) * sizeof(float));
+    if (!stats->realRanks || !stats->pageRanks) {
+        free(stats->realRanks);
+        free(stats->pageRanks);
+        free(stats);
+        return NULL;
+    }
+    for (v = 0; v < n; v++) {
+        stats->pageRanks[v] = stats->base_pr;
+        stats->realRanks[v] = v;
+    }
+    return stats;
+}
+
+void freePageRankStats(struct PageRankStats *stats)
+{
+    if (stats) {
+        free(stats->realRanks);
+        free(stats->pageRanks);
+        free(stats);
+    }
+}
+
+ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph,
+                                const ag_pr_opts *opts, struct PageRankStats **out)
+{
+    ag_pr_opts o;
+    ag_pr_result res;
+    ag_graph_t g = NULL;
+    ag_status_t st;
+    struct PageRankStats *stats;
+    uint32_t *h_active = NULL;
+    double *h_err = NULL, *h_sec = NULL;
+    uint32_t cap, i;
+    int quiet;
+    double t0 = ag_wall_seconds();
+
+    ag_clear_error();
+    if (!arguments || !graph || !out)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_pull_ex: NULL argument");
+    *out = NULL;
+    ag_pr_opts_init(&o);
+    if (opts)
+        memcpy(&o, opts, opts->struct_size && opts->struct_size < sizeof(o) ? opts->struct_size : sizeof(o));
+    quiet = o.quiet || env_quiet();
+
+    stats = newPageRankStatsGraphCSR((struct GraphCSR *)graph);
+    if (!stats)
+        return ag_set_error(AG_ERR_OOM, "stats allocation failed");
+
+    if (!quiet) {
+        printf(" -----------------------------------------------------\n");
+        printf("| %-51s | \n", "               ---->>> B200 <<<----");
+        printf(" -----------------------------------------------------\n");
+        printf("| %-51s | \n", "Starting Page Rank Pull (tolerance/epsilon)");
+        printf(" -----------------------------------------------------\n");
+        printf("| %-51.13lf | \n", arguments->epsilon);
+        printf(" -----------------------------------------------------\n");
+        printf("| %-10s | %-8s | %-15s | %-9s | \n", "Iteration", "Active", "Error", "Time (S)");
+        printf(" -----------------------------------------------------\n");
+    }
+
+    st = ag_graph_upload(graph, 0, &g);
+    if (st != AG_OK)
+        goto fail;
+    st = ag_pagerank_launch(g, arguments->iterations, arguments->epsilon, &o);
+    if (st != AG_OK)
+        goto fail;
+    cap = arguments->iterations ? arguments->iterations : 1;
+    h_active = (uint32_t *)calloc(cap, sizeof(uint32_t));
+    h_err = (double *)calloc(cap, sizeof(double));
+    h_sec = (double *)calloc(cap, sizeof(double));
+    if (!h_active || !h_err || !h_sec) {
+        st = ag_set_error(AG_ERR_OOM, "history allocation failed");
+        goto fail;
+    }
+    st = ag_pagerank_fetch(g, stats->pageRanks, &res, h_active, h_err, h_sec, cap);
+    if (st != AG_OK)
+        goto fail;
+    ag_graph_release(g);
+    g = NULL;
+
+    stats->iterations = res.iterations;
+    stats->error_total = res.error_total;
+    stats->activeVertices = res.active_last;
+    stats->time_total = ag_wall_seconds() - t0;
+
+    if (!quiet) {
+        for (i = 0; i < res.passes && i < cap; i++)
+            printf("| %-10u | %-8u | %-15.13lf | %-9f | \n", i, h_active[i], h_err[i], h_sec[i]);
+        printf(" -----------------------------------------------------\n");
+        printf("| %-10s | %-8s | %-15s | %-9s | \n", "Iterations", "PR Sum", "Error", "Time (S)");
+        printf(" -----------------------------------------------------\n");
+        printf("| %-10u | %-8lf | %-15.13lf | %-9f | \n", stats->iterations, res.rank_sum, stats->error_total,
+               stats->time_total);
+        printf(" -----------------------------------------------------\n");
+        fflush(stdout);
+    }
+    free(h_active);
+    free(h_err);
+    free(h_sec);
+    *out = stats;
+    return AG_OK;
+
+fail:
+    if (g)
+        ag_graph_release(g);
+    free(h_active);
+    free(h_err);
+    free(h_sec);
+    freePageRankStats(stats);
+    return st;
+}
+
+struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    struct PageRankStats *stats = NULL;
+    ag_status_t st = ag_pagerank_pull_ex(arguments, graph, NULL, &stats);
+    if (st != AG_OK)
+        fail_exit("pagerank-pull", st);
+    return stats;
+}
+
+struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    if (arguments && arguments->pushpull != 0)
+        fprintf(stderr, "pageRankGraphCSR: pushpull=%u runs the FP32 pull on the GPU\n", arguments->pushpull);
+    return pageRankPullGraphCSR(arguments, graph);
+}
+
+/* ---------------------------------------------------------------- SpMV */
+struct SPMVStats *newSPMVStatsGraphCSR(struct GraphCSR *graph)
+{
+    uint32_t n = graph ? graph->num_vertices : 0;
+    struct SPMVStats *stats = (struct SPMVStats *)calloc(1, sizeof(struct SPMVStats));
+    if (!stats)
+        return NULL;
+    stats->iterations = 0;
+    stats->num_vertices = n;
+    stats->time_total = 0.0;
+    stats->vector_output = (float *)calloc(n ? n : 1, sizeof(float));
+    stats->vector_input = (float *)calloc(n ? n : 1, sizeof(float));
+    if (!stats->vector_output || !stats->vector_input) {
+        free(stats->vector_output);
+        free(stats->vector_input);
+        free(stats);
+        return NULL;
+    }
+    return stats;
+}
+
+void freeSPMVStats(struct SPMVStats *stats)
+{
+    if (stats) {
+        free(stats->vector_output);
+        free(stats->vector_input);
+        free(stats);
+    }
+}
+
+ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph, int quiet,
+                            struct SPMVStats **out)
+{
+    ag_graph_t g = NULL;
+    ag_status_t st;
+    struct SPMVStats *stats;
+    double *sec = NULL;
+    double sum = 0.0;
+    uint32_t v, i, iters;
+    double t0;
+
+    ag_clear_error();
+    if (!arguments || !graph || !out)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_ex: NULL argument");
+    *out = NULL;
+    quiet = quiet || env_quiet();
+    stats = newSPMVStatsGraphCSR((struct GraphCSR *)graph);
+    if (!stats)
+        return ag_set_error(AG_ERR_OOM, "stats allocation failed");
+    iters = arguments->iterations;
+
+    st = ag_graph_upload(graph, AG_UPLOAD_WEIGHTS, &g);
+    if (st != AG_OK)
+        goto fail;
+    if (!quiet) {
+        printf(" -----------------------------------------------------\n");
+        printf("| %-51s | \n", "Starting SPMV-PULL");
+        printf(" -----------------------------------------------------\n");
+        printf("| %-21s | %-27s | \n", "Iteration", "Time (S)");
+        printf(" -----------------------------------------------------\n");
+    }
+    /* input vector of the reference benchmark (SPMV.c:694-701) */
+    for (v = 0; v < graph->num_vertices; v++) {
+        if (graph->vertices->out_degree[v])
+            stats->vector_input[v] = (1.0f / graph->vertices->out_degree[v]);
+        else
+            stats->vector_input[v] = 0.001f;
+    }
+    t0 = ag_wall_seconds();
+    sec = (double *)calloc(iters ? iters : 1, sizeof(double));
+    if (!sec) {
+        st = ag_set_error(AG_ERR_OOM, "allocation failed");
+        goto fail;
+    }
+    st = ag_spmv_run_host(g, stats->vector_input, stats->vector_output, iters, AG_SPMV_GRAPH_WEIGHTS, sec);
+    if (st != AG_OK)
+        goto fail;
+    stats->iterations = iters;
+    if (!quiet)
+        for (i = 0; i < iters; i++)
+            printf("| %-21u | %-27f | \n", i, sec[i]);
+    for (v = 0; v < graph->num_vertices; v++)
+        sum += ((int)(stats->vector_output[v] * 100 + .5) / 100.0);
+    stats->time_total = ag_wall_seconds() - t0;
+    if (!quiet) {
+        printf(" -----------------------------------------------------\n");
+        printf("| %-15s | %-15s | %-15s | \n", "Iterations", "Sum", "Time (S)");
+        printf(" -----------------------------------------------------\n");
+        printf("| %-15u | %-15lf | %-15f | \n", stats->iterations, sum, stats->time_total);
+        printf(" -----------------------------------------------------\n");
+        fflush(stdout);
+    }
+    ag_graph_release(g);
+    free(sec);
+    *out = stats;
+    return AG_OK;
+
+fail:
+    if (g)
+        ag_graph_release(g);
+    free(sec);
+    freeSPMVStats(stats);
+    return st;
+}
+
+struct SPMVStats *SPMVPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    struct SPMVStats *stats = NULL;
+    ag_status_t st = ag_spmv_pull_ex(arguments, graph, 0, &stats);
+    if (st != AG_OK)
+        fail_exit("spmv-pull", st);
+    return stats;
+}
+
+struct SPMVStats *SPMVGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    if (arguments && arguments->pushpull != 0)
+        fprintf(stderr, "SPMVGraphCSR: pushpull=%u runs the FP32 pull on the GPU\n", arguments->pushpull);
+    return SPMVPullGraphCSR(arguments, graph);
+}

@@ -1,0 +1,838 @@
+/*
+ * ag_runtime.cu -- device context, graph upload and work planning, the
+ * CUDA-graph iteration loop and the status-returning entry points.
+ *
+ * Replaces the reference's accelerator runtime for this path
+ * (02_capi_graph/src/capi_utils/capienv.c: mapGraphCSRToWED :832-874,
+ * setupAFUGraphCSR :329-372, startAFU/startCU/waitAFU :375-638,
+ * releaseAFU :765-782).  Where the reference crosses the host/accelerator
+ * boundary twice per iteration (startCU + waitAFU, pageRank.c:1041-1046),
+ * a solve here is one cudaGraphLaunch: init kernel -> WHILE(condition){pull
+ * pass} -> normalise, with the condition set on the device by the pass that
+ * converged or reached the iteration cap.  Host waits are bounded
+ * (AG_WAIT_TIMEOUT_S), after the pattern of the reference's watchdog
+ * (accelerator_verification.c:177-320), and return AG_ERR_TIMEOUT instead of
+ * exiting.
+ */
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "ag_device.h"
+#include "ag_internal.h"
+
+/* ------------------------------------------------------------ context */
+struct AgContext
+{
+    int ready;
+    int device;
+    int num_sms;
+    cudaStream_t stream;
+};
+
+static AgContext g_ctx = {0, -1, 0, nullptr};
+
+#define AG_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return ag_set_error(AG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                __FILE__, __LINE__);                                           \
+    } while (0)
+
+static ag_status_t ctx_ensure(int want_device)
+{
+    if (g_ctx.ready && (want_device < 0 || want_device == g_ctx.device))
+        return AG_OK;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return ag_set_error(AG_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    int dev = want_device;
+    if (dev < 0)
+        AG_CUDA(cudaGetDevice(&dev));
+    if (dev >= n)
+        return ag_set_error(AG_ERR_INVALID_ARG, "device %d out of range (%d devices)", dev, n);
+    AG_CUDA(cudaSetDevice(dev));
+    if (g_ctx.ready && g_ctx.stream) {
+        cudaStreamDestroy(g_ctx.stream);
+        g_ctx.stream = nullptr;
+    }
+    AG_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    AG_CUDA(cudaDeviceGetAttribute(&g_ctx.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    /* keep freed stream-ordered allocations in this process's pool so that
+     * repeated uploads reuse them */
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    g_ctx.device = dev;
+    g_ctx.ready = 1;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_init(int device)
+{
+    ag_clear_error();
+    return ctx_ensure(device);
+}
+
+extern "C" void *ag_stream(void)
+{
+    if (ctx_ensure(-1) != AG_OK)
+        return nullptr;
+    return (void *)g_ctx.stream;
+}
+
+extern "C" int ag_num_sms(void)
+{
+    if (ctx_ensure(-1) != AG_OK)
+        return 0;
+    return g_ctx.num_sms;
+}
+
+extern "C" const char *ag_version(void) { return "accelgraph-b200 0.1 sm_100a"; }
+
+static double wait_limit_s(double timeout_s)
+{
+    if (timeout_s > 0)
+        return timeout_s;
+    const char *env = getenv("AG_WAIT_TIMEOUT_S");
+    if (env) {
+        double v = atof(env);
+        if (v > 0)
+            return v;
+    }
+    return 600.0;
+}
+
+/* bounded wait: poll the stream until it drains or the deadline passes */
+static ag_status_t stream_wait(cudaStream_t s, double timeout_s)
+{
+    const double limit = wait_limit_s(timeout_s);
+    const double t0 = ag_wall_seconds();
+    unsigned spins = 0;
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess)
+            return AG_OK;
+        if (e != cudaErrorNotReady)
+            return ag_set_error(AG_ERR_CUDA, "stream failed: %s", cudaGetErrorString(e));
+        if (ag_wall_seconds() - t0 > limit)
+            return ag_set_error(AG_ERR_TIMEOUT, "device work did not finish within %.1f s", limit);
+        if (++spins > 64) {
+            struct timespec ts = {0, 20000};
+            nanosleep(&ts, nullptr);
+        }
+    }
+}
+
+extern "C" ag_status_t ag_synchronize(double timeout_s)
+{
+    ag_status_t st = ctx_ensure(-1);
+    if (st != AG_OK)
+        return st;
+    return stream_wait(g_ctx.stream, timeout_s);
+}
+
+extern "C" void *ag_rt_host_alloc(size_t bytes, int pinned, int *got_pinned)
+{
+    *got_pinned = 0;
+    if (pinned && ctx_ensure(-1) == AG_OK) {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) == cudaSuccess) {
+            *got_pinned = 1;
+            return p;
+        }
+        cudaGetLastError();
+    }
+    return malloc(bytes);
+}
+
+extern "C" void ag_rt_host_free(void *ptr, int pinned)
+{
+    if (!ptr)
+        return;
+    if (pinned)
+        cudaFreeHost(ptr);
+    else
+        free(ptr);
+}
+
+/* ------------------------------------------------------- graph handle */
+struct AgExec
+{
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    cudaGraphNode_t init_node;
+    cudaGraphConditionalHandle cond;
+    AgPullParams params;
+    unsigned grid;
+};
+
+struct ag_graph_s
+{
+    uint32_t N, E, E4;
+    uint32_t *row_off, *ids, *outdeg;
+    float *w;
+    uint4 *tasks_fast, *tasks_exact;
+    uint32_t ntasks_fast, ntasks_exact;
+    uint32_t nparts;
+    uint32_t num_hub_rows, max_in_degree;
+    float *rank;
+    float *c32[2];
+    uint16_t *c16[2];
+    float *hub_part;
+    uint32_t *hub_cnt;
+    AgControl *ctl;
+    float *init_buf;
+    uint32_t *flag;
+    AgExec exe[3][2];
+    int have_exe[3][2];
+    cudaEvent_t ev0, ev1;
+    int launched;
+    int last_prec, last_exact;
+    uint64_t device_bytes;
+};
+
+static void *dev_alloc(ag_graph_s *g, size_t bytes, ag_status_t *st)
+{
+    void *p = nullptr;
+    if (*st != AG_OK)
+        return nullptr;
+    if (bytes == 0)
+        bytes = 16;
+    cudaError_t e = cudaMallocAsync(&p, bytes, g_ctx.stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *st = ag_set_error(AG_ERR_OOM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        return nullptr;
+    }
+    g->device_bytes += bytes;
+    return p;
+}
+
+static void dev_free(void *p)
+{
+    if (p)
+        cudaFreeAsync(p, g_ctx.stream);
+}
+
+static void free_exec(AgExec *x)
+{
+    if (x->exec)
+        cudaGraphExecDestroy(x->exec);
+    if (x->graph)
+        cudaGraphDestroy(x->graph);
+    x->exec = nullptr;
+    x->graph = nullptr;
+}
+
+extern "C" ag_status_t ag_graph_release(ag_graph_t g)
+{
+    if (!g)
+        return AG_OK;
+    if (g_ctx.ready)
+        stream_wait(g_ctx.stream, 0);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            if (g->have_exe[a][b])
+                free_exec(&g->exe[a][b]);
+    dev_free(g->row_off);
+    dev_free(g->ids);
+    dev_free(g->outdeg);
+    dev_free(g->w);
+    dev_free(g->tasks_fast);
+    dev_free(g->tasks_exact);
+    dev_free(g->rank);
+    dev_free(g->c32[0]);
+    dev_free(g->c32[1]);
+    dev_free(g->c16[0]);
+    dev_free(g->c16[1]);
+    dev_free(g->hub_part);
+    dev_free(g->hub_cnt);
+    dev_free(g->ctl);
+    dev_free(g->init_buf);
+    dev_free(g->flag);
+    if (g->ev0)
+        cudaEventDestroy(g->ev0);
+    if (g->ev1)
+        cudaEventDestroy(g->ev1);
+    if (g_ctx.ready)
+        cudaStreamSynchronize(g_ctx.stream);
+    delete g;
+    return AG_OK;
+}
+
+/* Work list of the fused pull kernel.  FAST order: rows longer than AG_CAP
+ * run on their own CTA, rows longer than AG_HUB are split into AG_HUB-edge
+ * chunks; EXACT order keeps every long row on one CTA.  Everything else is
+ * packed into row blocks of <= AG_CAP in-edges and <= AG_RMAX rows.  Heavy
+ * items come first so that they start early. */
+static void plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out, uint32_t *nparts,
+                       uint32_t *nhub)
+{
+    std::vector<uint4> hubs, rows, blocks;
+    uint32_t pbase = 0, nh = 0;
+    uint32_t r = 0;
+    while (r < N) {
+        const uint32_t d = off[r + 1] - off[r];
+        if (d > AG_CAP) {
+            if (!exact && d > AG_HUB) {
+                const uint32_t nch = (d + AG_HUB - 1) / AG_HUB;
+                for (uint32_t c = 0; c < nch; ++c)
+                    hubs.push_back(make_uint4(AG_T_HUB | (c << 2), r, pbase, nch));
+                pbase += nch;
+                ++nh;
+            } else {
+                rows.push_back(make_uint4(AG_T_ROW, r, 0, 0));
+            }
+            ++r;
+            continue;
+        }
+        const uint32_t rb = r, eb = off[r];
+        while (r < N && r - rb < AG_RMAX) {
+            const uint32_t dr = off[r + 1] - off[r];
+            if (dr > AG_CAP || off[r + 1] - eb > AG_CAP)
+                break;
+            ++r;
+        }
+        blocks.push_back(make_uint4(AG_T_BLOCK, rb, r, 0));
+    }
+    out.clear();
+    out.reserve(hubs.size() + rows.size() + blocks.size());
+    out.insert(out.end(), hubs.begin(), hubs.end());
+    out.insert(out.end(), rows.begin(), rows.end());
+    out.insert(out.end(), blocks.begin(), blocks.end());
+    *nparts = pbase;
+    *nhub = nh;
+}
+
+extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out)
+{
+    ag_clear_error();
+    if (!graph || !out)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_upload: NULL argument");
+    *out = nullptr;
+    ag_status_t st = ctx_ensure(-1);
+    if (st != AG_OK)
+        return st;
+    const uint32_t N = graph->num_vertices, E = graph->num_edges;
+    const struct Vertex *iv = graph->inverse_vertices;
+    const struct Vertex *fv = graph->vertices;
+    const struct EdgeList *iel = graph->inverse_sorted_edges_array;
+    if (N > 0 && (!iv || !iv->out_degree || !iv->edges_idx || !fv || !fv->out_degree))
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: missing vertex arrays");
+    if (E > 0 && (!iel || !iel->edges_array_dest))
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: missing inverse edge array");
+    if (E >= 0xFFFFFFF0u)
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: too many edges");
+    const bool want_w = (flags & AG_UPLOAD_WEIGHTS) && iel && iel->edges_array_weight;
+
+    /* host view of the inverse rows: contiguous rows are uploaded as they
+     * are; any other layout (gaps, overlap, reordering) is repacked */
+    std::vector<uint32_t> off(N + 1);
+    bool contiguous = true;
+    uint64_t total = 0;
+    uint32_t maxd = 0;
+    for (uint32_t v = 0; v < N; ++v) {
+        const uint32_t d = iv->out_degree[v];
+        if (iv->edges_idx[v] != total)
+            contiguous = false;
+        if ((uint64_t)iv->edges_idx[v] + d > E)
+            return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: row %u [%u, +%u) exceeds %u edges", v,
+                                iv->edges_idx[v], d, E);
+        off[v] = (uint32_t)total;
+        total += d;
+        if (d > maxd)
+            maxd = d;
+    }
+    if (total != E)
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: in-degrees sum to %llu, expected %u edges",
+                            (unsigned long long)total, E);
+    off[N] = E;
+
+    ag_graph_s *g = new ag_graph_s();
+    memset((void *)g, 0, sizeof(*g));
+    g->N = N;
+    g->E = E;
+    g->E4 = ((E + 3u) & ~3u) + 4u;
+    g->max_in_degree = maxd;
+
+    std::vector<uint4> tf, te;
+    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
+    plan_tasks(off.data(), N, false, tf, &nparts, &nhub);
+    plan_tasks(off.data(), N, true, te, &np2, &nh2);
+    g->ntasks_fast = (uint32_t)tf.size();
+    g->ntasks_exact = (uint32_t)te.size();
+    g->nparts = nparts;
+    g->num_hub_rows = nhub;
+
+    cudaStream_t s = g_ctx.stream;
+    g->row_off = (uint32_t *)dev_alloc(g, (size_t)(N + 1) * 4, &st);
+    g->ids = (uint32_t *)dev_alloc(g, (size_t)g->E4 * 4, &st);
+    g->outdeg = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    if (want_w)
+        g->w = (float *)dev_alloc(g, (size_t)g->E4 * 4, &st);
+    g->tasks_fast = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
+    g->tasks_exact = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
+    g->rank = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    g->c32[0] = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    g->c32[1] = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    g->hub_part = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    g->hub_cnt = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    g->ctl = (AgControl *)dev_alloc(g, sizeof(AgControl), &st);
+    g->flag = (uint32_t *)dev_alloc(g, 16, &st);
+    if (st != AG_OK) {
+        ag_graph_release(g);
+        return st;
+    }
+#define UP(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            st = ag_set_error(AG_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+            ag_graph_release(g);                                                                 \
+            return st;                                                                           \
+        }                                                                                        \
+    } while (0)
+    UP(cudaMemcpyAsync(g->row_off, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
+    UP(cudaMemsetAsync(g->ids + (g->E4 - 8), 0, 32, s));
+    if (contiguous) {
+        if (E)
+            UP(cudaMemcpyAsync(g->ids, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+        if (want_w && E)
+            UP(cudaMemcpyAsync(g->w, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+    } else {
+        std::vector<uint32_t> packed(E);
+        std::vector<float> packw(want_w ? E : 0);
+        for (uint32_t v = 0; v < N; ++v) {
+            const uint32_t d = iv->out_degree[v], b = iv->edges_idx[v];
+            memcpy(packed.data() + off[v], iel->edges_array_dest + b, (size_t)d * 4);
+            if (want_w)
+                memcpy(packw.data() + off[v], iel->edges_array_weight + b, (size_t)d * 4);
+        }
+        if (E)
+            UP(cudaMemcpyAsync(g->ids, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+        if (want_w && E)
+            UP(cudaMemcpyAsync(g->w, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+        UP(cudaStreamSynchronize(s)); /* the packed copies are stack-owned */
+    }
+    if (want_w)
+        UP(cudaMemsetAsync(g->w + (g->E4 - 8), 0, 32, s));
+    if (N)
+        UP(cudaMemcpyAsync(g->outdeg, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+    if (!tf.empty())
+        UP(cudaMemcpyAsync(g->tasks_fast, tf.data(), tf.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    if (!te.empty())
+        UP(cudaMemcpyAsync(g->tasks_exact, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    UP(cudaMemsetAsync(g->hub_cnt, 0, (size_t)nparts * 4 + 16, s));
+    UP(cudaMemsetAsync(g->ctl, 0, sizeof(AgControl), s));
+    UP(cudaMemsetAsync(g->flag, 0, 4, s));
+    UP(cudaMemsetAsync(g->flag + 1, 0xFF, 4, s));
+    if (!(flags & AG_UPLOAD_TRUSTED)) {
+        uint32_t hflag[2] = {0, 0};
+        UP(ag_validate_ids(g->ids, E, N, g->flag, s));
+        UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
+        st = stream_wait(s, 0);
+        if (st != AG_OK) {
+            ag_graph_release(g);
+            return st;
+        }
+        if (hflag[0]) {
+            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1], N);
+            ag_graph_release(g);
+            return st;
+        }
+    }
+    UP(cudaEventCreate(&g->ev0));
+    UP(cudaEventCreate(&g->ev1));
+    /* the host-side vectors die at return: wait for the copies */
+    st = stream_wait(s, 0);
+    if (st != AG_OK) {
+        ag_graph_release(g);
+        return st;
+    }
+#undef UP
+    *out = g;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
+{
+    if (!g || !info)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_get_info: NULL argument");
+    memset(info, 0, sizeof(*info));
+    info->num_vertices = g->N;
+    info->num_edges = g->E;
+    info->num_tasks = g->ntasks_fast;
+    info->num_hub_rows = g->num_hub_rows;
+    info->max_in_degree = g->max_in_degree;
+    info->device_bytes = g->device_bytes;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ag_pull_kernel_ptr(AG_MODE_PR, 0, 0), AG_BLK, 0) ==
+        cudaSuccess)
+        info->grid = (uint32_t)std::min<uint64_t>((uint64_t)nb * g_ctx.num_sms, std::max<uint32_t>(1, g->ntasks_fast));
+    return AG_OK;
+}
+
+/* persistent grid: every SM filled to its occupancy, never more CTAs than
+ * work items */
+static unsigned pull_grid(const void *kern, uint32_t ntasks)
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, AG_BLK, 0) != cudaSuccess || nb < 1)
+        nb = 1;
+    uint64_t g = (uint64_t)nb * (uint64_t)g_ctx.num_sms;
+    if (g > ntasks)
+        g = ntasks;
+    if (g < 1)
+        g = 1;
+    return (unsigned)g;
+}
+
+static ag_status_t ensure_buffers(ag_graph_s *g, int prec)
+{
+    ag_status_t st = AG_OK;
+    if (prec != 0 && !g->c16[0]) {
+        g->c16[0] = (uint16_t *)dev_alloc(g, (size_t)g->N * 2 + 16, &st);
+        g->c16[1] = (uint16_t *)dev_alloc(g, (size_t)g->N * 2 + 16, &st);
+    }
+    return st;
+}
+
+static AgPullParams base_params(ag_graph_s *g, int exact)
+{
+    AgPullParams p;
+    memset(&p, 0, sizeof(p));
+    p.row_off = g->row_off;
+    p.ids = g->ids;
+    p.w = g->w;
+    p.outdeg = g->outdeg;
+    p.tasks = exact ? g->tasks_exact : g->tasks_fast;
+    p.ntasks = exact ? g->ntasks_exact : g->ntasks_fast;
+    p.N = g->N;
+    p.rank = g->rank;
+    p.c32_0 = g->c32[0];
+    p.c32_1 = g->c32[1];
+    p.c16_0 = g->c16[0];
+    p.c16_1 = g->c16[1];
+    p.hub_part = g->hub_part;
+    p.hub_cnt = g->hub_cnt;
+    p.ctl = g->ctl;
+    p.init_ranks = g->init_buf;
+    p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
+    p.damp = Damp;
+    return p;
+}
+
+static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
+{
+    AgExec *x = &g->exe[prec][exact];
+    memset(x, 0, sizeof(*x));
+    AG_CUDA(cudaGraphCreate(&x->graph, 0));
+    AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
+    x->params = base_params(g, exact);
+    x->params.cond = x->cond;
+    const void *kpull = ag_pull_kernel_ptr(AG_MODE_PR, prec, exact);
+    x->grid = pull_grid(kpull, x->params.ntasks);
+
+    AgRunConfig run;
+    memset(&run, 0, sizeof(run));
+    void *init_args[2] = {&x->params, &run};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *)ag_init_kernel_ptr(prec);
+    kp.gridDim = dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)g->N + AG_BLK - 1) / AG_BLK,
+                                                                          (uint64_t)g_ctx.num_sms * 8)));
+    kp.blockDim = dim3(AG_BLK);
+    kp.kernelParams = init_args;
+    AG_CUDA(cudaGraphAddKernelNode(&x->init_node, x->graph, nullptr, 0, &kp));
+
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = x->cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    AG_CUDA(cudaGraphAddNode(&wnode, x->graph, &x->init_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+    void *pull_args[1] = {&x->params};
+    cudaKernelNodeParams kb = {};
+    kb.func = (void *)kpull;
+    kb.gridDim = dim3(x->grid);
+    kb.blockDim = dim3(AG_BLK);
+    kb.kernelParams = pull_args;
+    cudaGraphNode_t pnode;
+    AG_CUDA(cudaGraphAddKernelNode(&pnode, body, nullptr, 0, &kb));
+
+    void *norm_args[1] = {&x->params};
+    cudaKernelNodeParams kn = {};
+    kn.func = (void *)ag_normalize_kernel_ptr();
+    kn.gridDim = kp.gridDim;
+    kn.blockDim = dim3(AG_BLK);
+    kn.kernelParams = norm_args;
+    cudaGraphNode_t nnode;
+    AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
+
+    AG_CUDA(cudaGraphInstantiate(&x->exec, x->graph, 0));
+    g->have_exe[prec][exact] = 1;
+    return AG_OK;
+}
+
+extern "C" void ag_pr_opts_init(ag_pr_opts *o)
+{
+    if (!o)
+        return;
+    memset(o, 0, sizeof(*o));
+    o->struct_size = sizeof(*o);
+    o->precision = AG_PREC_FP32;
+    o->order = AG_ORDER_FAST;
+    o->switch_residual = 1e-4;
+}
+
+extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations, double epsilon,
+                                          const ag_pr_opts *opts)
+{
+    ag_clear_error();
+    if (!g)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_launch: NULL graph");
+    ag_pr_opts o;
+    ag_pr_opts_init(&o);
+    if (opts)
+        memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
+    if (o.precision < 0 || o.precision > 2)
+        return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
+    const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
+    ag_status_t st = ensure_buffers(g, prec);
+    if (st != AG_OK)
+        return st;
+    if (o.init_ranks && !g->init_buf) {
+        g->init_buf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        /* rebuild cached graphs: their parameters carry the warm-start pointer */
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 2; ++b)
+                if (g->have_exe[a][b]) {
+                    free_exec(&g->exe[a][b]);
+                    g->have_exe[a][b] = 0;
+                }
+    }
+    if (!g->have_exe[prec][exact]) {
+        st = build_exec(g, prec, exact);
+        if (st != AG_OK)
+            return st;
+    }
+    AgExec *x = &g->exe[prec][exact];
+    cudaStream_t s = g_ctx.stream;
+    if (o.init_ranks && g->N)
+        AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4, cudaMemcpyHostToDevice, s));
+    AgRunConfig run;
+    memset(&run, 0, sizeof(run));
+    run.max_iter = std::min<uint32_t>(max_iterations, AG_MAX_HISTORY);
+    run.use_init = o.init_ranks ? 1u : 0u;
+    run.eps = epsilon;
+    run.switch_residual = o.switch_residual > 0 ? o.switch_residual : 1e-4;
+    void *init_args[2] = {&x->params, &run};
+    cudaKernelNodeParams kp;
+    AG_CUDA(cudaGraphKernelNodeGetParams(x->init_node, &kp));
+    kp.kernelParams = init_args;
+    AG_CUDA(cudaGraphExecKernelNodeSetParams(x->exec, x->init_node, &kp));
+    AG_CUDA(cudaEventRecord(g->ev0, s));
+    AG_CUDA(cudaGraphLaunch(x->exec, s));
+    AG_CUDA(cudaEventRecord(g->ev1, s));
+    g->launched = 1;
+    g->last_prec = prec;
+    g->last_exact = exact;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_result *res, uint32_t *hist_active,
+                                         double *hist_error, double *hist_seconds, uint32_t history_len)
+{
+    if (!g)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_fetch: NULL graph");
+    if (!g->launched)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_fetch: nothing launched on this graph");
+    cudaStream_t s = g_ctx.stream;
+    ag_status_t st = stream_wait(s, 0);
+    if (st != AG_OK)
+        return st;
+    AgControl *hc = (AgControl *)malloc(sizeof(AgControl));
+    if (!hc)
+        return ag_set_error(AG_ERR_OOM, "host allocation failed");
+    cudaError_t e = cudaMemcpy(hc, g->ctl, sizeof(AgControl), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        free(hc);
+        return ag_set_error(AG_ERR_CUDA, "control readback failed: %s", cudaGetErrorString(e));
+    }
+    if (ranks && g->N) {
+        e = cudaMemcpy(ranks, g->rank, (size_t)g->N * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            free(hc);
+            return ag_set_error(AG_ERR_CUDA, "rank readback failed: %s", cudaGetErrorString(e));
+        }
+    }
+    const uint32_t passes = hc->iter;
+    if (res) {
+        memset(res, 0, sizeof(*res));
+        res->passes = passes;
+        res->converged = hc->converged;
+        res->iterations = hc->converged ? (passes ? passes - 1 : 0) : passes;
+        res->active_last = passes ? hc->hist_active[std::min<uint32_t>(passes, AG_MAX_HISTORY) - 1] : 0;
+        res->error_total = passes ? hc->hist_err[std::min<uint32_t>(passes, AG_MAX_HISTORY) - 1] : 0.0;
+        res->rank_sum = hc->rank_sum;
+        res->switch_pass = hc->switch_pass;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, g->ev0, g->ev1) == cudaSuccess)
+            res->device_ms = ms;
+    }
+    const uint32_t n = std::min<uint32_t>(std::min<uint32_t>(passes, history_len), AG_MAX_HISTORY);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (hist_active)
+            hist_active[i] = hc->hist_active[i];
+        if (hist_error)
+            hist_error[i] = hc->hist_err[i];
+        if (hist_seconds) {
+            const unsigned long long prev = i ? hc->hist_t[i - 1] : hc->t0;
+            hist_seconds[i] = (double)(hc->hist_t[i] - prev) * 1e-9;
+        }
+    }
+    free(hc);
+    return AG_OK;
+}
+
+extern "C" const float *ag_pagerank_device_ranks(ag_graph_t g) { return g ? g->rank : nullptr; }
+
+/* ------------------------------------------------------------------ SpMV */
+extern "C" ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *y, uint32_t mode)
+{
+    ag_clear_error();
+    if (!g || (g->N && (!x || !y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_device: NULL argument");
+    if (g->N == 0)
+        return AG_OK;
+    const int exact = (mode & 2u) ? 1 : 0;
+    AgPullParams p = base_params(g, exact);
+    p.x = x;
+    p.rank = y;
+    p.wmode = (mode & AG_SPMV_UNIT) ? AG_SPMV_W_UNIT : (g->w ? AG_SPMV_W_GRAPH : AG_SPMV_W_CONST);
+    const void *k = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, exact);
+    const unsigned grid = pull_grid(k, p.ntasks);
+    void *args[1] = {&p};
+    AG_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, 0, g_ctx.stream));
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint32_t mode)
+{
+    ag_clear_error();
+    if (!g || (g->N && (!x || !y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull: NULL argument");
+    if (g->N == 0)
+        return AG_OK;
+    ag_status_t st = AG_OK;
+    float *dx = nullptr, *dy = nullptr;
+    cudaStream_t s = g_ctx.stream;
+    AG_CUDA(cudaMallocAsync((void **)&dx, (size_t)g->N * 4, s));
+    AG_CUDA(cudaMallocAsync((void **)&dy, (size_t)g->N * 4, s));
+    AG_CUDA(cudaMemcpyAsync(dx, x, (size_t)g->N * 4, cudaMemcpyHostToDevice, s));
+    st = ag_spmv_pull_device(g, dx, dy, mode);
+    if (st == AG_OK) {
+        cudaError_t e = cudaMemcpyAsync(y, dy, (size_t)g->N * 4, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess)
+            st = ag_set_error(AG_ERR_CUDA, "y readback failed: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(dx, s);
+    cudaFreeAsync(dy, s);
+    ag_status_t w = stream_wait(s, 0);
+    return st != AG_OK ? st : w;
+}
+
+/* -------------------------------------------------------- FP64 oracle */
+extern "C" ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, double tol, double *ranks,
+                                       uint32_t *passes)
+{
+    ag_clear_error();
+    if (!g || !ranks)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_f64: NULL argument");
+    cudaStream_t s = g_ctx.stream;
+    double *r = nullptr, *r2 = nullptr, *c = nullptr, *md = nullptr;
+    const size_t nb = (size_t)g->N * 8 + 16;
+    AG_CUDA(cudaMallocAsync((void **)&r, nb, s));
+    AG_CUDA(cudaMallocAsync((void **)&r2, nb, s));
+    AG_CUDA(cudaMallocAsync((void **)&c, nb, s));
+    AG_CUDA(cudaMallocAsync((void **)&md, 16, s));
+    uint32_t it = 0;
+    cudaError_t e = ag_pr_f64_run(g->row_off, g->ids, g->outdeg, g->N, max_iterations, tol, r, r2, c, md, &it, s);
+    if (e == cudaSuccess && g->N)
+        e = cudaMemcpyAsync(ranks, r, (size_t)g->N * 8, cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(r, s);
+    cudaFreeAsync(r2, s);
+    cudaFreeAsync(c, s);
+    cudaFreeAsync(md, s);
+    ag_status_t w = stream_wait(s, 0);
+    if (e != cudaSuccess)
+        return ag_set_error(AG_ERR_CUDA, "FP64 oracle failed: %s", cudaGetErrorString(e));
+    if (w != AG_OK)
+        return w;
+    for (uint32_t v = 0; v < g->N; ++v)
+        ranks[v] /= (double)g->N;
+    if (passes)
+        *passes = it;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_spmv_run_host(ag_graph_t g, const float *x, float *y, uint32_t iterations, uint32_t mode,
+                                        double *iter_seconds)
+{
+    if (!g || (g->N && (!x || !y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_run_host: NULL argument");
+    if (g->N == 0)
+        return AG_OK;
+    cudaStream_t s = g_ctx.stream;
+    float *dx = nullptr, *dy = nullptr;
+    std::vector<cudaEvent_t> ev(iterations + 1);
+    ag_status_t st = AG_OK;
+    AG_CUDA(cudaMallocAsync((void **)&dx, (size_t)g->N * 4, s));
+    AG_CUDA(cudaMallocAsync((void **)&dy, (size_t)g->N * 4, s));
+    AG_CUDA(cudaMemcpyAsync(dx, x, (size_t)g->N * 4, cudaMemcpyHostToDevice, s));
+    AG_CUDA(cudaMemsetAsync(dy, 0, (size_t)g->N * 4, s));
+    for (uint32_t i = 0; i <= iterations; ++i)
+        AG_CUDA(cudaEventCreate(&ev[i]));
+    AG_CUDA(cudaEventRecord(ev[0], s));
+    for (uint32_t i = 0; i < iterations && st == AG_OK; ++i) {
+        st = ag_spmv_pull_device(g, dx, dy, mode);
+        if (st == AG_OK)
+            AG_CUDA(cudaEventRecord(ev[i + 1], s));
+    }
+    if (st == AG_OK) {
+        cudaError_t e = cudaMemcpyAsync(y, dy, (size_t)g->N * 4, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess)
+            st = ag_set_error(AG_ERR_CUDA, "y readback failed: %s", cudaGetErrorString(e));
+    }
+    ag_status_t w = stream_wait(s, 0);
+    if (st == AG_OK && w == AG_OK && iter_seconds) {
+        for (uint32_t i = 0; i < iterations; ++i) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            iter_seconds[i] = ms * 1e-3;
+        }
+    }
+    for (uint32_t i = 0; i <= iterations; ++i)
+        cudaEventDestroy(ev[i]);
+    cudaFreeAsync(dx, s);
+    cudaFreeAsync(dy, s);
+    return st != AG_OK ? st : w;
+}

@@ -1,0 +1,214 @@
+/*
+ * accelgraph_b200.h -- extended C ABI of the B200 pull PageRank / SpMV library.
+ *
+ * The reference-compatible symbols (pageRankPullGraphCSR, SPMVPullGraphCSR,
+ * ...) are declared in pageRank.h and SPMV.h.  This header adds:
+ *   - status-returning entry points that never exit the process
+ *     (the reference's legacy calls exit on a device failure,
+ *     02_capi_graph/src/capi_utils/capienv.c:113-131);
+ *   - a device-resident graph handle, so repeated runs skip the upload that
+ *     the reference's coherent CAPI memory never needed (capienv.c:832-874
+ *     maps the same arrays into the accelerator's address space);
+ *   - the host graph substrate the reference takes from OpenGraph (edge-list
+ *     to CSR / inverse CSR, seeded RMAT and Erdos-Renyi generators, the 8-byte
+ *     binary edge-list reader) -- OpenGraph is absent from the reference
+ *     checkout, so these restate its documented behaviour (-k: drop self loops
+ *     and duplicates and sort, accel-graph.c:142-145,336-337).
+ * All pointers are plain host or device pointers; no library types from any
+ * framework appear in the signatures.  Every call is made from one host
+ * thread at a time (the reference is not re-entrant either, capienv.c:35-36).
+ */
+#ifndef ACCELGRAPH_B200_H
+#define ACCELGRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "graphConfig.h"
+#include "graphCSR.h"
+#include "pageRank.h"
+#include "SPMV.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef int32_t ag_status_t;
+#define AG_OK                  0
+#define AG_ERR_INVALID_ARG    -1  /* bad argument (NULL, size out of range)      */
+#define AG_ERR_INVALID_GRAPH  -2  /* malformed CSR found by the host or device    */
+#define AG_ERR_CUDA           -3  /* a CUDA call failed; see ag_last_error()      */
+#define AG_ERR_OOM            -4  /* host or device allocation failed             */
+#define AG_ERR_TIMEOUT        -5  /* a bounded host wait ran out                  */
+#define AG_ERR_NO_DEVICE      -6  /* no usable CUDA device                        */
+#define AG_ERR_UNSUPPORTED    -7  /* option not available for this input          */
+
+const char *ag_status_string(ag_status_t status);
+/* Detail of the most recent failure of this thread's last call ("" if none). */
+const char *ag_last_error(void);
+/* Library version string, e.g. "accelgraph-b200 0.1 sm_100a". */
+const char *ag_version(void);
+
+/* ------------------------------------------------------------ device set-up */
+/* Select the CUDA device for this process's library context.  Optional: the
+ * first call that needs a device uses the current device.  */
+ag_status_t ag_init(int device);
+/* The cudaStream_t (as void*) every launch of this library goes to. */
+void *ag_stream(void);
+/* Wait for the library stream, polling with a deadline (seconds; <=0 means
+ * the AG_WAIT_TIMEOUT_S environment variable, default 600).  Returns
+ * AG_ERR_TIMEOUT when the deadline passes with work still queued. */
+ag_status_t ag_synchronize(double timeout_s);
+/* Number of streaming multiprocessors of the library's device (0 if none). */
+int ag_num_sms(void);
+
+/* ------------------------------------------------- host graph substrate */
+#define AG_BUILD_DEDUPE   1u  /* drop self loops and duplicate edges; implies SORT */
+#define AG_BUILD_SORT     2u  /* rows ordered by neighbour id (radix sort)       */
+#define AG_BUILD_PINNED   4u  /* page-locked host arrays (faster uploads)        */
+#define AG_BUILD_WEIGHTS  8u  /* generators: attach weights uniform in [0,1)     */
+
+/* Build forward and inverse CSR from an edge list (src[i] -> dst[i]).
+ * Without SORT, rows keep the input order of their edges (stable counting
+ * sort by source, then a stable one by destination for the inverse).
+ * weight may be NULL.  Returns NULL on failure (see ag_last_error()). */
+struct GraphCSR *ag_graph_from_edges(uint32_t num_vertices, uint64_t num_edges,
+                                     const uint32_t *src, const uint32_t *dst,
+                                     const float *weight, uint32_t flags);
+/* Seeded R-MAT (Graph500 quadrant recursion, no noise, no relabelling):
+ * 2^scale vertices, edge_factor * 2^scale generated edges, quadrant
+ * probabilities a, b, c (d = 1-a-b-c).  Weights, when requested, are
+ * uniform in [0,1) drawn per forward edge from seed + 1. */
+struct GraphCSR *ag_graph_rmat(uint32_t scale, uint32_t edge_factor,
+                               double a, double b, double c,
+                               uint64_t seed, uint32_t flags);
+/* Seeded directed Erdos-Renyi: num_vertices * avg_degree edges with
+ * independent uniform endpoints. */
+struct GraphCSR *ag_graph_er(uint32_t num_vertices, uint32_t avg_degree,
+                             uint64_t seed, uint32_t flags);
+/* Binary edge list: 8 bytes per edge (uint32 src, uint32 dst), or 12 bytes
+ * (..., float weight) when weighted != 0.  num_vertices = max id + 1. */
+struct GraphCSR *ag_graph_read_edge_file(const char *path, int weighted, uint32_t flags);
+/* Free a graph returned by one of the builders above. */
+void ag_graph_free(struct GraphCSR *graph);
+/* n values uniform in [0,1) from the library's counter-based generator. */
+void ag_fill_uniform(float *out, uint64_t n, uint64_t seed);
+
+/* ------------------------------------------------- device-resident graph */
+typedef struct ag_graph_s *ag_graph_t;
+
+#define AG_UPLOAD_WEIGHTS  1u  /* also upload inverse edge weights (SpMV)    */
+#define AG_UPLOAD_VALIDATE 2u  /* kept for clarity: the check is the default  */
+#define AG_UPLOAD_TRUSTED  4u  /* skip the device check that every in-edge
+                                  names a vertex < num_vertices (the caller
+                                  guarantees it); without this flag a bad id
+                                  makes the upload fail with
+                                  AG_ERR_INVALID_GRAPH before any kernel
+                                  reads through it                          */
+
+typedef struct ag_graph_info
+{
+    uint32_t num_vertices;
+    uint32_t num_edges;
+    uint32_t num_tasks;      /* work items of the fused pull kernel           */
+    uint32_t num_hub_rows;   /* rows split across several CTAs                */
+    uint32_t grid;           /* persistent CTAs per launch                    */
+    uint32_t max_in_degree;
+    uint64_t device_bytes;   /* device memory held by the handle              */
+} ag_graph_info;
+
+/* Copy the inverse CSR (and forward out-degrees) of `graph` to the device
+ * and plan the kernel work list.  The handle stays valid until released;
+ * the host graph may be freed after the call returns. */
+ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out);
+ag_status_t ag_graph_release(ag_graph_t g);
+ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info);
+
+/* --------------------------------------------------------------- PageRank */
+#define AG_PREC_FP32 0   /* contributions stored in binary32 (reference)     */
+#define AG_PREC_BF16 1   /* contributions stored in bfloat16, FP32 accumulate */
+#define AG_PREC_FP16 2   /* contributions stored in binary16, FP32 accumulate */
+
+#define AG_ORDER_FAST  0 /* rows of <= 32 in-edges summed in stream order,
+                            longer rows by a fixed lane-strided tree         */
+#define AG_ORDER_EXACT 1 /* every row summed in stream order: bit-identical
+                            to a sequential binary32 loop                    */
+
+typedef struct ag_pr_opts
+{
+    uint32_t struct_size;      /* sizeof(ag_pr_opts)                          */
+    int32_t precision;         /* AG_PREC_*                                   */
+    int32_t order;             /* AG_ORDER_*                                  */
+    int32_t quiet;             /* nonzero: print no tables                    */
+    double switch_residual;    /* low-precision forms switch to FP32 storage
+                                  once a pass's error_total falls below this
+                                  (<= 0: 1e-4), or when the residual stops
+                                  falling                                     */
+    const float *init_ranks;   /* warm start: num_vertices un-normalised ranks,
+                                  host pointer; NULL = base_pr everywhere     */
+} ag_pr_opts;
+
+typedef struct ag_pr_result
+{
+    uint32_t iterations;       /* reference semantics (see pageRank.h)        */
+    uint32_t passes;           /* pull passes executed                        */
+    uint32_t converged;        /* 1 if a pass had no active vertex            */
+    uint32_t active_last;      /* active vertices of the last pass            */
+    uint32_t switch_pass;      /* first pass that read FP32 contributions
+                                  (low-precision forms; 0 for FP32)           */
+    uint32_t reserved;
+    double error_total;        /* last pass's mean |r' - r|                   */
+    double rank_sum;           /* sum of normalised ranks (FP64)              */
+    double device_ms;          /* device time of the solve                    */
+} ag_pr_result;
+
+void ag_pr_opts_init(ag_pr_opts *opts);
+
+/* Status-returning form of pageRankPullGraphCSR with the precision, order and
+ * warm-start options.  *out receives a stats object owned by the caller. */
+ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph,
+                                const ag_pr_opts *opts, struct PageRankStats **out);
+
+/* Device-resident solve: enqueue init, the iteration loop (one CUDA graph with
+ * an on-device convergence test) and normalisation on ag_stream().  Returns
+ * without waiting.  Results stay in the handle until the next launch. */
+ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations, double epsilon,
+                               const ag_pr_opts *opts);
+/* Wait for the last launch and copy its results.  ranks: host array of
+ * num_vertices normalised ranks, or NULL.  history arrays (host, may be NULL)
+ * receive per-pass active counts, error totals and device seconds for up to
+ * history_len passes. */
+ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_result *result,
+                              uint32_t *hist_active, double *hist_error,
+                              double *hist_seconds, uint32_t history_len);
+/* Device pointer to the normalised ranks of the last launch (valid until the
+ * next launch on the handle). */
+const float *ag_pagerank_device_ranks(ag_graph_t g);
+
+/* FP64 oracle on the GPU: every operation in binary64 (contribution,
+ * gather, update), iterated until max |r' - r| <= tol or max_iterations.
+ * ranks (host, num_vertices) receives normalised FP64 ranks. */
+ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, double tol,
+                            double *ranks, uint32_t *passes);
+
+/* ------------------------------------------------------------------- SpMV */
+#define AG_SPMV_GRAPH_WEIGHTS 0u /* w = uploaded inverse weights (0.0001f if none) */
+#define AG_SPMV_UNIT          1u /* pure gather: y[v] = sum x[u]                   */
+#define AG_SPMV_EXACT         2u /* every row summed in stream order (bit-identical
+                                    to a sequential binary32 loop)                */
+
+/* y = A x over the inverse CSR on ag_stream(); x and y are device pointers of
+ * num_vertices floats.  Rows without in-edges get y[v] = 0. */
+ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *y, uint32_t mode);
+/* Host-pointer form: uploads x, runs, copies y back and waits. */
+ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint32_t mode);
+/* Status-returning form of SPMVPullGraphCSR. */
+ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph,
+                            int quiet, struct SPMVStats **out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACCELGRAPH_B200_H */

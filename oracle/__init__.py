@@ -1,0 +1,120 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, as the checker or the timed CPU baseline.  The
+product package accelgraph_b200 never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+u32p = C.POINTER(C.c_uint32)
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+
+
+def build(force: bool = False) -> Path:
+    if force or not LIB.exists() or LIB.stat().st_mtime < (HERE / "ag_oracle.c").stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    return LIB
+
+
+def _load() -> C.CDLL:
+    build()
+    lib = C.CDLL(str(LIB))
+    lib.oracle_gather.argtypes = [C.c_uint32, u32p, u32p, u32p, f32p, f32p, C.c_int]
+    lib.oracle_spmv_pull.argtypes = [C.c_uint32, u32p, u32p, u32p, f32p, f32p, f32p, C.c_int]
+    lib.oracle_spmv_input.argtypes = [C.c_uint32, u32p, f32p]
+    lib.oracle_spmv_checksum.argtypes = [C.c_uint32, f32p]
+    lib.oracle_spmv_checksum.restype = C.c_double
+    lib.oracle_pagerank_pull.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p, f32p,
+                                         u32p, f64p, f64p, u32p, f64p, f64p, C.c_int]
+    lib.oracle_pagerank_pull.restype = C.c_uint32
+    lib.oracle_pagerank_f64.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f64p, C.c_int]
+    lib.oracle_pagerank_f64.restype = C.c_uint32
+    lib.oracle_max_threads.restype = C.c_int
+    return lib
+
+
+lib = _load()
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _csr(in_idx, in_deg, in_nb):
+    return (np.ascontiguousarray(in_idx, np.uint32), np.ascontiguousarray(in_deg, np.uint32),
+            np.ascontiguousarray(in_nb, np.uint32))
+
+
+def gather(in_idx, in_deg, in_nb, x, threads=0):
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros(len(in_deg), np.float32)
+    lib.oracle_gather(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(x, f32p),
+                      _p(y, f32p), threads)
+    return y
+
+
+def spmv_pull(in_idx, in_deg, in_nb, w, x, threads=0):
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    x = np.ascontiguousarray(x, np.float32)
+    w = None if w is None else np.ascontiguousarray(w, np.float32)
+    y = np.zeros(len(in_deg), np.float32)
+    lib.oracle_spmv_pull(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(w, f32p),
+                         _p(x, f32p), _p(y, f32p), threads)
+    return y
+
+
+def spmv_input(out_deg):
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    x = np.zeros(len(out_deg), np.float32)
+    lib.oracle_spmv_input(len(out_deg), _p(out_deg, u32p), _p(x, f32p))
+    return x
+
+
+def spmv_checksum(y):
+    y = np.ascontiguousarray(y, np.float32)
+    return lib.oracle_spmv_checksum(len(y), _p(y, f32p))
+
+
+def pagerank_pull(in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4, init=None, threads=0):
+    """Returns dict(ranks, iterations, passes, error_total, rank_sum, active, error, seconds)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    n = len(in_deg)
+    init = None if init is None else np.ascontiguousarray(init, np.float32)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    rs = C.c_double()
+    cap = max(iterations, 1)
+    ha = np.zeros(cap, np.uint32)
+    he = np.zeros(cap, np.float64)
+    hs = np.zeros(cap, np.float64)
+    passes = lib.oracle_pagerank_pull(n, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_deg, u32p),
+                                      iterations, epsilon, _p(init, f32p), _p(ranks, f32p), C.byref(it),
+                                      C.byref(et), C.byref(rs), _p(ha, u32p), _p(he, f64p), _p(hs, f64p), threads)
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "rank_sum": rs.value, "active": ha[:passes], "error": he[:passes], "seconds": hs[:passes]}
+
+
+def pagerank_f64(in_idx, in_deg, in_nb, out_deg, max_iter=1000, tol=1e-13, threads=0):
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    r = np.zeros(len(in_deg), np.float64)
+    passes = lib.oracle_pagerank_f64(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p),
+                                     _p(out_deg, u32p), max_iter, tol, _p(r, f64p), threads)
+    return r, passes
+
+
+def max_threads() -> int:
+    return lib.oracle_max_threads()

@@ -1,0 +1,224 @@
+/*
+ * ag_oracle.c -- CPU oracle of the pull PageRank / SpMV hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py load this library, and only
+ * as the checker or the timed CPU baseline; the product library never links
+ * or calls it.
+ *
+ * The reference's OpenMP pull PageRank lives in the OpenGraph submodule,
+ * which is empty in the reference checkout, so this is a restatement of the
+ * loops that are present in the reference sources:
+ *   host steps   02_capi_graph/src/algorithms/capi/pageRank.c:942-1109
+ *                (init 50-78, contribution loop 1026-1033, update/residual
+ *                loop 1055-1069, stop test 1073-1074, normalise 1079-1085)
+ *   CPU gather   pageRank.c:2890-2907 (inverse CSR: degree =
+ *                inverse_vertices->out_degree[v], u = edges_array_dest[j],
+ *                nodeIncomingPR += riDividedOnDiClause[u], from 0.0f) and
+ *                pageRank.c:3419-3439 (schedule(dynamic, 1024))
+ *   SpMV pull    02_capi_graph/src/algorithms/capi/SPMV.c:622-751 (input
+ *                vector 694-701, checksum 726-730) with the per-edge product
+ *                of SPMV.c:1200-1224 (weight * x[src]; 0.0001f unweighted)
+ * compiled with the reference's flags (-O3 -Wall -m64 -fopenmp,
+ * 02_capi_graph/Makefile:250), which on x86-64 keeps every binary32 multiply
+ * and add separate (no FMA contraction).
+ * The gather arithmetic (sequential binary32 in stream order) is pinned by the
+ * RTL testbench goldens (pagerank_kernel_tb.sv:303-314, spmv_kernel_tb.sv:
+ * 349-359) through tests/golden/rtl_fixtures.json.
+ */
+#include <math.h>
+#include <omp.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#define ORACLE_DAMP 0.85f
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* y[v] = sum over v's inverse row of x[u], binary32 from 0.0f in stream order */
+void oracle_gather(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                   const float *x, float *y, int threads)
+{
+    uint32_t v;
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (v = 0; v < n; v++) {
+        float s = 0.0f;
+        uint32_t j, b = in_idx[v], d = in_deg[v];
+        for (j = b; j < b + d; j++)
+            s += x[in_nb[j]];
+        y[v] = s;
+    }
+}
+
+/* y[v] = sum of (w_j * x[u_j]) -- one binary32 multiply, then a binary32 add
+ * in stream order; w == NULL uses the reference's unweighted 0.0001f */
+void oracle_spmv_pull(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                      const float *w, const float *x, float *y, int threads)
+{
+    uint32_t v;
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(threads > 0 ? threads : omp_get_max_threads())
+    for (v = 0; v < n; v++) {
+        float s = 0.0f;
+        uint32_t j, b = in_idx[v], d = in_deg[v];
+        for (j = b; j < b + d; j++) {
+            float wj = w ? w[j] : 0.0001f;
+            float prod = wj * x[in_nb[j]];
+            s += prod;
+        }
+        y[v] = s;
+    }
+}
+
+/* SPMV.c:694-701 input vector and SPMV.c:726-730 checksum */
+void oracle_spmv_input(uint32_t n, const uint32_t *out_deg, float *x)
+{
+    uint32_t v;
+    for (v = 0; v < n; v++)
+        x[v] = out_deg[v] ? (1.0f / out_deg[v]) : 0.001f;
+}
+
+double oracle_spmv_checksum(uint32_t n, const float *y)
+{
+    double sum = 0.0;
+    uint32_t v;
+    for (v = 0; v < n; v++)
+        sum += ((int)(y[v] * 100 + .5) / 100.0);
+    return sum;
+}
+
+/* pageRankPullGraphCSR restated.  ranks_out receives the normalised ranks.
+ * init (n floats, may be NULL) replaces base_pr as the starting ranks.
+ * hist_active / hist_err / hist_sec (may be NULL, >= iterations entries)
+ * receive the per-pass record.  Returns stats->iterations semantics in
+ * *iterations_out, the last pass's error_total in *error_total, the FP64
+ * rank sum in *rank_sum and the number of passes executed (return value). */
+uint32_t oracle_pagerank_pull(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                              const uint32_t *out_deg, uint32_t iterations, double epsilon, const float *init,
+                              float *ranks_out, uint32_t *iterations_out, double *error_total_out,
+                              double *rank_sum_out, uint32_t *hist_active, double *hist_err, double *hist_sec,
+                              int threads)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    float *pageRanks = ranks_out;
+    float *pageRanksNext = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    float *riDividedOnDiClause = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v;
+
+    for (v = 0; v < n; v++) {
+        pageRanks[v] = init ? init[v] : base_pr;
+        pageRanksNext[v] = 0.0f;
+    }
+    for (it = 0; it < iterations; it++) {
+        double t0 = now_s();
+        error_total = 0;
+        activeVertices = 0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++) {
+            if (out_deg[v])
+                riDividedOnDiClause[v] = pageRanks[v] / out_deg[v];
+            else
+                riDividedOnDiClause[v] = 0.0f;
+        }
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            uint32_t j, b = in_idx[v], d = in_deg[v];
+            float nodeIncomingPR = 0.0f;
+            for (j = b; j < b + d; j++)
+                nodeIncomingPR += riDividedOnDiClause[in_nb[j]];
+            pageRanksNext[v] = nodeIncomingPR;
+        }
+#pragma omp parallel for reduction(+ : error_total, activeVertices) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            float prevPageRank = pageRanks[v];
+            float nextPageRank = base_pr + (damp * pageRanksNext[v]);
+            pageRanks[v] = nextPageRank;
+            pageRanksNext[v] = 0.0f;
+            double error = fabs(nextPageRank - prevPageRank);
+            error_total += (error / n);
+            if (error >= epsilon)
+                activeVertices++;
+        }
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (hist_err)
+            hist_err[it] = error_total;
+        if (hist_sec)
+            hist_sec[it] = now_s() - t0;
+        if (activeVertices == 0)
+            break;
+    }
+    {
+        double sum = 0.0;
+#pragma omp parallel for reduction(+ : sum) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            pageRanks[v] = pageRanks[v] / n;
+            sum += pageRanks[v];
+        }
+        if (rank_sum_out)
+            *rank_sum_out = sum;
+    }
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(pageRanksNext);
+    free(riDividedOnDiClause);
+    return passes;
+}
+
+/* FP64 fixpoint with the reference's constants ((double)0.85f and
+ * (double)(1.0f - 0.85f)): every operation in binary64, iterated until
+ * max |r' - r| <= tol or max_iter passes.  ranks_out receives r / n. */
+uint32_t oracle_pagerank_f64(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                             const uint32_t *out_deg, uint32_t max_iter, double tol, double *ranks_out,
+                             int threads)
+{
+    const double damp = (double)0.85f, base = (double)(1.0f - 0.85f);
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    double *r = ranks_out;
+    double *c = (double *)malloc((size_t)(n ? n : 1) * sizeof(double));
+    double *rn = (double *)malloc((size_t)(n ? n : 1) * sizeof(double));
+    uint32_t it, v;
+    for (v = 0; v < n; v++)
+        r[v] = base;
+    for (it = 0; it < max_iter; it++) {
+        double md = 0.0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++)
+            c[v] = out_deg[v] ? r[v] / (double)out_deg[v] : 0.0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(max : md) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            double s = 0.0;
+            uint32_t j, b = in_idx[v], d = in_deg[v];
+            for (j = b; j < b + d; j++)
+                s += c[in_nb[j]];
+            rn[v] = base + damp * s;
+            double dd = fabs(rn[v] - r[v]);
+            if (dd > md)
+                md = dd;
+        }
+        memcpy(r, rn, (size_t)n * sizeof(double));
+        if (md <= tol) {
+            it++;
+            break;
+        }
+    }
+    for (v = 0; v < n; v++)
+        r[v] /= (double)n;
+    free(c);
+    free(rn);
+    return it;
+}
+
+int oracle_max_threads(void) { return omp_get_max_threads(); }
