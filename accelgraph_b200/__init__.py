@@ -123,6 +123,7 @@ AG_ERR_INVALID_ARG, AG_ERR_INVALID_GRAPH, AG_ERR_CUDA, AG_ERR_OOM = -1, -2, -3, 
 AG_ERR_TIMEOUT, AG_ERR_NO_DEVICE, AG_ERR_UNSUPPORTED = -5, -6, -7
 AG_BUILD_DEDUPE, AG_BUILD_SORT, AG_BUILD_PINNED, AG_BUILD_WEIGHTS = 1, 2, 4, 8
 AG_UPLOAD_WEIGHTS, AG_UPLOAD_VALIDATE, AG_UPLOAD_TRUSTED = 1, 2, 4
+AG_UPLOAD_KEEP_ORDER, AG_UPLOAD_NO_SMEM_CACHE = 8, 16
 AG_PREC_FP32, AG_PREC_BF16, AG_PREC_FP16 = 0, 1, 2
 AG_ORDER_FAST, AG_ORDER_EXACT = 0, 1
 AG_SPMV_GRAPH_WEIGHTS, AG_SPMV_UNIT, AG_SPMV_EXACT = 0, 1, 2
@@ -350,9 +351,9 @@ class Graph:
 class DeviceGraph:
     """ag_graph_t: the inverse CSR resident on the GPU."""
 
-    def __init__(self, graph: Graph, weights: bool = False, validate: bool = False):
+    def __init__(self, graph: Graph, weights: bool = False, validate: bool = False, flags: int = 0):
         h = C.c_void_p()
-        flags = (AG_UPLOAD_WEIGHTS if weights else 0) | (AG_UPLOAD_VALIDATE if validate else 0)
+        flags |= (AG_UPLOAD_WEIGHTS if weights else 0) | (AG_UPLOAD_VALIDATE if validate else 0)
         check(lib.ag_graph_upload(graph.ptr, flags, C.byref(h)), "ag_graph_upload")
         self.h = h
         self.num_vertices = graph.num_vertices

@@ -24,7 +24,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libaccelgraph_b200.so"
 
 C_SOURCES = ["graph_host.c", "ag_capi.c"]
-CU_SOURCES = ["ag_pull.cu", "ag_runtime.cu"]
+CU_SOURCES = ["ag_pull.cu", "ag_layout.cu", "ag_runtime.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -45,38 +45,44 @@ def _run(cmd: list[str], verbose: bool) -> None:
         print(res.stdout + res.stderr, flush=True)
 
 
-def _stale() -> bool:
-    if not LIB.exists():
+def _stale(lib: Path = LIB) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = [CSRC / s for s in C_SOURCES + CU_SOURCES]
     deps += list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h")) + [Path(__file__)]
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library if it is missing or out of date; return its path."""
-    if not force and not _stale():
-        return LIB
+def build(force: bool = False, verbose: bool = False, out: Path | None = None, defines: tuple = ()) -> Path:
+    """Compile the library if it is missing or out of date; return its path.
+
+    `defines` (e.g. ("AG_WHUB=1024",)) override the tiling constants of
+    csrc/ag_device.h for a tuning build written to `out`."""
+    lib = Path(out) if out else LIB
+    if not force and not _stale(lib):
+        return lib
     nvcc = _nvcc()
-    BUILD.mkdir(exist_ok=True)
+    build_dir = BUILD if not out else lib.parent / "_build"
+    build_dir.mkdir(parents=True, exist_ok=True)
+    dflags = [f"-D{d}" for d in defines]
     inc = ["-I", str(INCLUDE), "-I", str(CSRC)]
     objs = []
     for src in C_SOURCES:
-        obj = BUILD / (src + ".o")
-        _run(["gcc", "-O3", "-Wall", "-m64", "-fopenmp", "-fPIC", "-std=gnu11", *inc, "-c", str(CSRC / src),
+        obj = build_dir / (src + ".o")
+        _run(["gcc", "-O3", "-Wall", "-m64", "-fopenmp", "-fPIC", "-std=gnu11", *inc, *dflags, "-c", str(CSRC / src),
               "-o", str(obj)], verbose)
         objs.append(str(obj))
     for src in CU_SOURCES:
-        obj = BUILD / (src + ".o")
-        _run([nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", *inc, "-c",
+        obj = build_dir / (src + ".o")
+        _run([nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", *inc, *dflags, "-c",
               str(CSRC / src), "-o", str(obj)], verbose)
         objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp",
           "-lpthread", "-lrt"], verbose)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

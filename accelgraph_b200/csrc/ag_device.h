@@ -22,21 +22,54 @@
 #include <stdint.h>
 
 /* ---------------------------------------------------------- tiling */
-#define AG_BLK 256        /* threads per CTA of the pull kernel             */
-#define AG_CAP 2048       /* in-edges staged in shared memory per row block */
-#define AG_RMAX 1024      /* rows per row block                             */
+#ifndef AG_BLK
+#define AG_BLK 1024       /* threads per CTA of the pull kernel              */
+#endif
+#ifndef AG_CTAS_PER_SM
+#define AG_CTAS_PER_SM 1  /* pull CTAs resident per SM; each holds its own
+                             copy of the hot table                          */
+#endif
+#define AG_WARPS (AG_BLK / 32)
+#define AG_SBLK 256       /* threads per CTA of the element-wise kernels     */
+#ifndef AG_WCAP
+#define AG_WCAP 256       /* in-edges staged in shared memory per warp task  */
+#endif
+#define AG_WROWS 32       /* rows per warp task (one per lane)              */
 #define AG_TSEQ 32        /* FAST order: rows up to this length summed by
-                             one thread in stream order                     */
-#define AG_HUB 8192       /* rows longer than this are split into chunks of
-                             AG_HUB in-edges processed by separate CTAs     */
-#define AG_LONG_MAX 64    /* rows longer than AG_TSEQ inside one row block  */
+                             one lane in stream order                       */
+#ifndef AG_WHUB
+#define AG_WHUB 2048      /* FAST order: rows longer than this are split
+                             into chunks of AG_WHUB in-edges on separate
+                             warps; EXACT order keeps them on one warp      */
+#endif
+#define AG_STAGE_BYTES (AG_WARPS * AG_WCAP * 4)
+#if AG_CTAS_PER_SM == 1
+#define AG_SMEM_MAX 232448 /* shared memory per CTA: the 227 KB maximum     */
+#else
+#define AG_SMEM_MAX (233472 / AG_CTAS_PER_SM - 1024)
+#endif
+#define AG_SMEM_STATIC 1024 /* static shared memory of the pull kernel (upper bound) */
+#ifndef AG_HOT_CAP
+#define AG_HOT_CAP (1u << 30)
+#endif
+#define AG_HOT_FIT ((AG_SMEM_MAX - AG_SMEM_STATIC - AG_STAGE_BYTES) / 4 / 64 * 64)
+#define AG_HOT_MAX (AG_HOT_FIT < AG_HOT_CAP ? AG_HOT_FIT : AG_HOT_CAP)
+#define AG_BULK_CHUNK 32768u
 
-/* task kinds (low 2 bits of task.x) */
-#define AG_T_BLOCK 0u     /* y = first row, z = end row                     */
-#define AG_T_ROW 1u       /* y = row (AG_CAP < degree <= AG_HUB, or any
-                             degree > AG_CAP in EXACT order)                */
-#define AG_T_HUB 2u       /* x >> 2 = chunk, y = row, z = partial base,
-                             w = number of chunks                           */
+/* A task is one warp's work item (uint4):
+ *   x = kind << 30 | first row      y = end row (ROWS) or partial slot (HUB)
+ *   z = first in-edge               w = end in-edge
+ * ROWS: rows [x, y) holding <= AG_WCAP in-edges, at most AG_WROWS rows,
+ *       each of degree <= AG_WCAP.
+ * LONG: one row x with AG_WCAP < degree (<= AG_WHUB in FAST order).
+ * HUB : in-edges [z, w) of row x; y = partial base (low 20 bits) |
+ *       chunk index << 20.  The row's chunk count follows from its degree. */
+#define AG_T_ROWS 0u
+#define AG_T_LONG 1u
+#define AG_T_HUB 2u
+#define AG_ROW_MASK 0x3FFFFFFFu
+#define AG_SLOT_BITS 20
+#define AG_SLOT_MASK ((1u << AG_SLOT_BITS) - 1u)
 
 #define AG_MODE_PR 0
 #define AG_MODE_SPMV 1
@@ -65,6 +98,8 @@ typedef struct AgControl
     unsigned long long t0;    /* %globaltimer at the end of the init kernel */
     uint32_t use_init;        /* warm start from init_ranks                 */
     uint32_t low_passes;      /* passes that read 16-bit contributions      */
+    uint32_t stop;            /* 1 once the loop is over (stream launches)  */
+    uint32_t fault;           /* nonzero: a bounded device wait ran out     */
     uint32_t hist_active[AG_MAX_HISTORY];
     double hist_err[AG_MAX_HISTORY];
     unsigned long long hist_t[AG_MAX_HISTORY];
@@ -99,6 +134,12 @@ typedef struct AgPullParams
     const float *init_ranks;
     float base, damp;
     int wmode;             /* AG_SPMV_W_* */
+    uint32_t use_cond;     /* 1: launched by the CUDA graph's WHILE node      */
+    uint32_t hot_n;        /* contributions (ids < hot_n) served from shared
+                              memory; a multiple of 64                         */
+    const uint32_t *perm;  /* device row i is caller vertex perm[i]            */
+    const uint32_t *inv;   /* caller vertex v is device row inv[v]             */
+    float *out;            /* normalised ranks in caller order                 */
     cudaGraphConditionalHandle cond;
 } AgPullParams;
 
@@ -111,6 +152,12 @@ const void *ag_pull_kernel_ptr(int mode, int prec, int exact);
 const void *ag_init_kernel_ptr(int prec);
 const void *ag_normalize_kernel_ptr(void);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
+cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
+                                     const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,
+                                     uint32_t *inv, uint32_t *off_new, uint32_t *ids_new, float *w_new,
+                                     uint32_t *outdeg_new, cudaStream_t s);
+cudaError_t ag_permute_in(const uint32_t *perm, const float *x, float *x_new, uint32_t n, cudaStream_t s);
+cudaError_t ag_permute_out(const uint32_t *inv, const float *y_new, float *y, uint32_t n, cudaStream_t s);
 cudaError_t ag_pr_f64_run(const uint32_t *row_off, const uint32_t *ids, const uint32_t *outdeg, uint32_t N,
                           uint32_t max_iter, double tol, double *r, double *r2, double *c, double *maxdiff,
                           uint32_t *passes_out, cudaStream_t s);

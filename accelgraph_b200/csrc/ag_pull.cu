@@ -15,20 +15,24 @@
  * the last CTA to finish closing the pass: it records the pass, decides
  * whether another pass runs and sets the CUDA-graph WHILE condition.
  *
- * Work decomposition (planned once per graph on the host, see ag_runtime.cu):
- *   row block : consecutive rows holding <= AG_CAP in-edges.  Phase 1 streams
- *               the block's ids with 16-byte loads (L1 no-allocate, L2
- *               evict-first) and gathers c[id] (L2 evict-last) into shared
- *               memory -- every gather of the block is independent, so the
- *               loads overlap.  Phase 2 reduces each row from shared memory:
- *               one thread per row in stream order for rows of <= AG_TSEQ
- *               edges (bit-identical to the reference's sequential sum), one
- *               warp per longer row (lane-strided partial sums + xor tree).
- *   long row  : AG_CAP < degree <= AG_HUB, one CTA, lane-strided partials and
- *               a fixed-order CTA reduction.
- *   hub chunk : rows > AG_HUB split into AG_HUB chunks on separate CTAs; the
- *               last chunk to arrive sums the chunk partials in chunk order.
- * In EXACT order every row is summed in stream order by one thread.
+ * Work decomposition (planned once per graph on the host, see ag_runtime.cu).
+ * Every task is one WARP's work item; warps of a persistent grid take tasks
+ * in a fixed stride and never wait for each other inside a pass, so the SM
+ * always holds warps in every phase (loading ids, gathering, reducing):
+ *   rows : up to 32 consecutive rows holding <= AG_WCAP in-edges.  The warp
+ *          streams the ids with 16-byte loads (L1 no-allocate, L2
+ *          evict-first), gathers c[id] (L2 evict-last) into its slice of
+ *          shared memory -- up to 256 independent gathers in flight -- while
+ *          each lane's row bounds, previous rank and out-degree load in the
+ *          background.  A lane then sums its row in stream order (rows of
+ *          <= AG_TSEQ edges: bit-identical to the reference's sequential
+ *          sum); longer rows are summed by the whole warp (lane-strided
+ *          partials + xor tree).  The update runs lane-parallel.
+ *   long : one row of AG_WCAP < degree <= AG_WHUB, warp-strided partials
+ *          straight from memory + xor tree.
+ *   hub  : rows > AG_WHUB split into AG_WHUB-edge chunks on separate warps;
+ *          the last chunk to arrive sums the chunk partials in chunk order.
+ * In EXACT order every row is summed in stream order by one lane.
  * All reductions have a fixed order: results do not depend on scheduling.
  */
 #include <cuda_bf16.h>
@@ -39,7 +43,7 @@
 
 #include "ag_device.h"
 
-#define AG_NW (AG_BLK / 32)
+#define AG_SNW (AG_SBLK / 32)
 
 /* ------------------------------------------------------ memory access */
 __device__ __forceinline__ uint64_t ag_policy_evict_first()
@@ -107,6 +111,53 @@ __device__ __forceinline__ unsigned long long ag_globaltimer()
     return t;
 }
 
+/* ---------------------------------------------- TMA bulk copy to smem */
+__device__ __forceinline__ uint32_t ag_smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void ag_mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ag_smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void ag_mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ag_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+/* one bulk global->shared copy (16-byte aligned, size a multiple of 16)
+ * completing on the CTA's mbarrier */
+__device__ __forceinline__ void ag_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     ag_smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(ag_smem_addr(bar))
+                 : "memory");
+}
+
+/* bounded wait for the mbarrier phase to complete; false if the limit ran
+ * out first */
+__device__ __forceinline__ bool ag_mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit)
+{
+    const uint32_t a = ag_smem_addr(bar);
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(a), "r"(phase)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
 /* 16-bit contribution formats of the precision form */
 template <int PREC>
 __device__ __forceinline__ float ag_low_to_f32(uint16_t h)
@@ -149,25 +200,6 @@ __device__ __forceinline__ uint32_t ag_warp_sum_u(uint32_t v)
     return v;
 }
 
-/* fixed-order CTA sum; the result is valid in thread 0 */
-__device__ __forceinline__ float ag_block_sum_f(float v, float *sh)
-{
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = ag_warp_sum_f(v);
-    if (lane == 0)
-        sh[warp] = v;
-    __syncthreads();
-    float s = 0.0f;
-    if (threadIdx.x == 0) {
-        s = sh[0];
-#pragma unroll
-        for (int w = 1; w < AG_NW; ++w)
-            s = __fadd_rn(s, sh[w]);
-    }
-    __syncthreads();
-    return s;
-}
-
 /* ------------------------------------------------------------- kernel */
 template <int MODE, int PREC, bool EXACT>
 struct AgPass
@@ -182,9 +214,15 @@ struct AgPass
     double eps;
     double my_err;
     uint32_t my_active;
+    const float *hot32;     /* shared-memory copy of the first hot_n values */
+    const uint16_t *hot16;
+    uint32_t hot_n;
 
     __device__ __forceinline__ AgPass(const AgPullParams &pp) : p(pp)
     {
+        hot32 = nullptr;
+        hot16 = nullptr;
+        hot_n = 0;
         pol_first = ag_policy_evict_first();
         pol_last = ag_policy_evict_last();
         my_err = 0.0;
@@ -210,34 +248,46 @@ struct AgPass
         }
     }
 
-    /* value gathered for in-edge j with source u (weight wj for SpMV) */
+    /* the vector this pass gathers from, and its element size */
+    __device__ __forceinline__ const void *gather_source() const
+    {
+        if (MODE == AG_MODE_SPMV)
+            return p.x;
+        if (PREC != 0 && read_low)
+            return c_in16;
+        return c_in32;
+    }
+
+    __device__ __forceinline__ uint32_t gather_elem_bytes() const { return (PREC != 0 && read_low) ? 2u : 4u; }
+
+    /* value gathered for an in-edge with source u (weight wj for SpMV):
+     * from the shared-memory table when u is hot, else from global memory */
     __device__ __forceinline__ float gather(uint32_t u, float wj) const
     {
         if (MODE == AG_MODE_SPMV) {
-            const float xv = ag_ld_gather_f32(p.x + u, pol_last);
+            const float xv = (u < hot_n) ? hot32[u] : ag_ld_gather_f32(p.x + u, pol_last);
             if (p.wmode == AG_SPMV_W_UNIT)
                 return xv;
             return __fmul_rn(wj, xv);
         }
         if (PREC != 0 && read_low)
-            return ag_low_to_f32<PREC>(ag_ld_gather_u16(c_in16 + u, pol_last));
-        return ag_ld_gather_f32(c_in32 + u, pol_last);
+            return ag_low_to_f32<PREC>((u < hot_n) ? hot16[u] : ag_ld_gather_u16(c_in16 + u, pol_last));
+        return (u < hot_n) ? hot32[u] : ag_ld_gather_f32(c_in32 + u, pol_last);
     }
 
-    /* the reference's per-vertex update for a finished row sum */
-    __device__ __forceinline__ void finish(uint32_t r, float s)
+    /* the reference's per-vertex update for a finished row sum; rp and od
+     * are the row's previous rank and out-degree, loaded ahead of time */
+    __device__ __forceinline__ void finish(uint32_t r, float s, float rp, uint32_t od)
     {
         if (MODE == AG_MODE_SPMV) {
             p.rank[r] = s;
             return;
         }
-        const float rp = p.rank[r];
         const float rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
         p.rank[r] = rn;
         const double err = (double)fabsf(__fsub_rn(rn, rp));
         my_err += err;
         my_active += (err >= eps) ? 1u : 0u;
-        const uint32_t od = p.outdeg[r];
         const float c = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
         if (PREC != 0 && write_low)
             ag_st_keep_u16(c_out16 + r, ag_f32_to_low<PREC>(c), pol_last);
@@ -245,161 +295,281 @@ struct AgPass
             ag_st_keep_f32(c_out32 + r, c, pol_last);
     }
 
-    /* phase 1: vals[j - eb] = gathered value of in-edge j, j in [eb, ee) */
-    __device__ __forceinline__ void stage(float *vals, uint32_t eb, uint32_t ee) const
+    /* two 16-byte groups of in-edges per lane: quads qa and qa + 32 (ids and,
+     * for a weighted SpMV, weights); quads at or past q1 read as zero */
+    struct Pair
+    {
+        uint4 a, b;
+        float4 wa, wb;
+    };
+
+    __device__ __forceinline__ Pair load_pair(uint32_t qa, uint32_t q1) const
     {
         const uint4 *ids4 = reinterpret_cast<const uint4 *>(p.ids);
         const float4 *w4 = reinterpret_cast<const float4 *>(p.w);
+        Pair r;
+        r.a = make_uint4(0, 0, 0, 0);
+        r.b = make_uint4(0, 0, 0, 0);
+        r.wa = make_float4(0.0001f, 0.0001f, 0.0001f, 0.0001f);
+        r.wb = r.wa;
+        const bool ha = qa < q1, hb = qa + 32 < q1;
+        if (ha)
+            r.a = ag_ld_stream_u4(ids4 + qa, pol_first);
+        if (hb)
+            r.b = ag_ld_stream_u4(ids4 + qa + 32, pol_first);
+        if (MODE == AG_MODE_SPMV && p.wmode == AG_SPMV_W_GRAPH) {
+            if (ha)
+                r.wa = ag_ld_stream_f4(w4 + qa, pol_first);
+            if (hb)
+                r.wb = ag_ld_stream_f4(w4 + qa + 32, pol_first);
+        }
+        return r;
+    }
+
+    /* first pair of a task's edge range, issued one task ahead */
+    __device__ __forceinline__ Pair prefetch(uint32_t eb, uint32_t ee, uint32_t lane) const
+    {
+        return load_pair((eb >> 2) + lane, (ee + 3u) >> 2);
+    }
+
+    /* the eight values of a pair (in-edge j valid when eb <= j < ee) */
+    __device__ __forceinline__ void gather8(const Pair &q, uint32_t qa, uint32_t eb, uint32_t ee, float *v,
+                                            bool *in) const
+    {
+        const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            in[k] = ja + k >= eb && ja + k < ee;
+            in[4 + k] = jb + k >= eb && jb + k < ee;
+        }
+        v[0] = in[0] ? gather(q.a.x, q.wa.x) : 0.f;
+        v[1] = in[1] ? gather(q.a.y, q.wa.y) : 0.f;
+        v[2] = in[2] ? gather(q.a.z, q.wa.z) : 0.f;
+        v[3] = in[3] ? gather(q.a.w, q.wa.w) : 0.f;
+        v[4] = in[4] ? gather(q.b.x, q.wb.x) : 0.f;
+        v[5] = in[5] ? gather(q.b.y, q.wb.y) : 0.f;
+        v[6] = in[6] ? gather(q.b.z, q.wb.z) : 0.f;
+        v[7] = in[7] ? gather(q.b.w, q.wb.w) : 0.f;
+    }
+
+    /* warp stage: vals[j - eb] = gathered value of in-edge j, j in [eb, ee).
+     * `first` holds the lane's first pair (loaded a task ahead); a lane
+     * gathers all eight values of a pair before it stores any of them. */
+    __device__ __forceinline__ void stage(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
+                                          const Pair &first) const
+    {
         const uint32_t q1 = (ee + 3u) >> 2;
-        for (uint32_t q = (eb >> 2) + threadIdx.x; q < q1; q += AG_BLK) {
-            const uint4 u = ag_ld_stream_u4(ids4 + q, pol_first);
-            float4 wv = make_float4(0.0001f, 0.0001f, 0.0001f, 0.0001f);
-            if (MODE == AG_MODE_SPMV && p.wmode == AG_SPMV_W_GRAPH)
-                wv = ag_ld_stream_f4(w4 + q, pol_first);
-            const uint32_t j0 = q << 2;
-            const bool in0 = j0 >= eb && j0 < ee;
-            const bool in1 = j0 + 1 >= eb && j0 + 1 < ee;
-            const bool in2 = j0 + 2 >= eb && j0 + 2 < ee;
-            const bool in3 = j0 + 3 < ee && j0 + 3 >= eb;
-            float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-            if (in0) v0 = gather(u.x, wv.x);
-            if (in1) v1 = gather(u.y, wv.y);
-            if (in2) v2 = gather(u.z, wv.z);
-            if (in3) v3 = gather(u.w, wv.w);
-            if (in0) vals[j0 - eb] = v0;
-            if (in1) vals[j0 + 1 - eb] = v1;
-            if (in2) vals[j0 + 2 - eb] = v2;
-            if (in3) vals[j0 + 3 - eb] = v3;
+        uint32_t qa = (eb >> 2) + lane;
+        Pair cur = first;
+        while (qa < q1) {
+            float v[8];
+            bool in[8];
+            gather8(cur, qa, eb, ee, v, in);
+            const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (in[k])
+                    vals[ja + k - eb] = v[k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (in[4 + k])
+                    vals[jb + k - eb] = v[4 + k];
+            qa += 64;
+            if (qa < q1)
+                cur = load_pair(qa, q1);
         }
     }
 
-    /* lane-strided partial sum of in-edges [eb, ee) straight from memory:
-     * each thread adds its own 4-edge groups in edge order */
-    __device__ __forceinline__ float strided_partial(uint32_t eb, uint32_t ee) const
+    /* warp-strided partial sum of in-edges [eb, ee) straight from memory;
+     * the next pair is in flight while the current one is gathered and
+     * added (fixed lane assignment, edge order within a lane) */
+    __device__ __forceinline__ float strided_partial(uint32_t eb, uint32_t ee, uint32_t lane,
+                                                     const Pair &first) const
     {
-        const uint4 *ids4 = reinterpret_cast<const uint4 *>(p.ids);
-        const float4 *w4 = reinterpret_cast<const float4 *>(p.w);
         const uint32_t q1 = (ee + 3u) >> 2;
+        uint32_t qa = (eb >> 2) + lane;
+        Pair cur = first;
         float s = 0.0f;
-        for (uint32_t q = (eb >> 2) + threadIdx.x; q < q1; q += AG_BLK) {
-            const uint4 u = ag_ld_stream_u4(ids4 + q, pol_first);
-            float4 wv = make_float4(0.0001f, 0.0001f, 0.0001f, 0.0001f);
-            if (MODE == AG_MODE_SPMV && p.wmode == AG_SPMV_W_GRAPH)
-                wv = ag_ld_stream_f4(w4 + q, pol_first);
-            const uint32_t j0 = q << 2;
-            const bool in0 = j0 >= eb && j0 < ee;
-            const bool in1 = j0 + 1 >= eb && j0 + 1 < ee;
-            const bool in2 = j0 + 2 >= eb && j0 + 2 < ee;
-            const bool in3 = j0 + 3 < ee && j0 + 3 >= eb;
-            float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-            if (in0) v0 = gather(u.x, wv.x);
-            if (in1) v1 = gather(u.y, wv.y);
-            if (in2) v2 = gather(u.z, wv.z);
-            if (in3) v3 = gather(u.w, wv.w);
-            if (in0) s = __fadd_rn(s, v0);
-            if (in1) s = __fadd_rn(s, v1);
-            if (in2) s = __fadd_rn(s, v2);
-            if (in3) s = __fadd_rn(s, v3);
+        while (qa < q1) {
+            const Pair nxt = load_pair(qa + 64, q1);
+            float v[8];
+            bool in[8];
+            gather8(cur, qa, eb, ee, v, in);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (in[k])
+                    s = __fadd_rn(s, v[k]);
+            cur = nxt;
+            qa += 64;
+        }
+        return s;
+    }
+
+    /* stream-order sum of in-edges [eb, ee) on one warp: stage AG_WCAP
+     * values at a time, lane 0 adds them one by one (EXACT order) */
+    __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane) const
+    {
+        float s = 0.0f;
+        for (uint32_t cb = eb; cb < ee; cb += AG_WCAP) {
+            const uint32_t ce = min(ee, cb + (uint32_t)AG_WCAP);
+            stage(vals, cb, ce, lane, prefetch(cb, ce, lane));
+            __syncwarp();
+            if (lane == 0) {
+                uint32_t j = 0;
+                if (cb == eb) {
+                    s = vals[0];
+                    j = 1;
+                }
+                for (; j < ce - cb; ++j)
+                    s = __fadd_rn(s, vals[j]);
+            }
+            __syncwarp();
         }
         return s;
     }
 };
 
-template <int MODE, int PREC, bool EXACT>
-__global__ void __launch_bounds__(AG_BLK) ag_pull_kernel(const AgPullParams p)
-{
-    __shared__ float vals[AG_CAP];
-    __shared__ uint16_t s_long[AG_LONG_MAX];
-    __shared__ uint32_t s_nlong;
-    __shared__ float s_redf[AG_NW];
-    __shared__ double s_redd[AG_NW];
-    __shared__ uint32_t s_redu[AG_NW];
-    __shared__ uint32_t s_last;
+extern __shared__ __align__(128) unsigned char ag_dsmem[];
 
+template <int MODE, int PREC, bool EXACT>
+__global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const AgPullParams p)
+{
+    __shared__ double s_redd[AG_WARPS];
+    __shared__ uint32_t s_redu[AG_WARPS];
+    __shared__ uint32_t s_last;
+    __shared__ __align__(8) uint64_t s_bar;
+
+    /* stream launches (profiling) run a fixed number of kernels: the ones
+     * after the loop has ended return at once */
+    if (MODE == AG_MODE_PR && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
+        return;
     AgPass<MODE, PREC, EXACT> ps(p);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float *vals = reinterpret_cast<float *>(ag_dsmem) + warp * AG_WCAP;
+    unsigned char *hot = ag_dsmem + AG_STAGE_BYTES;
+    const uint32_t nwarps = gridDim.x * AG_WARPS;
 
-    for (uint32_t t = blockIdx.x; t < p.ntasks; t += gridDim.x) {
-        const uint4 task = p.tasks[t];
-        const uint32_t kind = task.x & 3u;
-        if (kind == AG_T_BLOCK) {
-            const uint32_t rb = task.y, re = task.z;
-            const uint32_t eb = p.row_off[rb], ee = p.row_off[re];
-            if (!EXACT && tid == 0)
-                s_nlong = 0;
-            ps.stage(vals, eb, ee);
-            __syncthreads();
-            for (uint32_t i = tid; i < re - rb; i += AG_BLK) {
-                const uint32_t r = rb + i;
-                const uint32_t o0 = p.row_off[r] - eb, o1 = p.row_off[r + 1] - eb;
-                if (EXACT || o1 - o0 <= AG_TSEQ) {
-                    /* stream order: the accumulator restarts with the first
-                     * value and adds the rest one by one */
-                    float s = 0.0f;
-                    if (o1 > o0) {
-                        s = vals[o0];
-                        for (uint32_t j = o0 + 1; j < o1; ++j)
-                            s = __fadd_rn(s, vals[j]);
-                    }
-                    ps.finish(r, s);
-                } else {
-                    const uint32_t k = atomicAdd(&s_nlong, 1u);
-                    s_long[k] = (uint16_t)i;
+    /* hot table: the first hot_n values of the gathered vector, one TMA bulk
+     * copy per 32 KB, completing on an mbarrier that every thread waits on
+     * (bounded; a wait that runs out is reported through ctl->fault) */
+    if (p.hot_n) {
+        const uint32_t bytes = p.hot_n * ps.gather_elem_bytes();
+        if (tid == 0) {
+            ag_mbar_init(&s_bar, 1);
+            ag_mbar_expect_tx(&s_bar, bytes);
+            const unsigned char *src = reinterpret_cast<const unsigned char *>(ps.gather_source());
+            for (uint32_t off = 0; off < bytes; off += AG_BULK_CHUNK)
+                ag_bulk_g2s(hot + off, src + off, min(AG_BULK_CHUNK, bytes - off), &s_bar);
+        }
+        __syncthreads();
+        if (!ag_mbar_wait(&s_bar, 0, 1u << 20)) {
+            if (p.ctl)
+                atomicOr(&p.ctl->fault, 1u);
+            /* the copies may still be in flight: give them a long, bounded
+             * second chance before this CTA can exit */
+            ag_mbar_wait(&s_bar, 0, 1u << 24);
+        }
+        ps.hot32 = reinterpret_cast<const float *>(hot);
+        ps.hot16 = reinterpret_cast<const uint16_t *>(hot);
+        ps.hot_n = p.hot_n;
+    }
+
+    /* each warp walks its tasks with a stride of all warps; the first id
+     * pair of the next task is requested before the current task is
+     * gathered, reduced and written, so it is in flight meanwhile */
+    uint32_t t = blockIdx.x * AG_WARPS + warp;
+    uint4 task = t < p.ntasks ? p.tasks[t] : make_uint4(0, 0, 0, 0);
+    typename AgPass<MODE, PREC, EXACT>::Pair pf = ps.prefetch(task.z, task.w, lane);
+    while (t < p.ntasks) {
+        const uint32_t tn = t + nwarps;
+        const uint4 task_n = tn < p.ntasks ? p.tasks[tn] : make_uint4(0, 0, 0, 0);
+        const uint32_t kind = task.x >> 30;
+        const uint32_t r0 = task.x & AG_ROW_MASK;
+        const uint32_t eb = task.z, ee = task.w;
+        if (kind == AG_T_ROWS) {
+            /* one row per lane; its bounds, previous rank and out-degree are
+             * loaded first so that they arrive while the stage runs */
+            const uint32_t r = r0 + lane;
+            const bool live = r < task.y;
+            uint32_t o0 = ee, o1 = ee, od = 0;
+            float rp = 0.0f;
+            if (live) {
+                o0 = p.row_off[r];
+                o1 = p.row_off[r + 1];
+                if (MODE == AG_MODE_PR) {
+                    rp = p.rank[r];
+                    od = p.outdeg[r];
                 }
+            }
+            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            ps.stage(vals, eb, ee, lane, pf);
+            __syncwarp();
+            o0 -= eb;
+            o1 -= eb;
+            float s = 0.0f;
+            bool is_long = false;
+            if (EXACT || o1 - o0 <= AG_TSEQ) {
+                /* stream order: the accumulator restarts with the first value
+                 * and adds the rest one by one */
+                if (o1 > o0) {
+                    s = vals[o0];
+                    for (uint32_t j = o0 + 1; j < o1; ++j)
+                        s = __fadd_rn(s, vals[j]);
+                }
+            } else {
+                is_long = true;
             }
             if (!EXACT) {
-                __syncthreads();
-                const uint32_t nl = s_nlong;
-                for (uint32_t k = warp; k < nl; k += AG_NW) {
-                    const uint32_t r = rb + s_long[k];
-                    const uint32_t o0 = p.row_off[r] - eb, o1 = p.row_off[r + 1] - eb;
-                    float s = 0.0f;
-                    for (uint32_t j = o0 + lane; j < o1; j += 32)
-                        s = __fadd_rn(s, vals[j]);
-                    s = ag_warp_sum_f(s);
-                    if (lane == 0)
-                        ps.finish(r, s);
+                /* rows of AG_TSEQ+1 .. AG_WCAP in-edges: the whole warp sums
+                 * each one (lane-strided partials, xor tree) */
+                unsigned m = __ballot_sync(0xffffffffu, is_long);
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t a = __shfl_sync(0xffffffffu, o0, src);
+                    const uint32_t b = __shfl_sync(0xffffffffu, o1, src);
+                    float tsum = 0.0f;
+                    for (uint32_t j = a + lane; j < b; j += 32)
+                        tsum = __fadd_rn(tsum, vals[j]);
+                    tsum = ag_warp_sum_f(tsum);
+                    if ((int)lane == src)
+                        s = tsum;
                 }
             }
-            __syncthreads();
-        } else if (kind == AG_T_ROW) {
-            const uint32_t r = task.y;
-            const uint32_t eb = p.row_off[r], ee = p.row_off[r + 1];
+            if (live)
+                ps.finish(r, s, rp, od);
+            __syncwarp();
+            pf = pn;
+        } else if (kind == AG_T_LONG) {
+            float rp = 0.0f;
+            uint32_t od = 0;
+            if (MODE == AG_MODE_PR && lane == 0) {
+                rp = p.rank[r0];
+                od = p.outdeg[r0];
+            }
+            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            float s;
             if (EXACT) {
-                float s = 0.0f;
-                for (uint32_t cb = eb; cb < ee; cb += AG_CAP) {
-                    const uint32_t ce = min(ee, cb + (uint32_t)AG_CAP);
-                    ps.stage(vals, cb, ce);
-                    __syncthreads();
-                    if (tid == 0) {
-                        uint32_t j = 0;
-                        if (cb == eb) {
-                            s = vals[0];
-                            j = 1;
-                        }
-                        for (; j < ce - cb; ++j)
-                            s = __fadd_rn(s, vals[j]);
-                    }
-                    __syncthreads();
-                }
-                if (tid == 0)
-                    ps.finish(r, s);
+                s = ps.ordered_sum(vals, eb, ee, lane);
             } else {
-                float s = ps.strided_partial(eb, ee);
-                s = ag_block_sum_f(s, s_redf);
-                if (tid == 0)
-                    ps.finish(r, s);
+                s = ps.strided_partial(eb, ee, lane, pf);
+                s = ag_warp_sum_f(s);
             }
-            __syncthreads();
+            if (lane == 0)
+                ps.finish(r0, s, rp, od);
+            __syncwarp();
+            pf = pn;
         } else {
             /* hub chunk (FAST order only) */
-            const uint32_t chunk = task.x >> 2, r = task.y, pbase = task.z, nch = task.w;
-            const uint32_t rb0 = p.row_off[r], re0 = p.row_off[r + 1];
-            const uint32_t cb = rb0 + chunk * (uint32_t)AG_HUB;
-            const uint32_t ce = min(re0, cb + (uint32_t)AG_HUB);
-            float s = ps.strided_partial(cb, ce);
-            s = ag_block_sum_f(s, s_redf);
-            if (tid == 0) {
+            const uint32_t pbase = task.y & AG_SLOT_MASK, chunk = task.y >> AG_SLOT_BITS;
+            uint32_t deg = 0;
+            if (lane == 0)
+                deg = p.row_off[r0 + 1] - p.row_off[r0];
+            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            float s = ps.strided_partial(eb, ee, lane, pf);
+            s = ag_warp_sum_f(s);
+            if (lane == 0) {
+                const uint32_t nch = (deg + AG_WHUB - 1) / AG_WHUB;
                 p.hub_part[pbase + chunk] = s;
                 __threadfence();
                 const uint32_t prev = atomicAdd(&p.hub_cnt[pbase], 1u);
@@ -409,11 +579,20 @@ __global__ void __launch_bounds__(AG_BLK) ag_pull_kernel(const AgPullParams p)
                     for (uint32_t c = 1; c < nch; ++c)
                         tot = __fadd_rn(tot, __ldcg(p.hub_part + pbase + c));
                     p.hub_cnt[pbase] = 0;
-                    ps.finish(r, tot);
+                    float rp = 0.0f;
+                    uint32_t od = 0;
+                    if (MODE == AG_MODE_PR) {
+                        rp = p.rank[r0];
+                        od = p.outdeg[r0];
+                    }
+                    ps.finish(r0, tot, rp, od);
                 }
             }
-            __syncthreads();
+            __syncwarp();
+            pf = pn;
         }
+        task = task_n;
+        t = tn;
     }
 
     if (MODE != AG_MODE_PR)
@@ -432,7 +611,7 @@ __global__ void __launch_bounds__(AG_BLK) ag_pull_kernel(const AgPullParams p)
         if (tid == 0) {
             double be = 0.0;
             uint32_t ba = 0;
-            for (int w = 0; w < AG_NW; ++w) {
+            for (int w = 0; w < AG_WARPS; ++w) {
                 be += s_redd[w];
                 ba += s_redu[w];
             }
@@ -483,18 +662,21 @@ __global__ void __launch_bounds__(AG_BLK) ag_pull_kernel(const AgPullParams p)
         c->active_acc = 0;
         c->err_acc = 0.0;
         c->done_ctas = 0;
+        c->stop = cont ? 0u : 1u;
         __threadfence();
-        cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
+        if (p.use_cond)
+            cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
     }
 }
 
 /* init: r = base (or the warm start), first contributions, control reset */
 template <int PREC>
-__global__ void __launch_bounds__(AG_BLK) ag_pr_init_kernel2(const AgPullParams p, const AgRunConfig run)
+__global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams p, const AgRunConfig run)
 {
     const uint64_t pol_last = ag_policy_evict_last();
-    for (uint32_t v = blockIdx.x * AG_BLK + threadIdx.x; v < p.N; v += gridDim.x * AG_BLK) {
-        const float r0 = run.use_init ? p.init_ranks[v] : p.base;
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        /* device row v is caller vertex perm[v]; the warm start is in caller order */
+        const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
         p.rank[v] = r0;
         const uint32_t od = p.outdeg[v];
         const float c = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
@@ -521,19 +703,21 @@ __global__ void __launch_bounds__(AG_BLK) ag_pr_init_kernel2(const AgPullParams 
         c->use_init = run.use_init;
         c->low_passes = 0;
         c->t0 = ag_globaltimer();
-        cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
+        c->stop = (run.max_iter > 0 && p.N > 0) ? 0u : 1u;
+        if (p.use_cond)
+            cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
     }
 }
 
-/* ranks / N in binary32 (pageRank.c:1079-1085), FP64 sum */
-__global__ void __launch_bounds__(AG_BLK) ag_normalize_kernel(const AgPullParams p)
+/* ranks / N in binary32 (pageRank.c:1079-1085), back in caller order, FP64 sum */
+__global__ void __launch_bounds__(AG_SBLK) ag_normalize_kernel(const AgPullParams p)
 {
-    __shared__ double sh[AG_NW];
+    __shared__ double sh[AG_SNW];
     const float fN = __uint2float_rn(p.N);
     double s = 0.0;
-    for (uint32_t v = blockIdx.x * AG_BLK + threadIdx.x; v < p.N; v += gridDim.x * AG_BLK) {
-        const float r = __fdiv_rn(p.rank[v], fN);
-        p.rank[v] = r;
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        const float r = __fdiv_rn(p.rank[p.inv ? p.inv[v] : v], fN);
+        p.out[v] = r;
         s += (double)r;
     }
     s = ag_warp_sum_d(s);
@@ -542,7 +726,7 @@ __global__ void __launch_bounds__(AG_BLK) ag_normalize_kernel(const AgPullParams
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int w = 0; w < AG_NW; ++w)
+        for (int w = 0; w < AG_SNW; ++w)
             t += sh[w];
         atomicAdd(&p.ctl->rank_sum, t);
     }

@@ -43,7 +43,7 @@ static AgContext g_ctx = {0, -1, 0, nullptr};
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
         if (e_ != cudaSuccess)                                                                 \
-            return ag_set_error(AG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+            return cudaGetLastError(), ag_set_error(AG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
                                 __FILE__, __LINE__);                                           \
     } while (0)
 
@@ -185,6 +185,10 @@ struct ag_graph_s
     uint32_t N, E, E4;
     uint32_t *row_off, *ids, *outdeg;
     float *w;
+    uint32_t *perm, *inv;   /* relabelling (NULL with AG_UPLOAD_KEEP_ORDER)  */
+    float *out;             /* normalised ranks, caller order                */
+    float *xbuf, *ybuf;     /* SpMV vectors in device order                  */
+    uint32_t hot_n;         /* entries of the shared-memory hot table        */
     uint4 *tasks_fast, *tasks_exact;
     uint32_t ntasks_fast, ntasks_exact;
     uint32_t nparts;
@@ -250,6 +254,11 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
                 free_exec(&g->exe[a][b]);
     dev_free(g->row_off);
     dev_free(g->ids);
+    dev_free(g->perm);
+    dev_free(g->inv);
+    dev_free(g->out);
+    dev_free(g->xbuf);
+    dev_free(g->ybuf);
     dev_free(g->outdeg);
     dev_free(g->w);
     dev_free(g->tasks_fast);
@@ -274,48 +283,57 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     return AG_OK;
 }
 
-/* Work list of the fused pull kernel.  FAST order: rows longer than AG_CAP
- * run on their own CTA, rows longer than AG_HUB are split into AG_HUB-edge
- * chunks; EXACT order keeps every long row on one CTA.  Everything else is
- * packed into row blocks of <= AG_CAP in-edges and <= AG_RMAX rows.  Heavy
- * items come first so that they start early. */
-static void plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out, uint32_t *nparts,
-                       uint32_t *nhub)
+/* Work list of the fused pull kernel (one item per warp).  FAST order:
+ * rows longer than AG_WCAP run on their own warp, rows longer than AG_WHUB
+ * are split into AG_WHUB-edge chunks; EXACT order keeps every long row on one
+ * warp.  Everything else is packed into items of <= AG_WROWS consecutive rows
+ * holding <= AG_WCAP in-edges.  Heavy items come first so that they start
+ * early. */
+static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out,
+                              uint32_t *nparts, uint32_t *nhub)
 {
-    std::vector<uint4> hubs, rows, blocks;
+    std::vector<uint4> hubs, longs, rows;
     uint32_t pbase = 0, nh = 0;
     uint32_t r = 0;
+    if (N > AG_ROW_MASK)
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "%u vertices exceed the 2^30 row limit", N);
     while (r < N) {
         const uint32_t d = off[r + 1] - off[r];
-        if (d > AG_CAP) {
-            if (!exact && d > AG_HUB) {
-                const uint32_t nch = (d + AG_HUB - 1) / AG_HUB;
-                for (uint32_t c = 0; c < nch; ++c)
-                    hubs.push_back(make_uint4(AG_T_HUB | (c << 2), r, pbase, nch));
+        if (d > AG_WCAP) {
+            if (!exact && d > AG_WHUB) {
+                const uint32_t nch = (d + AG_WHUB - 1) / AG_WHUB;
+                if (nch >= (1u << (32 - AG_SLOT_BITS)) || pbase + nch > AG_SLOT_MASK)
+                    return ag_set_error(AG_ERR_UNSUPPORTED, "row %u: %u in-edges exceed the hub split limits", r, d);
+                for (uint32_t c = 0; c < nch; ++c) {
+                    const uint32_t cb = off[r] + c * AG_WHUB;
+                    const uint32_t ce = std::min(off[r + 1], cb + (uint32_t)AG_WHUB);
+                    hubs.push_back(make_uint4((AG_T_HUB << 30) | r, pbase | (c << AG_SLOT_BITS), cb, ce));
+                }
                 pbase += nch;
                 ++nh;
             } else {
-                rows.push_back(make_uint4(AG_T_ROW, r, 0, 0));
+                longs.push_back(make_uint4((AG_T_LONG << 30) | r, r + 1, off[r], off[r + 1]));
             }
             ++r;
             continue;
         }
         const uint32_t rb = r, eb = off[r];
-        while (r < N && r - rb < AG_RMAX) {
+        while (r < N && r - rb < AG_WROWS) {
             const uint32_t dr = off[r + 1] - off[r];
-            if (dr > AG_CAP || off[r + 1] - eb > AG_CAP)
+            if (dr > AG_WCAP || off[r + 1] - eb > AG_WCAP)
                 break;
             ++r;
         }
-        blocks.push_back(make_uint4(AG_T_BLOCK, rb, r, 0));
+        rows.push_back(make_uint4((AG_T_ROWS << 30) | rb, r, eb, off[r]));
     }
     out.clear();
-    out.reserve(hubs.size() + rows.size() + blocks.size());
+    out.reserve(hubs.size() + longs.size() + rows.size());
     out.insert(out.end(), hubs.begin(), hubs.end());
+    out.insert(out.end(), longs.begin(), longs.end());
     out.insert(out.end(), rows.begin(), rows.end());
-    out.insert(out.end(), blocks.begin(), blocks.end());
     *nparts = pbase;
     *nhub = nh;
+    return AG_OK;
 }
 
 extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out)
@@ -369,31 +387,40 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
     g->E4 = ((E + 3u) & ~3u) + 4u;
     g->max_in_degree = maxd;
 
-    std::vector<uint4> tf, te;
-    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
-    plan_tasks(off.data(), N, false, tf, &nparts, &nhub);
-    plan_tasks(off.data(), N, true, te, &np2, &nh2);
-    g->ntasks_fast = (uint32_t)tf.size();
-    g->ntasks_exact = (uint32_t)te.size();
-    g->nparts = nparts;
-    g->num_hub_rows = nhub;
-
     cudaStream_t s = g_ctx.stream;
-    g->row_off = (uint32_t *)dev_alloc(g, (size_t)(N + 1) * 4, &st);
-    g->ids = (uint32_t *)dev_alloc(g, (size_t)g->E4 * 4, &st);
-    g->outdeg = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
-    if (want_w)
-        g->w = (float *)dev_alloc(g, (size_t)g->E4 * 4, &st);
-    g->tasks_fast = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
-    g->tasks_exact = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
+    const bool relabel = !(flags & AG_UPLOAD_KEEP_ORDER) && N > 0;
+    /* the caller's layout first ("old"); relabelled copies replace it */
+    uint32_t *off_old = (uint32_t *)dev_alloc(g, (size_t)(N + 1) * 4, &st);
+    uint32_t *ids_old = (uint32_t *)dev_alloc(g, (size_t)g->E4 * 4, &st);
+    uint32_t *outdeg_old = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    float *w_old = want_w ? (float *)dev_alloc(g, (size_t)g->E4 * 4, &st) : nullptr;
     g->rank = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+    g->out = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
     g->c32[0] = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
     g->c32[1] = (float *)dev_alloc(g, (size_t)N * 4 + 16, &st);
-    g->hub_part = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
-    g->hub_cnt = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
     g->ctl = (AgControl *)dev_alloc(g, sizeof(AgControl), &st);
     g->flag = (uint32_t *)dev_alloc(g, 16, &st);
+    if (relabel) {
+        g->perm = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+        g->inv = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+        g->row_off = (uint32_t *)dev_alloc(g, (size_t)(N + 1) * 4, &st);
+        g->ids = (uint32_t *)dev_alloc(g, (size_t)g->E4 * 4, &st);
+        g->outdeg = (uint32_t *)dev_alloc(g, (size_t)N * 4 + 16, &st);
+        if (want_w)
+            g->w = (float *)dev_alloc(g, (size_t)g->E4 * 4, &st);
+    } else {
+        g->row_off = off_old;
+        g->ids = ids_old;
+        g->outdeg = outdeg_old;
+        g->w = w_old;
+    }
     if (st != AG_OK) {
+        if (relabel) {
+            dev_free(off_old);
+            dev_free(ids_old);
+            dev_free(outdeg_old);
+            dev_free(w_old);
+        }
         ag_graph_release(g);
         return st;
     }
@@ -401,18 +428,25 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
     do {                                                                                         \
         cudaError_t e_ = (call);                                                                 \
         if (e_ != cudaSuccess) {                                                                 \
+            cudaGetLastError();                                                                  \
             st = ag_set_error(AG_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+            if (relabel) {                                                                       \
+                dev_free(off_old);                                                               \
+                dev_free(ids_old);                                                               \
+                dev_free(outdeg_old);                                                            \
+                dev_free(w_old);                                                                 \
+            }                                                                                    \
             ag_graph_release(g);                                                                 \
             return st;                                                                           \
         }                                                                                        \
     } while (0)
-    UP(cudaMemcpyAsync(g->row_off, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
-    UP(cudaMemsetAsync(g->ids + (g->E4 - 8), 0, 32, s));
+    UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
+    UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
     if (contiguous) {
         if (E)
-            UP(cudaMemcpyAsync(g->ids, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
         if (want_w && E)
-            UP(cudaMemcpyAsync(g->w, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
     } else {
         std::vector<uint32_t> packed(E);
         std::vector<float> packw(want_w ? E : 0);
@@ -423,38 +457,81 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
                 memcpy(packw.data() + off[v], iel->edges_array_weight + b, (size_t)d * 4);
         }
         if (E)
-            UP(cudaMemcpyAsync(g->ids, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            UP(cudaMemcpyAsync(ids_old, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
         if (want_w && E)
-            UP(cudaMemcpyAsync(g->w, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            UP(cudaMemcpyAsync(w_old, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
         UP(cudaStreamSynchronize(s)); /* the packed copies are stack-owned */
     }
     if (want_w)
-        UP(cudaMemsetAsync(g->w + (g->E4 - 8), 0, 32, s));
+        UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, s));
     if (N)
-        UP(cudaMemcpyAsync(g->outdeg, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        UP(cudaMemcpyAsync(outdeg_old, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+    UP(cudaMemsetAsync(g->ctl, 0, sizeof(AgControl), s));
+    UP(cudaMemsetAsync(g->flag, 0, 4, s));
+    UP(cudaMemsetAsync(g->flag + 1, 0xFF, 4, s));
+    /* every in-edge must name a vertex < N before anything reads through it */
+    if (!(flags & AG_UPLOAD_TRUSTED)) {
+        uint32_t hflag[2] = {0, 0};
+        UP(ag_validate_ids(ids_old, E, N, g->flag, s));
+        UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
+        UP(cudaStreamSynchronize(s));
+        if (hflag[0]) {
+            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1], N);
+            if (relabel) {
+                dev_free(off_old);
+                dev_free(ids_old);
+                dev_free(outdeg_old);
+                dev_free(w_old);
+            }
+            ag_graph_release(g);
+            return st;
+        }
+    }
+    if (relabel) {
+        UP(cudaMemsetAsync(g->ids + E, 0, (size_t)(g->E4 - E) * 4, s));
+        if (want_w)
+            UP(cudaMemsetAsync(g->w + E, 0, (size_t)(g->E4 - E) * 4, s));
+        UP(ag_relabel_by_out_degree(off_old, ids_old, w_old, outdeg_old, N, E, g->perm, g->inv, g->row_off, g->ids,
+                                    g->w, g->outdeg, s));
+        /* the planner walks the device row offsets */
+        UP(cudaMemcpyAsync(off.data(), g->row_off, (size_t)(N + 1) * 4, cudaMemcpyDeviceToHost, s));
+        UP(cudaStreamSynchronize(s));
+        dev_free(off_old);
+        dev_free(ids_old);
+        dev_free(outdeg_old);
+        dev_free(w_old);
+        g->device_bytes -= (uint64_t)(N + 1) * 4 + (uint64_t)g->E4 * 4 * (want_w ? 2 : 1) + (uint64_t)N * 4 + 16;
+        off_old = ids_old = outdeg_old = nullptr;
+        w_old = nullptr;
+    }
+    g->hot_n = (flags & AG_UPLOAD_NO_SMEM_CACHE) ? 0u : std::min<uint32_t>(N & ~63u, AG_HOT_MAX);
+
+    std::vector<uint4> tf, te;
+    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
+    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub);
+    if (st == AG_OK)
+        st = plan_tasks(off.data(), N, true, te, &np2, &nh2);
+    if (st != AG_OK) {
+        ag_graph_release(g);
+        return st;
+    }
+    g->ntasks_fast = (uint32_t)tf.size();
+    g->ntasks_exact = (uint32_t)te.size();
+    g->nparts = nparts;
+    g->num_hub_rows = nhub;
+    g->tasks_fast = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
+    g->tasks_exact = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
+    g->hub_part = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    g->hub_cnt = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    if (st != AG_OK) {
+        ag_graph_release(g);
+        return st;
+    }
     if (!tf.empty())
         UP(cudaMemcpyAsync(g->tasks_fast, tf.data(), tf.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
     if (!te.empty())
         UP(cudaMemcpyAsync(g->tasks_exact, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
     UP(cudaMemsetAsync(g->hub_cnt, 0, (size_t)nparts * 4 + 16, s));
-    UP(cudaMemsetAsync(g->ctl, 0, sizeof(AgControl), s));
-    UP(cudaMemsetAsync(g->flag, 0, 4, s));
-    UP(cudaMemsetAsync(g->flag + 1, 0xFF, 4, s));
-    if (!(flags & AG_UPLOAD_TRUSTED)) {
-        uint32_t hflag[2] = {0, 0};
-        UP(ag_validate_ids(g->ids, E, N, g->flag, s));
-        UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
-        st = stream_wait(s, 0);
-        if (st != AG_OK) {
-            ag_graph_release(g);
-            return st;
-        }
-        if (hflag[0]) {
-            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1], N);
-            ag_graph_release(g);
-            return st;
-        }
-    }
     UP(cudaEventCreate(&g->ev0));
     UP(cudaEventCreate(&g->ev1));
     /* the host-side vectors die at return: wait for the copies */
@@ -468,6 +545,9 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
     return AG_OK;
 }
 
+static size_t pull_smem(const ag_graph_s *g);
+static ag_status_t pull_kernel_prepare(const void *kern);
+
 extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
 {
     if (!g || !info)
@@ -480,22 +560,38 @@ extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
     info->max_in_degree = g->max_in_degree;
     info->device_bytes = g->device_bytes;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ag_pull_kernel_ptr(AG_MODE_PR, 0, 0), AG_BLK, 0) ==
-        cudaSuccess)
-        info->grid = (uint32_t)std::min<uint64_t>((uint64_t)nb * g_ctx.num_sms, std::max<uint32_t>(1, g->ntasks_fast));
+    if (pull_kernel_prepare(ag_pull_kernel_ptr(AG_MODE_PR, 0, 0)) == AG_OK &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ag_pull_kernel_ptr(AG_MODE_PR, 0, 0), AG_BLK,
+                                                      pull_smem(g)) == cudaSuccess)
+        info->grid = (uint32_t)std::min<uint64_t>((uint64_t)nb * g_ctx.num_sms,
+                                                  std::max<uint64_t>(1, ((uint64_t)g->ntasks_fast + AG_WARPS - 1) / AG_WARPS));
     return AG_OK;
 }
 
 /* persistent grid: every SM filled to its occupancy, never more CTAs than
  * work items */
-static unsigned pull_grid(const void *kern, uint32_t ntasks)
+static size_t pull_smem(const ag_graph_s *g) { return (size_t)AG_STAGE_BYTES + (size_t)g->hot_n * 4; }
+
+/* the pull kernels take up to AG_SMEM_MAX bytes of shared memory */
+static ag_status_t pull_kernel_prepare(const void *kern)
+{
+    AG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 AG_SMEM_MAX - AG_SMEM_STATIC));
+    return AG_OK;
+}
+
+static unsigned pull_grid(const void *kern, uint32_t ntasks, size_t smem)
 {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, AG_BLK, 0) != cudaSuccess || nb < 1)
+    if (pull_kernel_prepare(kern) != AG_OK ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, AG_BLK, smem) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
         nb = 1;
+    }
     uint64_t g = (uint64_t)nb * (uint64_t)g_ctx.num_sms;
-    if (g > ntasks)
-        g = ntasks;
+    const uint64_t need = ((uint64_t)ntasks + AG_WARPS - 1) / AG_WARPS;
+    if (g > need)
+        g = need;
     if (g < 1)
         g = 1;
     return (unsigned)g;
@@ -531,6 +627,10 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.hub_cnt = g->hub_cnt;
     p.ctl = g->ctl;
     p.init_ranks = g->init_buf;
+    p.perm = g->perm;
+    p.inv = g->inv;
+    p.out = g->out;
+    p.hot_n = g->hot_n;
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
@@ -544,17 +644,18 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
     AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
+    x->params.use_cond = 1;
     const void *kpull = ag_pull_kernel_ptr(AG_MODE_PR, prec, exact);
-    x->grid = pull_grid(kpull, x->params.ntasks);
+    x->grid = pull_grid(kpull, x->params.ntasks, pull_smem(g));
 
     AgRunConfig run;
     memset(&run, 0, sizeof(run));
     void *init_args[2] = {&x->params, &run};
     cudaKernelNodeParams kp = {};
     kp.func = (void *)ag_init_kernel_ptr(prec);
-    kp.gridDim = dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)g->N + AG_BLK - 1) / AG_BLK,
+    kp.gridDim = dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK,
                                                                           (uint64_t)g_ctx.num_sms * 8)));
-    kp.blockDim = dim3(AG_BLK);
+    kp.blockDim = dim3(AG_SBLK);
     kp.kernelParams = init_args;
     AG_CUDA(cudaGraphAddKernelNode(&x->init_node, x->graph, nullptr, 0, &kp));
 
@@ -572,6 +673,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
     kb.func = (void *)kpull;
     kb.gridDim = dim3(x->grid);
     kb.blockDim = dim3(AG_BLK);
+    kb.sharedMemBytes = (unsigned)pull_smem(g);
     kb.kernelParams = pull_args;
     cudaGraphNode_t pnode;
     AG_CUDA(cudaGraphAddKernelNode(&pnode, body, nullptr, 0, &kb));
@@ -580,7 +682,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
     cudaKernelNodeParams kn = {};
     kn.func = (void *)ag_normalize_kernel_ptr();
     kn.gridDim = kp.gridDim;
-    kn.blockDim = dim3(AG_BLK);
+    kn.blockDim = dim3(AG_SBLK);
     kn.kernelParams = norm_args;
     cudaGraphNode_t nnode;
     AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
@@ -650,7 +752,24 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
     kp.kernelParams = init_args;
     AG_CUDA(cudaGraphExecKernelNodeSetParams(x->exec, x->init_node, &kp));
     AG_CUDA(cudaEventRecord(g->ev0, s));
-    AG_CUDA(cudaGraphLaunch(x->exec, s));
+    const char *mode = getenv("AG_LAUNCH_MODE");
+    if (mode && strcmp(mode, "stream") == 0) {
+        /* profiling form: the same kernels as separate launches (a profiler
+         * sees every pass); passes after convergence return at once */
+        AgPullParams sp = x->params;
+        sp.use_cond = 0;
+        cudaKernelNodeParams ki;
+        AG_CUDA(cudaGraphKernelNodeGetParams(x->init_node, &ki));
+        void *ia[2] = {&sp, &run};
+        AG_CUDA(cudaLaunchKernel(ki.func, ki.gridDim, ki.blockDim, ia, 0, s));
+        void *pa[1] = {&sp};
+        const void *kpull = ag_pull_kernel_ptr(AG_MODE_PR, prec, exact);
+        for (uint32_t i = 0; i < run.max_iter; ++i)
+            AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, pull_smem(g), s));
+        AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
+    } else {
+        AG_CUDA(cudaGraphLaunch(x->exec, s));
+    }
     AG_CUDA(cudaEventRecord(g->ev1, s));
     g->launched = 1;
     g->last_prec = prec;
@@ -678,7 +797,7 @@ extern "C" ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_resul
         return ag_set_error(AG_ERR_CUDA, "control readback failed: %s", cudaGetErrorString(e));
     }
     if (ranks && g->N) {
-        e = cudaMemcpy(ranks, g->rank, (size_t)g->N * 4, cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(ranks, g->out, (size_t)g->N * 4, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) {
             free(hc);
             return ag_set_error(AG_ERR_CUDA, "rank readback failed: %s", cudaGetErrorString(e));
@@ -713,7 +832,7 @@ extern "C" ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_resul
     return AG_OK;
 }
 
-extern "C" const float *ag_pagerank_device_ranks(ag_graph_t g) { return g ? g->rank : nullptr; }
+extern "C" const float *ag_pagerank_device_ranks(ag_graph_t g) { return g ? g->out : nullptr; }
 
 /* ------------------------------------------------------------------ SpMV */
 extern "C" ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *y, uint32_t mode)
@@ -723,15 +842,32 @@ extern "C" ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_device: NULL argument");
     if (g->N == 0)
         return AG_OK;
-    const int exact = (mode & 2u) ? 1 : 0;
+    cudaStream_t s = g_ctx.stream;
+    ag_status_t st = AG_OK;
+    if (g->perm && !g->xbuf) {
+        g->xbuf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        g->ybuf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        if (st != AG_OK)
+            return st;
+    }
+    const int exact = (mode & AG_SPMV_EXACT) ? 1 : 0;
     AgPullParams p = base_params(g, exact);
-    p.x = x;
-    p.rank = y;
+    /* caller order in and out; the product runs in device order */
+    if (g->perm)
+        AG_CUDA(ag_permute_in(g->perm, x, g->xbuf, g->N, s));
+    p.x = g->perm ? g->xbuf : x;
+    p.rank = g->perm ? g->ybuf : y;
+    /* the hot table needs a 16-byte aligned vector */
+    if (((uintptr_t)p.x & 15u) != 0)
+        p.hot_n = 0;
     p.wmode = (mode & AG_SPMV_UNIT) ? AG_SPMV_W_UNIT : (g->w ? AG_SPMV_W_GRAPH : AG_SPMV_W_CONST);
     const void *k = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, exact);
-    const unsigned grid = pull_grid(k, p.ntasks);
+    const size_t smem = (size_t)AG_STAGE_BYTES + (size_t)p.hot_n * 4;
+    const unsigned grid = pull_grid(k, p.ntasks, smem);
     void *args[1] = {&p};
-    AG_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, 0, g_ctx.stream));
+    AG_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, smem, s));
+    if (g->perm)
+        AG_CUDA(ag_permute_out(g->inv, g->ybuf, y, g->N, s));
     return AG_OK;
 }
 
@@ -787,6 +923,13 @@ extern "C" ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, do
         return ag_set_error(AG_ERR_CUDA, "FP64 oracle failed: %s", cudaGetErrorString(e));
     if (w != AG_OK)
         return w;
+    if (g->inv) {
+        std::vector<uint32_t> inv(g->N);
+        std::vector<double> dev_order(ranks, ranks + g->N);
+        AG_CUDA(cudaMemcpy(inv.data(), g->inv, (size_t)g->N * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t v = 0; v < g->N; ++v)
+            ranks[v] = dev_order[inv[v]];
+    }
     for (uint32_t v = 0; v < g->N; ++v)
         ranks[v] /= (double)g->N;
     if (passes)

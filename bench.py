@@ -62,6 +62,21 @@ def dist_env():
     return rank, world, local
 
 
+def reduce_time_work(seconds_or_ms: float, work: float, device=None):
+    """Max of the timed region and sum of the work over all ranks (the
+    whole-job rate is sum(work) / max(time)).  Identity without a process
+    group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(seconds_or_ms), float(work)
+    t = torch.tensor([float(seconds_or_ms)], dtype=torch.float64, device=device)
+    w = torch.tensor([float(work)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(w.item())
+
+
 def workload_config(a, world):
     return {
         "workload": f"PageRank pull FP32, RMAT scale {a.scale} edge factor {a.edge_factor} "
@@ -235,13 +250,7 @@ def run_b200(a):
     ranks, res, hist = dg.fetch(history=a.iterations)
     passes = int(res.passes)
     edges_all = E * passes * a.steps
-    t_max = ms
-    if world > 1:
-        tt = torch.tensor([ms, float(edges_all)], device="cuda")
-        mx = tt.clone()
-        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(tt[1:], op=torch.distributed.ReduceOp.SUM)
-        t_max, edges_all = float(mx[0]), float(tt[1])
+    t_max, edges_all = reduce_time_work(ms, edges_all, device="cuda")
     value = edges_all / (t_max * 1e-3) / 1e9
 
     # -------- roofline of the pull pass
@@ -281,13 +290,7 @@ def run_b200(a):
         ag.lib.freePageRankStats(out)
     torch.cuda.synchronize()
     e2e_t = time.perf_counter() - t0
-    e2e_edges = float(E * e2e_passes)
-    if world > 1:
-        tt = torch.tensor([e2e_t, e2e_edges], device="cuda")
-        mx = tt.clone()
-        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(tt[1:], op=torch.distributed.ReduceOp.SUM)
-        e2e_t, e2e_edges = float(mx[0]), float(tt[1])
+    e2e_t, e2e_edges = reduce_time_work(e2e_t, float(E * e2e_passes), device="cuda")
     e4 = ((E + 3) & ~3) + 4
     h2d = 4 * e4 + 4 * (N + 1) + 4 * N + 16 * info.num_tasks
     d2h = 4 * N

@@ -106,6 +106,13 @@ typedef struct ag_graph_s *ag_graph_t;
                                   makes the upload fail with
                                   AG_ERR_INVALID_GRAPH before any kernel
                                   reads through it                          */
+#define AG_UPLOAD_KEEP_ORDER 8u  /* keep the caller's vertex order on the
+                                    device (default: relabel by descending
+                                    out-degree so the most-gathered
+                                    contributions are contiguous)           */
+#define AG_UPLOAD_NO_SMEM_CACHE 16u /* serve every gather from global memory
+                                    (default: the most-gathered values are
+                                    copied into shared memory each pass)    */
 
 typedef struct ag_graph_info
 {
