@@ -50,10 +50,16 @@
 #endif
 #define AG_SMEM_STATIC 1024 /* static shared memory of the pull kernel (upper bound) */
 #ifndef AG_HOT_CAP
-#define AG_HOT_CAP (1u << 30)
+#define AG_HOT_CAP 16384  /* default hot-table entries: a 64 KB table leaves
+                             about 150 KB of the SM's unified L1/shared
+                             memory to L1, which keeps the next tier of warm
+                             contributions (measured best on R-MAT s20, s22) */
+#endif
+#ifndef AG_WARM_DEFAULT
+#define AG_WARM_DEFAULT 65536 /* ids below this may allocate L1 lines      */
 #endif
 #define AG_HOT_FIT ((AG_SMEM_MAX - AG_SMEM_STATIC - AG_STAGE_BYTES) / 4 / 64 * 64)
-#define AG_HOT_MAX (AG_HOT_FIT < AG_HOT_CAP ? AG_HOT_FIT : AG_HOT_CAP)
+#define AG_HOT_MAX AG_HOT_FIT
 #define AG_BULK_CHUNK 32768u
 
 /* A task is one warp's work item (uint4):
@@ -137,6 +143,8 @@ typedef struct AgPullParams
     uint32_t use_cond;     /* 1: launched by the CUDA graph's WHILE node      */
     uint32_t hot_n;        /* contributions (ids < hot_n) served from shared
                               memory; a multiple of 64                         */
+    uint32_t warm_n;       /* gathers of ids in [hot_n, warm_n) may take L1
+                              lines; colder ones bypass L1                     */
     const uint32_t *perm;  /* device row i is caller vertex perm[i]            */
     const uint32_t *inv;   /* caller vertex v is device row inv[v]             */
     float *out;            /* normalised ranks in caller order                 */

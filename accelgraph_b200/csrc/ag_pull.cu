@@ -87,6 +87,38 @@ __device__ __forceinline__ float ag_ld_gather_f32(const float *p, uint64_t pol)
     return v;
 }
 
+/* cold gather: beyond the warm tier, do not displace warm lines from L1 */
+__device__ __forceinline__ float ag_ld_cold_f32(const float *p, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ uint16_t ag_ld_cold_u16(const uint16_t *p, uint64_t pol)
+{
+    uint16_t v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
+/* per-row data read once per pass: bypass L1 */
+__device__ __forceinline__ uint32_t ag_ld_row_u32(const uint32_t *p)
+{
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+/* rank: read and later written by the same lane in the same kernel, so the
+ * coherent path, still without an L1 line */
+__device__ __forceinline__ float ag_ld_rank(const float *p)
+{
+    float v;
+    asm volatile("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ uint16_t ag_ld_gather_u16(const uint16_t *p, uint64_t pol)
 {
     uint16_t v;
@@ -265,14 +297,18 @@ struct AgPass
     __device__ __forceinline__ float gather(uint32_t u, float wj) const
     {
         if (MODE == AG_MODE_SPMV) {
-            const float xv = (u < hot_n) ? hot32[u] : ag_ld_gather_f32(p.x + u, pol_last);
+            const float xv = (u < hot_n) ? hot32[u]
+                             : (u < p.warm_n ? ag_ld_gather_f32(p.x + u, pol_last) : ag_ld_cold_f32(p.x + u, pol_last));
             if (p.wmode == AG_SPMV_W_UNIT)
                 return xv;
             return __fmul_rn(wj, xv);
         }
         if (PREC != 0 && read_low)
-            return ag_low_to_f32<PREC>((u < hot_n) ? hot16[u] : ag_ld_gather_u16(c_in16 + u, pol_last));
-        return (u < hot_n) ? hot32[u] : ag_ld_gather_f32(c_in32 + u, pol_last);
+            return ag_low_to_f32<PREC>((u < hot_n) ? hot16[u]
+                                       : (u < p.warm_n ? ag_ld_gather_u16(c_in16 + u, pol_last)
+                                                       : ag_ld_cold_u16(c_in16 + u, pol_last)));
+        return (u < hot_n) ? hot32[u]
+                           : (u < p.warm_n ? ag_ld_gather_f32(c_in32 + u, pol_last) : ag_ld_cold_f32(c_in32 + u, pol_last));
     }
 
     /* the reference's per-vertex update for a finished row sum; rp and od
@@ -494,11 +530,11 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             uint32_t o0 = ee, o1 = ee, od = 0;
             float rp = 0.0f;
             if (live) {
-                o0 = p.row_off[r];
-                o1 = p.row_off[r + 1];
+                o0 = ag_ld_row_u32(p.row_off + r);
+                o1 = ag_ld_row_u32(p.row_off + r + 1);
                 if (MODE == AG_MODE_PR) {
-                    rp = p.rank[r];
-                    od = p.outdeg[r];
+                    rp = ag_ld_rank(p.rank + r);
+                    od = ag_ld_row_u32(p.outdeg + r);
                 }
             }
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);

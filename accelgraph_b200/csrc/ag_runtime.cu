@@ -189,6 +189,7 @@ struct ag_graph_s
     float *out;             /* normalised ranks, caller order                */
     float *xbuf, *ybuf;     /* SpMV vectors in device order                  */
     uint32_t hot_n;         /* entries of the shared-memory hot table        */
+    uint32_t warm_n;        /* ids below this may allocate L1 lines          */
     uint4 *tasks_fast, *tasks_exact;
     uint32_t ntasks_fast, ntasks_exact;
     uint32_t nparts;
@@ -504,7 +505,21 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
         off_old = ids_old = outdeg_old = nullptr;
         w_old = nullptr;
     }
-    g->hot_n = (flags & AG_UPLOAD_NO_SMEM_CACHE) ? 0u : std::min<uint32_t>(N & ~63u, AG_HOT_MAX);
+    {
+        /* tunables (the defaults were measured best on R-MAT s20/s22):
+         * AG_HOT_ENTRIES -- shared-memory table entries (<= AG_HOT_MAX)
+         * AG_WARM_ENTRIES -- ids below this may allocate L1 lines */
+        uint32_t hot = AG_HOT_CAP, warm = AG_WARM_DEFAULT;
+        const char *eh = getenv("AG_HOT_ENTRIES");
+        const char *ew = getenv("AG_WARM_ENTRIES");
+        if (eh)
+            hot = (uint32_t)strtoul(eh, nullptr, 10);
+        if (ew)
+            warm = (uint32_t)strtoul(ew, nullptr, 10);
+        hot = std::min<uint32_t>(hot, AG_HOT_MAX);
+        g->hot_n = (flags & AG_UPLOAD_NO_SMEM_CACHE) ? 0u : std::min<uint32_t>(N & ~63u, hot & ~63u);
+        g->warm_n = std::max<uint32_t>(warm, g->hot_n);
+    }
 
     std::vector<uint4> tf, te;
     uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
@@ -546,7 +561,7 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
 }
 
 static size_t pull_smem(const ag_graph_s *g);
-static ag_status_t pull_kernel_prepare(const void *kern);
+static ag_status_t pull_kernel_prepare(const void *kern, size_t smem);
 
 extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
 {
@@ -560,7 +575,7 @@ extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
     info->max_in_degree = g->max_in_degree;
     info->device_bytes = g->device_bytes;
     int nb = 0;
-    if (pull_kernel_prepare(ag_pull_kernel_ptr(AG_MODE_PR, 0, 0)) == AG_OK &&
+    if (pull_kernel_prepare(ag_pull_kernel_ptr(AG_MODE_PR, 0, 0), pull_smem(g)) == AG_OK &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ag_pull_kernel_ptr(AG_MODE_PR, 0, 0), AG_BLK,
                                                       pull_smem(g)) == cudaSuccess)
         info->grid = (uint32_t)std::min<uint64_t>((uint64_t)nb * g_ctx.num_sms,
@@ -573,17 +588,26 @@ extern "C" ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info)
 static size_t pull_smem(const ag_graph_s *g) { return (size_t)AG_STAGE_BYTES + (size_t)g->hot_n * 4; }
 
 /* the pull kernels take up to AG_SMEM_MAX bytes of shared memory */
-static ag_status_t pull_kernel_prepare(const void *kern)
+static ag_status_t pull_kernel_prepare(const void *kern, size_t smem = 0)
 {
     AG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  AG_SMEM_MAX - AG_SMEM_STATIC));
+    if (smem) {
+        /* carve out only the shared memory the CTAs need: the rest of the
+         * SM's unified 256 KB is L1 for the warm gathers */
+        const size_t per_sm = (smem + AG_SMEM_STATIC + 1024) * AG_CTAS_PER_SM;
+        int pct = (int)((per_sm * 100 + 233471) / 233472);
+        if (pct > 100)
+            pct = 100;
+        AG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    }
     return AG_OK;
 }
 
 static unsigned pull_grid(const void *kern, uint32_t ntasks, size_t smem)
 {
     int nb = 0;
-    if (pull_kernel_prepare(kern) != AG_OK ||
+    if (pull_kernel_prepare(kern, smem) != AG_OK ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, AG_BLK, smem) != cudaSuccess || nb < 1) {
         cudaGetLastError();
         nb = 1;
@@ -631,6 +655,7 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.inv = g->inv;
     p.out = g->out;
     p.hot_n = g->hot_n;
+    p.warm_n = g->warm_n;
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
