@@ -170,10 +170,26 @@ SIGNATURES = [
     ("ag_spmv_pull_device", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     ("ag_spmv_pull", C.c_int32, [C.c_void_p, f32p, f32p, C.c_uint32]),
     ("ag_spmv_pull_ex", C.c_int32, [C.POINTER(Arguments), GraphP, C.c_int, C.POINTER(C.POINTER(SPMVStats))]),
+    ("ag_spmv_pull_noalloc", C.c_int32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_uint32, C.c_void_p]),
 ]
 
 
+def _ensure_built() -> None:
+    """Rebuild the in-tree library when a source is newer than it (the build
+    recipe is loaded from its file so that it needs nothing from this
+    package)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_accelgraph_b200_build", _PKG / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    if mod._stale():
+        mod.build()
+
+
 def _load() -> C.CDLL:
+    if "AG_LIBRARY" not in os.environ:
+        _ensure_built()
     path = Path(os.environ.get("AG_LIBRARY", LIB_PATH))
     if not path.exists():
         raise ImportError(

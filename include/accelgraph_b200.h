@@ -210,6 +210,28 @@ ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, double tol,
 ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *y, uint32_t mode);
 /* Host-pointer form: uploads x, runs, copies y back and waits. */
 ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint32_t mode);
+/* SpMV pull that allocates nothing, for callers that may not allocate device
+ * memory once running (a host framework that owns all device memory, or a
+ * latency-critical path that cannot afford cudaMalloc's device-wide
+ * synchronisation).  No counterpart in the reference: it has no device
+ * memory of its own to manage.
+ * Inputs and outputs are caller-owned DEVICE pointers: row_off[num_vertices+1]
+ * (inverse-CSR row starts), ids[num_edges] (in-neighbours), w[num_edges] (or
+ * NULL: the reference's unweighted 0.0001f), x and y[num_vertices]; mode is
+ * AG_SPMV_GRAPH_WEIGHTS or AG_SPMV_UNIT; stream is a cudaStream_t (NULL: the
+ * legacy default stream).  The work is enqueued on that stream and the call
+ * returns without waiting.
+ * Limit: its only scratch is a fixed 256 KB device array listing the rows of
+ * more than 4096 in-edges (at most 65536 of them), so num_edges must be at
+ * most 2^28; larger inputs are rejected with AG_ERR_UNSUPPORTED.  Every GPU
+ * that loads the library holds that array until the process exits.  The
+ * first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array: calls whose work
+ * overlaps on the GPU race, so issue them on one stream. */
+ag_status_t ag_spmv_pull_noalloc(uint32_t num_vertices, uint32_t num_edges, const uint32_t *row_off,
+                                 const uint32_t *ids, const float *w, const float *x, float *y,
+                                 uint32_t mode, void *stream);
+
 /* Status-returning form of SPMVPullGraphCSR. */
 ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph,
                             int quiet, struct SPMVStats **out);
