@@ -170,6 +170,9 @@ SIGNATURES = [
     ("ag_spmv_pull_device", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     ("ag_spmv_pull", C.c_int32, [C.c_void_p, f32p, f32p, C.c_uint32]),
     ("ag_spmv_pull_ex", C.c_int32, [C.POINTER(Arguments), GraphP, C.c_int, C.POINTER(C.POINTER(SPMVStats))]),
+    ("ag_multigraph_upload", C.c_int32, [C.POINTER(GraphP), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("ag_multigraph_fetch", C.c_int32, [C.c_void_p, f32p, u32p, u32p, u32p, f64p, f64p]),
+    ("ag_ppr_spmm", C.c_int32, [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_double, f32p, C.POINTER(PRResult)]),
     ("ag_spmv_pull_noalloc", C.c_int32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_uint32, C.c_void_p]),
 ]
@@ -423,11 +426,62 @@ class DeviceGraph:
               "ag_pagerank_f64")
         return r, passes.value
 
+    def ppr(self, sources, iterations=100, epsilon=1e-6, want_ranks=True):
+        """Batched personalized PageRank (k = len(sources) <= 64); returns
+        (ranks N x k or None, PRResult)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        k = len(src)
+        out = np.empty((self.num_vertices, k), np.float32) if want_ranks else None
+        res = PRResult()
+        check(lib.ag_ppr_spmm(self.h, src.ctypes.data_as(u32p), k, iterations, epsilon,
+                              out.ctypes.data_as(f32p) if want_ranks else None, C.byref(res)), "ag_ppr_spmm")
+        return out, res
+
     def spmv(self, x, mode=AG_SPMV_GRAPH_WEIGHTS) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float32)
         y = np.empty(self.num_vertices, np.float32)
         check(lib.ag_spmv_pull(self.h, x.ctypes.data_as(f32p), y.ctypes.data_as(f32p), mode), "ag_spmv_pull")
         return y
+
+
+class MultiGraph:
+    """Many independent graphs solved in one launch (ag_multigraph_*)."""
+
+    def __init__(self, graphs, flags: int = 0):
+        arr = (GraphP * len(graphs))(*[g.ptr for g in graphs])
+        h = C.c_void_p()
+        check(lib.ag_multigraph_upload(arr, len(graphs), flags, C.byref(h)), "ag_multigraph_upload")
+        self.h = h
+        self.sizes = [g.num_vertices for g in graphs]
+        self.edges = [g.num_edges for g in graphs]
+        self.count = len(graphs)
+
+    def release(self) -> None:
+        if self.h:
+            lib.ag_graph_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def pagerank(self, iterations=100, epsilon=1e-6, order=AG_ORDER_FAST):
+        o = make_opts(order=order)
+        check(lib.ag_pagerank_launch(self.h, iterations, epsilon, C.byref(o)), "ag_pagerank_launch")
+        n = sum(self.sizes)
+        ranks = np.empty(n, np.float32)
+        it = np.zeros(self.count, np.uint32)
+        ps = np.zeros(self.count, np.uint32)
+        cv = np.zeros(self.count, np.uint32)
+        er = np.zeros(self.count, np.float64)
+        ms = C.c_double()
+        check(lib.ag_multigraph_fetch(self.h, ranks.ctypes.data_as(f32p), it.ctypes.data_as(u32p),
+                                      ps.ctypes.data_as(u32p), cv.ctypes.data_as(u32p), er.ctypes.data_as(f64p),
+                                      C.byref(ms)), "ag_multigraph_fetch")
+        parts = np.split(ranks, np.cumsum(self.sizes)[:-1])
+        return parts, {"iterations": it, "passes": ps, "converged": cv, "error_total": er, "device_ms": ms.value}
 
 
 def make_opts(precision=AG_PREC_FP32, order=AG_ORDER_FAST, init_ranks=None, switch_residual=1e-4,

@@ -79,6 +79,8 @@
 
 #define AG_MODE_PR 0
 #define AG_MODE_SPMV 1
+#define AG_MODE_MULTI 2   /* PageRank over a union of independent graphs,
+                             each with its own convergence                  */
 
 #define AG_SPMV_W_GRAPH 0 /* multiply by the uploaded weight                */
 #define AG_SPMV_W_CONST 1 /* multiply by 0.0001f (graph without weights)    */
@@ -148,12 +150,32 @@ typedef struct AgPullParams
     const uint32_t *perm;  /* device row i is caller vertex perm[i]            */
     const uint32_t *inv;   /* caller vertex v is device row inv[v]             */
     float *out;            /* normalised ranks in caller order                 */
+    /* union of independent graphs (AG_MODE_MULTI) */
+    const uint32_t *gstart; /* first row of each graph, ngraphs + 1 entries    */
+    uint32_t ngraphs;
+    uint32_t *g_active;    /* per graph: active vertices of the running pass   */
+    double *g_err;         /* per graph: sum |r' - r| of the running pass      */
+    uint32_t *g_done;      /* per graph: 1 once converged or capped            */
+    uint32_t *g_passes;    /* per graph: passes run                            */
+    uint32_t *g_conv;      /* per graph: 1 if a pass had no active vertex      */
+    double *g_err_last;    /* per graph: error total of its last pass          */
     cudaGraphConditionalHandle cond;
 } AgPullParams;
+
+/* read-only view of a device graph for the other kernels of this library */
+typedef struct AgGraphView
+{
+    const uint32_t *row_off, *ids, *outdeg, *perm, *inv;
+    uint32_t N, E;
+    cudaStream_t stream;
+} AgGraphView;
 
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+struct ag_graph_s;
+int32_t ag_rt_graph_view(struct ag_graph_s *g, AgGraphView *v);
 
 /* Kernel selection (prec: 0 fp32, 1 bf16, 2 fp16; exact: stream-order sums) */
 const void *ag_pull_kernel_ptr(int mode, int prec, int exact);

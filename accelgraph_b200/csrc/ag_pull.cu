@@ -265,7 +265,7 @@ struct AgPass
         c_in16 = nullptr;
         c_out32 = nullptr;
         c_out16 = nullptr;
-        if (MODE == AG_MODE_PR) {
+        if (MODE != AG_MODE_SPMV) {
             const uint32_t pass = p.ctl->iter;
             eps = p.ctl->eps;
             if (PREC != 0) {
@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
 
     /* stream launches (profiling) run a fixed number of kernels: the ones
      * after the loop has ended return at once */
-    if (MODE == AG_MODE_PR && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
+    if (MODE != AG_MODE_SPMV && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
         return;
     AgPass<MODE, PREC, EXACT> ps(p);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -522,6 +522,25 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         const uint32_t kind = task.x >> 30;
         const uint32_t r0 = task.x & AG_ROW_MASK;
         const uint32_t eb = task.z, ee = task.w;
+        uint32_t gid = 0;
+        if (MODE == AG_MODE_MULTI) {
+            /* the item's graph; items of finished graphs are skipped */
+            uint32_t lo = 0, hi = p.ngraphs;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(p.gstart + mid) <= r0)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            gid = lo;
+            if (*((volatile uint32_t *)(p.g_done + gid))) {
+                pf = ps.prefetch(task_n.z, task_n.w, lane);
+                task = task_n;
+                t = tn;
+                continue;
+            }
+        }
         if (kind == AG_T_ROWS) {
             /* one row per lane; its bounds, previous rank and out-degree are
              * loaded first so that they arrive while the stage runs */
@@ -532,7 +551,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             if (live) {
                 o0 = ag_ld_row_u32(p.row_off + r);
                 o1 = ag_ld_row_u32(p.row_off + r + 1);
-                if (MODE == AG_MODE_PR) {
+                if (MODE != AG_MODE_SPMV) {
                     rp = ag_ld_rank(p.rank + r);
                     od = ag_ld_row_u32(p.outdeg + r);
                 }
@@ -579,7 +598,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         } else if (kind == AG_T_LONG) {
             float rp = 0.0f;
             uint32_t od = 0;
-            if (MODE == AG_MODE_PR && lane == 0) {
+            if (MODE != AG_MODE_SPMV && lane == 0) {
                 rp = p.rank[r0];
                 od = p.outdeg[r0];
             }
@@ -617,7 +636,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                     p.hub_cnt[pbase] = 0;
                     float rp = 0.0f;
                     uint32_t od = 0;
-                    if (MODE == AG_MODE_PR) {
+                    if (MODE != AG_MODE_SPMV) {
                         rp = p.rank[r0];
                         od = p.outdeg[r0];
                     }
@@ -627,11 +646,24 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             __syncwarp();
             pf = pn;
         }
+        if (MODE == AG_MODE_MULTI) {
+            /* the item's totals go to its graph */
+            const double e = ag_warp_sum_d(ps.my_err);
+            const uint32_t a = ag_warp_sum_u(ps.my_active);
+            if (lane == 0) {
+                if (e != 0.0)
+                    atomicAdd(p.g_err + gid, e);
+                if (a)
+                    atomicAdd(p.g_active + gid, a);
+            }
+            ps.my_err = 0.0;
+            ps.my_active = 0;
+        }
         task = task_n;
         t = tn;
     }
 
-    if (MODE != AG_MODE_PR)
+    if (MODE == AG_MODE_SPMV)
         return;
 
     /* close the pass: CTA totals, then the last CTA records the pass and
@@ -660,6 +692,49 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             s_last = (ticket == gridDim.x - 1) ? 1u : 0u;
         }
         __syncthreads();
+    }
+    if (MODE == AG_MODE_MULTI) {
+        if (!s_last)
+            return;
+        /* every thread of the last CTA closes the pass of some graphs */
+        __threadfence();
+        AgControl *c = p.ctl;
+        volatile AgControl *vc = c;
+        const uint32_t P = vc->iter;
+        const uint32_t max_iter = vc->max_iter;
+        int running = 0;
+        for (uint32_t g = tid; g < p.ngraphs; g += blockDim.x) {
+            if (*((volatile uint32_t *)(p.g_done + g)))
+                continue;
+            const uint32_t a = *((volatile uint32_t *)(p.g_active + g));
+            const uint32_t np = p.g_passes[g] + 1;
+            const double n_g = (double)(__ldg(p.gstart + g + 1) - __ldg(p.gstart + g));
+            p.g_passes[g] = np;
+            p.g_err_last[g] = *((volatile double *)(p.g_err + g)) / (n_g > 0 ? n_g : 1.0);
+            p.g_active[g] = 0;
+            p.g_err[g] = 0.0;
+            if (a == 0) {
+                p.g_conv[g] = 1;
+                p.g_done[g] = 1;
+            } else if (np >= max_iter) {
+                p.g_done[g] = 1;
+            } else {
+                running = 1;
+            }
+        }
+        running = __syncthreads_or(running);
+        if (tid == 0) {
+            if (P < AG_MAX_HISTORY)
+                c->hist_t[P] = ag_globaltimer();
+            c->iter = P + 1;
+            c->done_ctas = 0;
+            c->converged = running ? 0u : 1u;
+            c->stop = running ? 0u : 1u;
+            __threadfence();
+            if (p.use_cond)
+                cudaGraphSetConditional(p.cond, running ? 1u : 0u);
+        }
+        return;
     }
     if (s_last && tid == 0) {
         __threadfence();
@@ -721,6 +796,14 @@ __global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams
         else
             ag_st_keep_f32(p.c32_0 + v, c, pol_last);
     }
+    for (uint32_t g = blockIdx.x * AG_SBLK + threadIdx.x; g < p.ngraphs; g += gridDim.x * AG_SBLK) {
+        p.g_active[g] = 0;
+        p.g_err[g] = 0.0;
+        p.g_done[g] = (run.max_iter > 0 && p.gstart[g + 1] > p.gstart[g]) ? 0u : 1u;
+        p.g_passes[g] = 0;
+        p.g_conv[g] = 0;
+        p.g_err_last[g] = 0.0;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         AgControl *c = p.ctl;
         c->iter = 0;
@@ -752,7 +835,20 @@ __global__ void __launch_bounds__(AG_SBLK) ag_normalize_kernel(const AgPullParam
     const float fN = __uint2float_rn(p.N);
     double s = 0.0;
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
-        const float r = __fdiv_rn(p.rank[p.inv ? p.inv[v] : v], fN);
+        float div = fN;
+        if (p.ngraphs) {
+            /* each graph of a union is normalised by its own vertex count */
+            uint32_t lo = 0, hi = p.ngraphs;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(p.gstart + mid) <= v)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            div = __uint2float_rn(__ldg(p.gstart + lo + 1) - __ldg(p.gstart + lo));
+        }
+        const float r = __fdiv_rn(p.rank[p.inv ? p.inv[v] : v], div);
         p.out[v] = r;
         s += (double)r;
     }
@@ -823,6 +919,9 @@ extern "C" const void *ag_pull_kernel_ptr(int mode, int prec, int exact)
     if (mode == AG_MODE_SPMV)
         return exact ? (const void *)ag_pull_kernel<AG_MODE_SPMV, 0, true>
                      : (const void *)ag_pull_kernel<AG_MODE_SPMV, 0, false>;
+    if (mode == AG_MODE_MULTI)
+        return exact ? (const void *)ag_pull_kernel<AG_MODE_MULTI, 0, true>
+                     : (const void *)ag_pull_kernel<AG_MODE_MULTI, 0, false>;
     switch (prec) {
     case 1:
         return exact ? (const void *)ag_pull_kernel<AG_MODE_PR, 1, true> : (const void *)ag_pull_kernel<AG_MODE_PR, 1, false>;

@@ -190,6 +190,11 @@ struct ag_graph_s
     float *xbuf, *ybuf;     /* SpMV vectors in device order                  */
     uint32_t hot_n;         /* entries of the shared-memory hot table        */
     uint32_t warm_n;        /* ids below this may allocate L1 lines          */
+    /* union of independent graphs (ag_multigraph_upload) */
+    uint32_t ngraphs;
+    uint32_t *gstart;       /* device, ngraphs + 1                           */
+    uint32_t *g_u32;        /* device: active, done, passes, conv (4 x ngraphs) */
+    double *g_f64;          /* device: err, err_last (2 x ngraphs)           */
     uint4 *tasks_fast, *tasks_exact;
     uint32_t ntasks_fast, ntasks_exact;
     uint32_t nparts;
@@ -257,6 +262,9 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->ids);
     dev_free(g->perm);
     dev_free(g->inv);
+    dev_free(g->gstart);
+    dev_free(g->g_u32);
+    dev_free(g->g_f64);
     dev_free(g->out);
     dev_free(g->xbuf);
     dev_free(g->ybuf);
@@ -291,11 +299,13 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
  * holding <= AG_WCAP in-edges.  Heavy items come first so that they start
  * early. */
 static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out,
-                              uint32_t *nparts, uint32_t *nhub)
+                              uint32_t *nparts, uint32_t *nhub, const uint32_t *gstart = nullptr,
+                              uint32_t ngraphs = 0)
 {
     std::vector<uint4> hubs, longs, rows;
     uint32_t pbase = 0, nh = 0;
     uint32_t r = 0;
+    uint32_t gnext = 0; /* rows items never cross the start of a graph */
     if (N > AG_ROW_MASK)
         return ag_set_error(AG_ERR_INVALID_GRAPH, "%u vertices exceed the 2^30 row limit", N);
     while (r < N) {
@@ -319,7 +329,10 @@ static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::
             continue;
         }
         const uint32_t rb = r, eb = off[r];
-        while (r < N && r - rb < AG_WROWS) {
+        while (gstart && gnext <= ngraphs && gstart[gnext] <= rb)
+            ++gnext;
+        const uint32_t limit = (gstart && gnext <= ngraphs) ? gstart[gnext] : N;
+        while (r < N && r < limit && r - rb < AG_WROWS) {
             const uint32_t dr = off[r + 1] - off[r];
             if (dr > AG_WCAP || off[r + 1] - eb > AG_WCAP)
                 break;
@@ -337,7 +350,16 @@ static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::
     return AG_OK;
 }
 
+static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
+                               uint32_t ngraphs, ag_graph_t *out);
+
 extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out)
+{
+    return upload_impl(graph, flags, nullptr, 0, out);
+}
+
+static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
+                               uint32_t ngraphs, ag_graph_t *out)
 {
     ag_clear_error();
     if (!graph || !out)
@@ -523,9 +545,9 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
 
     std::vector<uint4> tf, te;
     uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
-    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub);
+    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gstart_host, ngraphs);
     if (st == AG_OK)
-        st = plan_tasks(off.data(), N, true, te, &np2, &nh2);
+        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gstart_host, ngraphs);
     if (st != AG_OK) {
         ag_graph_release(g);
         return st;
@@ -547,6 +569,17 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
     if (!te.empty())
         UP(cudaMemcpyAsync(g->tasks_exact, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
     UP(cudaMemsetAsync(g->hub_cnt, 0, (size_t)nparts * 4 + 16, s));
+    if (ngraphs) {
+        g->ngraphs = ngraphs;
+        g->gstart = (uint32_t *)dev_alloc(g, (size_t)(ngraphs + 1) * 4, &st);
+        g->g_u32 = (uint32_t *)dev_alloc(g, (size_t)ngraphs * 4 * 4, &st);
+        g->g_f64 = (double *)dev_alloc(g, (size_t)ngraphs * 2 * 8, &st);
+        if (st != AG_OK) {
+            ag_graph_release(g);
+            return st;
+        }
+        UP(cudaMemcpyAsync(g->gstart, gstart_host, (size_t)(ngraphs + 1) * 4, cudaMemcpyHostToDevice, s));
+    }
     UP(cudaEventCreate(&g->ev0));
     UP(cudaEventCreate(&g->ev1));
     /* the host-side vectors die at return: wait for the copies */
@@ -656,6 +689,16 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.out = g->out;
     p.hot_n = g->hot_n;
     p.warm_n = g->warm_n;
+    p.ngraphs = g->ngraphs;
+    p.gstart = g->gstart;
+    if (g->ngraphs) {
+        p.g_active = g->g_u32;
+        p.g_done = g->g_u32 + g->ngraphs;
+        p.g_passes = g->g_u32 + 2 * g->ngraphs;
+        p.g_conv = g->g_u32 + 3 * g->ngraphs;
+        p.g_err = g->g_f64;
+        p.g_err_last = g->g_f64 + g->ngraphs;
+    }
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
@@ -670,7 +713,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
     x->params.use_cond = 1;
-    const void *kpull = ag_pull_kernel_ptr(AG_MODE_PR, prec, exact);
+    const void *kpull = ag_pull_kernel_ptr(g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR, prec, exact);
     x->grid = pull_grid(kpull, x->params.ntasks, pull_smem(g));
 
     AgRunConfig run;
@@ -740,6 +783,8 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
     if (o.precision < 0 || o.precision > 2)
         return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
+    if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "a graph union runs the FP32 form without a warm start");
     const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
     ag_status_t st = ensure_buffers(g, prec);
     if (st != AG_OK)
@@ -788,7 +833,7 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         void *ia[2] = {&sp, &run};
         AG_CUDA(cudaLaunchKernel(ki.func, ki.gridDim, ki.blockDim, ia, 0, s));
         void *pa[1] = {&sp};
-        const void *kpull = ag_pull_kernel_ptr(AG_MODE_PR, prec, exact);
+        const void *kpull = ag_pull_kernel_ptr(g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR, prec, exact);
         for (uint32_t i = 0; i < run.max_iter; ++i)
             AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, pull_smem(g), s));
         AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
@@ -1003,4 +1048,113 @@ extern "C" ag_status_t ag_spmv_run_host(ag_graph_t g, const float *x, float *y, 
     cudaFreeAsync(dx, s);
     cudaFreeAsync(dy, s);
     return st != AG_OK ? st : w;
+}
+
+
+extern "C" ag_status_t ag_rt_graph_view(ag_graph_t g, AgGraphView *v)
+{
+    if (!g || !v)
+        return ag_set_error(AG_ERR_INVALID_ARG, "NULL graph");
+    v->row_off = g->row_off;
+    v->ids = g->ids;
+    v->outdeg = g->outdeg;
+    v->perm = g->perm;
+    v->inv = g->inv;
+    v->N = g->N;
+    v->E = g->E;
+    v->stream = g_ctx.stream;
+    return AG_OK;
+}
+
+/* ------------------------------------------------- union of graphs */
+extern "C" ag_status_t ag_multigraph_upload(const struct GraphCSR *const *graphs, uint32_t count, uint32_t flags,
+                                            ag_graph_t *out)
+{
+    ag_clear_error();
+    if (!graphs || !out || count == 0)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_multigraph_upload: need at least one graph");
+    uint64_t N = 0, E = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!graphs[i])
+            return ag_set_error(AG_ERR_INVALID_ARG, "ag_multigraph_upload: graph %u is NULL", i);
+        N += graphs[i]->num_vertices;
+        E += graphs[i]->num_edges;
+    }
+    if (N > AG_ROW_MASK || E >= 0xFFFFFFF0ull)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_multigraph_upload: union of %llu vertices, %llu edges too large",
+                            (unsigned long long)N, (unsigned long long)E);
+    /* block-diagonal union: graph i's vertices follow graph i-1's */
+    std::vector<uint32_t> gstart(count + 1), indeg(N), idx(N), outdeg(N), nb(E);
+    uint64_t vb = 0, ebase = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const struct GraphCSR *gi = graphs[i];
+        const uint32_t n = gi->num_vertices;
+        gstart[i] = (uint32_t)vb;
+        uint64_t pos = ebase;
+        for (uint32_t v = 0; v < n; ++v) {
+            const uint32_t d = gi->inverse_vertices->out_degree[v], b = gi->inverse_vertices->edges_idx[v];
+            if ((uint64_t)b + d > gi->num_edges)
+                return ag_set_error(AG_ERR_INVALID_GRAPH, "graph %u row %u exceeds its edges", i, v);
+            indeg[vb + v] = d;
+            idx[vb + v] = (uint32_t)pos;
+            outdeg[vb + v] = gi->vertices->out_degree[v];
+            for (uint32_t j = 0; j < d; ++j) {
+                const uint32_t u = gi->inverse_sorted_edges_array->edges_array_dest[b + j];
+                if (u >= n)
+                    return ag_set_error(AG_ERR_INVALID_GRAPH, "graph %u: in-edge names vertex %u >= %u", i, u, n);
+                nb[pos + j] = (uint32_t)(vb + u);
+            }
+            pos += d;
+        }
+        vb += n;
+        ebase = pos;
+    }
+    gstart[count] = (uint32_t)vb;
+    struct Vertex fv = {outdeg.data(), indeg.data(), nullptr};
+    struct Vertex iv = {indeg.data(), outdeg.data(), idx.data()};
+    struct EdgeList iel;
+    memset(&iel, 0, sizeof(iel));
+    iel.num_edges = (uint32_t)E;
+    iel.num_vertices = (uint32_t)N;
+    iel.edges_array_dest = nb.data();
+    struct GraphCSR u;
+    memset(&u, 0, sizeof(u));
+    u.num_vertices = (uint32_t)N;
+    u.num_edges = (uint32_t)E;
+    u.vertices = &fv;
+    u.inverse_vertices = &iv;
+    u.inverse_sorted_edges_array = &iel;
+    /* vertices stay grouped by graph; the union is L2-resident at the sizes
+     * it is meant for, so no shared-memory table */
+    return upload_impl(&u, flags | AG_UPLOAD_KEEP_ORDER | AG_UPLOAD_NO_SMEM_CACHE, gstart.data(), count, out);
+}
+
+extern "C" ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t *iterations, uint32_t *passes,
+                                           uint32_t *converged, double *error_total, double *device_ms)
+{
+    if (!g || !g->ngraphs)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_multigraph_fetch: not a graph union");
+    ag_pr_result res;
+    ag_status_t st = ag_pagerank_fetch(g, ranks, &res, nullptr, nullptr, nullptr, 0);
+    if (st != AG_OK)
+        return st;
+    const uint32_t n = g->ngraphs;
+    std::vector<uint32_t> h(4 * (size_t)n);
+    std::vector<double> hd(2 * (size_t)n);
+    AG_CUDA(cudaMemcpy(h.data(), g->g_u32, h.size() * 4, cudaMemcpyDeviceToHost));
+    AG_CUDA(cudaMemcpy(hd.data(), g->g_f64, hd.size() * 8, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t np = h[2 * (size_t)n + i], cv = h[3 * (size_t)n + i];
+        if (passes)
+            passes[i] = np;
+        if (converged)
+            converged[i] = cv;
+        if (iterations)
+            iterations[i] = cv ? (np ? np - 1 : 0) : np; /* reference semantics per graph */
+        if (error_total)
+            error_total[i] = hd[(size_t)n + i];
+    }
+    if (device_ms)
+        *device_ms = res.device_ms;
+    return AG_OK;
 }

@@ -199,6 +199,33 @@ const float *ag_pagerank_device_ranks(ag_graph_t g);
 ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, double tol,
                             double *ranks, uint32_t *passes);
 
+/* --------------------------------------------- many independent graphs */
+/* Upload `count` graphs as one block-diagonal union (vertex ids of graph i
+ * follow those of graph i-1).  ag_pagerank_launch on the handle then solves
+ * every graph in the same CUDA-graph launch: one pass covers all graphs still
+ * running, each graph stops on its own convergence test or at the iteration
+ * cap, and its items are skipped afterwards; ag_pagerank_fetch's ranks are
+ * each graph's ranks normalised by its own vertex count, concatenated. */
+ag_status_t ag_multigraph_upload(const struct GraphCSR *const *graphs, uint32_t count, uint32_t flags,
+                                 ag_graph_t *out);
+/* Per-graph results of the last launch on a union (arrays of `count`
+ * entries, each may be NULL): iterations (reference semantics), passes,
+ * converged flags, last-pass error totals; device_ms for the whole launch. */
+ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t *iterations, uint32_t *passes,
+                                uint32_t *converged, double *error_total, double *device_ms);
+
+/* ------------------------------------------------- batched personalized PR */
+/* Personalized PageRank of k <= 64 source vertices (caller ids) solved
+ * together: one pass is one sparse x dense (N x 64) product.  Column i
+ * teleports to sources[i] with mass (1 - 0.85) * N (the reference's
+ * un-normalised scale, so epsilon keeps its meaning); the loop stops when no
+ * (vertex, column) pair changes by >= epsilon, or after max_iterations.
+ * ranks (host, may be NULL) receives num_vertices x k binary32 values r / N,
+ * row-major in caller vertex order.  result->error_total is the mean
+ * |r' - r| over all pairs of the last pass. */
+ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32_t k, uint32_t max_iterations,
+                        double epsilon, float *ranks, ag_pr_result *result);
+
 /* ------------------------------------------------------------------- SpMV */
 #define AG_SPMV_GRAPH_WEIGHTS 0u /* w = uploaded inverse weights (0.0001f if none) */
 #define AG_SPMV_UNIT          1u /* pure gather: y[v] = sum x[u]                   */

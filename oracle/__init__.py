@@ -39,6 +39,9 @@ def _load() -> C.CDLL:
     lib.oracle_pagerank_pull.restype = C.c_uint32
     lib.oracle_pagerank_f64.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f64p, C.c_int]
     lib.oracle_pagerank_f64.restype = C.c_uint32
+    lib.oracle_ppr.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, C.c_double, f32p,
+                               u32p, C.c_int]
+    lib.oracle_ppr.restype = C.c_uint32
     lib.oracle_max_threads.restype = C.c_int
     return lib
 
@@ -114,6 +117,19 @@ def pagerank_f64(in_idx, in_deg, in_nb, out_deg, max_iter=1000, tol=1e-13, threa
     passes = lib.oracle_pagerank_f64(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p),
                                      _p(out_deg, u32p), max_iter, tol, _p(r, f64p), threads)
     return r, passes
+
+
+def ppr(in_idx, in_deg, in_nb, out_deg, sources, iterations=100, epsilon=1e-6, threads=0):
+    """Returns (ranks n x k, iterations, passes)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    src = np.ascontiguousarray(sources, np.uint32)
+    n, k = len(in_deg), len(src)
+    r = np.zeros((n, k), np.float32)
+    it = C.c_uint32()
+    passes = lib.oracle_ppr(n, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_deg, u32p), k,
+                            _p(src, u32p), iterations, epsilon, r.ctypes.data_as(f32p), C.byref(it), threads)
+    return r, it.value, passes
 
 
 def max_threads() -> int:

@@ -221,4 +221,52 @@ uint32_t oracle_pagerank_f64(uint32_t n, const uint32_t *in_idx, const uint32_t 
     return it;
 }
 
+/* Batched personalized PageRank restated column by column: column i is the
+ * pull loop above with the teleport mass (1.0f - 0.85f) * n on sources[i]
+ * (zero elsewhere); a pass is active while any (vertex, column) pair changes
+ * by >= epsilon.  ranks_out receives n x k values r / n (row-major). */
+uint32_t oracle_ppr(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                    const uint32_t *out_deg, uint32_t k, const uint32_t *sources, uint32_t iterations, double epsilon,
+                    float *ranks_out, uint32_t *iterations_out, int threads)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_src = (1.0f - damp) * (float)n;
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    float *r = ranks_out;
+    float *c = (float *)malloc((size_t)(n ? n : 1) * k * sizeof(float));
+    uint32_t it, passes = 0, v;
+    for (v = 0; v < n; v++)
+        for (uint32_t i = 0; i < k; i++)
+            r[(size_t)v * k + i] = (v == sources[i]) ? base_src : 0.0f;
+    for (it = 0; it < iterations; it++) {
+        unsigned long long active = 0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++)
+            for (uint32_t i = 0; i < k; i++)
+                c[(size_t)v * k + i] = out_deg[v] ? r[(size_t)v * k + i] / out_deg[v] : 0.0f;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : active) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            for (uint32_t i = 0; i < k; i++) {
+                float s = 0.0f;
+                for (uint32_t j = in_idx[v]; j < in_idx[v] + in_deg[v]; j++)
+                    s += c[(size_t)in_nb[j] * k + i];
+                float prev = r[(size_t)v * k + i];
+                float next = ((v == sources[i]) ? base_src : 0.0f) + damp * s;
+                r[(size_t)v * k + i] = next;
+                if (fabs(next - prev) >= epsilon)
+                    active++;
+            }
+        }
+        passes++;
+        if (active == 0)
+            break;
+    }
+    for (size_t t = 0; t < (size_t)n * k; t++)
+        r[t] = r[t] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    free(c);
+    return passes;
+}
+
 int oracle_max_threads(void) { return omp_get_max_threads(); }
