@@ -109,6 +109,11 @@ class PRResult(C.Structure):
     ]
 
 
+class TileConfig(C.Structure):
+    _fields_ = [("task_edges", C.c_uint32), ("hub_chunk", C.c_uint32), ("hot_entries", C.c_uint32),
+                ("warm_entries", C.c_uint32)]
+
+
 class GraphInfo(C.Structure):
     _fields_ = [
         ("num_vertices", C.c_uint32), ("num_edges", C.c_uint32), ("num_tasks", C.c_uint32),
@@ -160,6 +165,9 @@ SIGNATURES = [
     ("ag_graph_upload", C.c_int32, [GraphP, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("ag_graph_release", C.c_int32, [C.c_void_p]),
     ("ag_graph_get_info", C.c_int32, [C.c_void_p, C.POINTER(GraphInfo)]),
+    ("ag_graph_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
+    ("ag_graph_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
+    ("ag_autotune", C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(TileConfig), f64p]),
     ("ag_pr_opts_init", None, [C.POINTER(PROpts)]),
     ("ag_pagerank_pull_ex", C.c_int32, [C.POINTER(Arguments), GraphP, C.POINTER(PROpts),
                                         C.POINTER(C.POINTER(PageRankStats))]),
@@ -172,6 +180,17 @@ SIGNATURES = [
     ("ag_spmv_pull_ex", C.c_int32, [C.POINTER(Arguments), GraphP, C.c_int, C.POINTER(C.POINTER(SPMVStats))]),
     ("ag_multigraph_upload", C.c_int32, [C.POINTER(GraphP), C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("ag_multigraph_fetch", C.c_int32, [C.c_void_p, f32p, u32p, u32p, u32p, f64p, f64p]),
+    ("ag_mlp_num_params", C.c_uint32, []),
+    ("ag_mlp_create", C.c_int32, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("ag_mlp_release", C.c_int32, [C.c_void_p]),
+    ("ag_mlp_set_params", C.c_int32, [C.c_void_p, f32p]),
+    ("ag_mlp_get_params", C.c_int32, [C.c_void_p, f32p]),
+    ("ag_features", C.c_int32, [C.c_void_p, C.c_void_p]),
+    ("ag_mlp_forward", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("ag_mlp_gradients", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, f32p, f32p]),
+    ("ag_mlp_train", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                 f32p]),
+    ("ag_mlp_warm_start", C.c_int32, [C.c_void_p, C.c_void_p, f32p]),
     ("ag_ppr_spmm", C.c_int32, [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_double, f32p, C.POINTER(PRResult)]),
     ("ag_spmv_pull_noalloc", C.c_int32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -394,6 +413,21 @@ class DeviceGraph:
         except Exception:
             pass
 
+    def tiles(self) -> TileConfig:
+        t = TileConfig()
+        check(lib.ag_graph_get_tiles(self.h, C.byref(t)), "ag_graph_get_tiles")
+        return t
+
+    def set_tiles(self, task_edges=256, hub_chunk=2048, hot_entries=16384, warm_entries=65536) -> None:
+        t = TileConfig(task_edges, hub_chunk, hot_entries, warm_entries)
+        check(lib.ag_graph_set_tiles(self.h, C.byref(t)), "ag_graph_set_tiles")
+
+    def autotune(self, passes=8):
+        t = TileConfig()
+        us = C.c_double()
+        check(lib.ag_autotune(self.h, passes, C.byref(t), C.byref(us)), "ag_autotune")
+        return t, us.value
+
     def launch(self, iterations=20, epsilon=1e-4, precision=AG_PREC_FP32, order=AG_ORDER_FAST,
                init_ranks=None, switch_residual=1e-4) -> None:
         o = make_opts(precision, order, init_ranks, switch_residual)
@@ -466,6 +500,12 @@ class MultiGraph:
             self.release()
         except Exception:
             pass
+
+    def autotune(self, passes=8):
+        t = TileConfig()
+        us = C.c_double()
+        check(lib.ag_autotune(self.h, passes, C.byref(t), C.byref(us)), "ag_autotune")
+        return t, us.value
 
     def pagerank(self, iterations=100, epsilon=1e-6, order=AG_ORDER_FAST):
         o = make_opts(order=order)

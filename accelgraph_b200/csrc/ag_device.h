@@ -133,6 +133,7 @@ typedef struct AgPullParams
     uint32_t N;
     float *rank;           /* PR: ranks; SpMV: y                               */
     const float *x;        /* SpMV input                                       */
+    uint32_t whub;         /* in-edges per hub chunk of this work list         */
     float *c32_0, *c32_1;
     uint16_t *c16_0, *c16_1;
     float *hub_part;

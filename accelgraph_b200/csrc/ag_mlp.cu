@@ -1,0 +1,546 @@
+/*
+ * ag_mlp.cu -- learned warm start for the pull PageRank: per-vertex degree
+ * features, and a small MLP (8 -> 64 -> 64 -> 1, ReLU) that predicts the
+ * log of a vertex's un-normalised rank, with hand-written training and
+ * inference kernels.
+ *
+ * Features of vertex v (in-neighbours u over the inverse CSR), all log1p:
+ *   f0 in-degree(v)            f1 out-degree(v)
+ *   f2 sum in-degree(u)        f3 sum out-degree(u)          (2-hop degrees)
+ *   f4 min out-degree(u)       f5 max out-degree(u)          (0 without u)
+ *   f6 sum 1/out-degree(u)     (one pull pass from uniform ranks)
+ *   f7 max in-degree(u)
+ *
+ * Precision: master weights are binary32; the forward pass of training and
+ * inference uses their bfloat16 rounding (round to nearest even) with binary32
+ * accumulation; gradients are taken with respect to the bfloat16 weights and
+ * applied to the binary32 masters (Adam).
+ *
+ * Training step (mini-batch of B samples):
+ *   k1  one thread per sample: forward, loss, and the per-sample backward
+ *       signals dh2 = d loss / d pre-activation of layer 2 (masked by ReLU),
+ *       dh1 likewise for layer 1; stores x, h1, h2, dh1, dh2 and d3.
+ *   k2  one CTA per chunk of 128 samples: the weight gradients as
+ *       chunk-local sums over samples staged in shared memory
+ *       (dW2 = dh2^T h1, dW1 = dh1^T x, dW3 = d3 h2, biases), added to the
+ *       global gradient with one atomic per weight per chunk.
+ *   k3  Adam update of the 4801 parameters, refresh of the bfloat16 copies.
+ */
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "ag_device.h"
+#include "ag_internal.h"
+#include "ag_rng.h"
+
+#define AG_MLP_IN 8
+#define AG_MLP_H 64
+/* parameter layout (binary32 masters): W1[64][8] b1[64] W2[64][64] b2[64] w3[64] b3 */
+#define AG_MLP_OFF_W1 0
+#define AG_MLP_OFF_B1 (AG_MLP_OFF_W1 + AG_MLP_H * AG_MLP_IN)
+#define AG_MLP_OFF_W2 (AG_MLP_OFF_B1 + AG_MLP_H)
+#define AG_MLP_OFF_B2 (AG_MLP_OFF_W2 + AG_MLP_H * AG_MLP_H)
+#define AG_MLP_OFF_W3 (AG_MLP_OFF_B2 + AG_MLP_H)
+#define AG_MLP_OFF_B3 (AG_MLP_OFF_W3 + AG_MLP_H)
+#define AG_MLP_NPARAM (AG_MLP_OFF_B3 + 1)
+#define AG_MLP_BLK 128
+#define AG_MLP_CHUNK 128
+
+struct ag_mlp_s
+{
+    float *w;        /* masters (device)              */
+    __nv_bfloat16 *wb; /* bfloat16 copies (device)    */
+    float *g;        /* gradient accumulator          */
+    float *m, *v;    /* Adam moments                  */
+    float *buf;      /* per-sample training signals   */
+    uint32_t buf_cap;
+    float *loss;     /* device scalar                 */
+    uint32_t step;
+};
+
+/* ---------------------------------------------------------- features */
+__global__ void ag_features_kernel(AgGraphView gv, float *X)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < gv.N; v += nw) {
+        const uint32_t b = gv.row_off[v], e = gv.row_off[v + 1];
+        float s_in = 0.f, s_out = 0.f, s_c = 0.f, mx_in = 0.f, mx_out = 0.f, mn_out = 3.0e38f;
+        for (uint32_t j = b + lane; j < e; j += 32) {
+            const uint32_t u = gv.ids[j];
+            const float din = (float)(gv.row_off[u + 1] - gv.row_off[u]);
+            const uint32_t od = gv.outdeg[u];
+            const float dout = (float)od;
+            s_in += din;
+            s_out += dout;
+            s_c += od ? 1.0f / dout : 0.0f;
+            mx_in = fmaxf(mx_in, din);
+            mx_out = fmaxf(mx_out, dout);
+            mn_out = fminf(mn_out, dout);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s_in += __shfl_xor_sync(0xffffffffu, s_in, o);
+            s_out += __shfl_xor_sync(0xffffffffu, s_out, o);
+            s_c += __shfl_xor_sync(0xffffffffu, s_c, o);
+            mx_in = fmaxf(mx_in, __shfl_xor_sync(0xffffffffu, mx_in, o));
+            mx_out = fmaxf(mx_out, __shfl_xor_sync(0xffffffffu, mx_out, o));
+            mn_out = fminf(mn_out, __shfl_xor_sync(0xffffffffu, mn_out, o));
+        }
+        if (lane < AG_MLP_IN) {
+            float f;
+            switch (lane) {
+            case 0: f = (float)(e - b); break;
+            case 1: f = (float)gv.outdeg[v]; break;
+            case 2: f = s_in; break;
+            case 3: f = s_out; break;
+            case 4: f = (e > b) ? mn_out : 0.0f; break;
+            case 5: f = mx_out; break;
+            case 6: f = s_c; break;
+            default: f = mx_in; break;
+            }
+            const uint32_t dst = gv.perm ? gv.perm[v] : v;
+            X[(size_t)dst * AG_MLP_IN + lane] = log1pf(f);
+        }
+    }
+}
+
+/* ------------------------------------------------------------ MLP math */
+__device__ __forceinline__ void ag_mlp_load_weights(const __nv_bfloat16 *wb, float *sw)
+{
+    for (uint32_t i = threadIdx.x; i < AG_MLP_NPARAM; i += blockDim.x)
+        sw[i] = __bfloat162float(wb[i]);
+    __syncthreads();
+}
+
+/* layer 1 and 2 activations of one sample */
+__device__ __forceinline__ void ag_mlp_hidden(const float *sw, const float *x, float *h1, float *h2)
+{
+#pragma unroll 8
+    for (int j = 0; j < AG_MLP_H; ++j) {
+        float a = sw[AG_MLP_OFF_B1 + j];
+#pragma unroll
+        for (int i = 0; i < AG_MLP_IN; ++i)
+            a = fmaf(sw[AG_MLP_OFF_W1 + j * AG_MLP_IN + i], x[i], a);
+        h1[j] = fmaxf(a, 0.0f);
+    }
+#pragma unroll 4
+    for (int k = 0; k < AG_MLP_H; ++k) {
+        float a = sw[AG_MLP_OFF_B2 + k];
+#pragma unroll
+        for (int j = 0; j < AG_MLP_H; ++j)
+            a = fmaf(sw[AG_MLP_OFF_W2 + k * AG_MLP_H + j], h1[j], a);
+        h2[k] = fmaxf(a, 0.0f);
+    }
+}
+
+__device__ __forceinline__ float ag_mlp_out(const float *sw, const float *h2)
+{
+    float y = sw[AG_MLP_OFF_B3];
+#pragma unroll
+    for (int k = 0; k < AG_MLP_H; ++k)
+        y = fmaf(sw[AG_MLP_OFF_W3 + k], h2[k], y);
+    return y;
+}
+
+__global__ void __launch_bounds__(AG_MLP_BLK) ag_mlp_infer_kernel(const __nv_bfloat16 *wb, const float *X, uint32_t n,
+                                                                  float *Y)
+{
+    __shared__ float sw[AG_MLP_NPARAM];
+    ag_mlp_load_weights(wb, sw);
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        float x[AG_MLP_IN], h1[AG_MLP_H], h2[AG_MLP_H];
+#pragma unroll
+        for (int i = 0; i < AG_MLP_IN; ++i)
+            x[i] = X[(size_t)s * AG_MLP_IN + i];
+        ag_mlp_hidden(sw, x, h1, h2);
+        Y[s] = ag_mlp_out(sw, h2);
+    }
+}
+
+/* per-sample training signals; buf layout per sample (stride 2 + 4*64 + 8):
+ * [x(8) h1(64) h2(64) dh1(64) dh2(64) d3 pad] */
+#define AG_MLP_REC (AG_MLP_IN + 4 * AG_MLP_H + 2)
+__global__ void __launch_bounds__(AG_MLP_BLK) ag_mlp_k1(const __nv_bfloat16 *wb, const float *X, const float *T,
+                                                        uint32_t n, float scale, float *buf, float *loss)
+{
+    __shared__ float sw[AG_MLP_NPARAM];
+    __shared__ float sl[AG_MLP_BLK / 32];
+    ag_mlp_load_weights(wb, sw);
+    float my_loss = 0.0f;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        float x[AG_MLP_IN], h1[AG_MLP_H], h2[AG_MLP_H];
+#pragma unroll
+        for (int i = 0; i < AG_MLP_IN; ++i)
+            x[i] = X[(size_t)s * AG_MLP_IN + i];
+        ag_mlp_hidden(sw, x, h1, h2);
+        const float y = ag_mlp_out(sw, h2);
+        const float r = y - T[s];
+        my_loss += r * r;
+        const float d3 = 2.0f * r * scale; /* d (mean squared error) / d y */
+        float *rec = buf + (size_t)s * AG_MLP_REC;
+#pragma unroll
+        for (int i = 0; i < AG_MLP_IN; ++i)
+            rec[i] = x[i];
+        float dh2[AG_MLP_H];
+#pragma unroll
+        for (int k = 0; k < AG_MLP_H; ++k) {
+            dh2[k] = h2[k] > 0.0f ? d3 * sw[AG_MLP_OFF_W3 + k] : 0.0f;
+            rec[AG_MLP_IN + k] = h1[k];
+            rec[AG_MLP_IN + AG_MLP_H + k] = h2[k];
+            rec[AG_MLP_IN + 3 * AG_MLP_H + k] = dh2[k];
+        }
+#pragma unroll 4
+        for (int j = 0; j < AG_MLP_H; ++j) {
+            float a = 0.0f;
+#pragma unroll
+            for (int k = 0; k < AG_MLP_H; ++k)
+                a = fmaf(dh2[k], sw[AG_MLP_OFF_W2 + k * AG_MLP_H + j], a);
+            rec[AG_MLP_IN + 2 * AG_MLP_H + j] = h1[j] > 0.0f ? a : 0.0f;
+        }
+        rec[AG_MLP_IN + 4 * AG_MLP_H] = d3;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        my_loss += __shfl_xor_sync(0xffffffffu, my_loss, o);
+    if ((threadIdx.x & 31) == 0)
+        sl[threadIdx.x >> 5] = my_loss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < AG_MLP_BLK / 32; ++w)
+            t += sl[w];
+        atomicAdd(loss, t);
+    }
+}
+
+/* chunk sums of the weight gradients over AG_MLP_CHUNK samples */
+__global__ void __launch_bounds__(256) ag_mlp_k2(const float *buf, uint32_t n, float *grad)
+{
+    extern __shared__ float sm[]; /* AG_MLP_CHUNK x AG_MLP_REC */
+    const uint32_t s0 = blockIdx.x * AG_MLP_CHUNK;
+    const uint32_t cnt = min((uint32_t)AG_MLP_CHUNK, n - s0);
+    for (uint32_t i = threadIdx.x; i < cnt * AG_MLP_REC; i += blockDim.x)
+        sm[i] = buf[(size_t)s0 * AG_MLP_REC + i];
+    __syncthreads();
+    for (uint32_t o = threadIdx.x; o < AG_MLP_NPARAM; o += blockDim.x) {
+        float a = 0.0f;
+        if (o < AG_MLP_OFF_B1) { /* W1[j][i] = sum dh1[j] x[i] */
+            const uint32_t j = o / AG_MLP_IN, i = o % AG_MLP_IN;
+            for (uint32_t s = 0; s < cnt; ++s)
+                a = fmaf(sm[s * AG_MLP_REC + AG_MLP_IN + 2 * AG_MLP_H + j], sm[s * AG_MLP_REC + i], a);
+        } else if (o < AG_MLP_OFF_W2) { /* b1[j] */
+            const uint32_t j = o - AG_MLP_OFF_B1;
+            for (uint32_t s = 0; s < cnt; ++s)
+                a += sm[s * AG_MLP_REC + AG_MLP_IN + 2 * AG_MLP_H + j];
+        } else if (o < AG_MLP_OFF_B2) { /* W2[k][j] = sum dh2[k] h1[j] */
+            const uint32_t k = (o - AG_MLP_OFF_W2) / AG_MLP_H, j = (o - AG_MLP_OFF_W2) % AG_MLP_H;
+            for (uint32_t s = 0; s < cnt; ++s)
+                a = fmaf(sm[s * AG_MLP_REC + AG_MLP_IN + 3 * AG_MLP_H + k], sm[s * AG_MLP_REC + AG_MLP_IN + j], a);
+        } else if (o < AG_MLP_OFF_W3) { /* b2[k] */
+            const uint32_t k = o - AG_MLP_OFF_B2;
+            for (uint32_t s = 0; s < cnt; ++s)
+                a += sm[s * AG_MLP_REC + AG_MLP_IN + 3 * AG_MLP_H + k];
+        } else if (o < AG_MLP_OFF_B3) { /* w3[k] = sum d3 h2[k] */
+            const uint32_t k = o - AG_MLP_OFF_W3;
+            for (uint32_t s = 0; s < cnt; ++s)
+                a = fmaf(sm[s * AG_MLP_REC + AG_MLP_IN + 4 * AG_MLP_H], sm[s * AG_MLP_REC + AG_MLP_IN + AG_MLP_H + k],
+                         a);
+        } else { /* b3 */
+            for (uint32_t s = 0; s < cnt; ++s)
+                a += sm[s * AG_MLP_REC + AG_MLP_IN + 4 * AG_MLP_H];
+        }
+        atomicAdd(grad + o, a);
+    }
+}
+
+__global__ void ag_mlp_adam_kernel(float *w, __nv_bfloat16 *wb, const float *g, float *m, float *v, float lr,
+                                   float b1t, float b2t)
+{
+    const float b1 = 0.9f, b2 = 0.999f, epsv = 1e-8f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < AG_MLP_NPARAM; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float mh = mi / (1.0f - b1t), vh = vi / (1.0f - b2t);
+        const float wi = w[i] - lr * mh / (sqrtf(vh) + epsv);
+        w[i] = wi;
+        wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+__global__ void ag_mlp_round_kernel(const float *w, __nv_bfloat16 *wb)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < AG_MLP_NPARAM; i += gridDim.x * blockDim.x)
+        wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+/* init[v] = exp(prediction) in caller order, floored at base_pr */
+__global__ void ag_mlp_to_ranks_kernel(const float *Y, uint32_t n, float floor_v, float *out)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        out[v] = fmaxf(expf(Y[v]), floor_v);
+}
+
+/* ------------------------------------------------------------- host API */
+#define MCHK(call)                                                                                       \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            cudaGetLastError();                                                                          \
+            return ag_set_error(AG_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));            \
+        }                                                                                                \
+    } while (0)
+
+static cudaStream_t mlp_stream()
+{
+    return (cudaStream_t)ag_stream();
+}
+
+extern "C" uint32_t ag_mlp_num_params(void) { return AG_MLP_NPARAM; }
+
+extern "C" ag_status_t ag_mlp_create(uint64_t seed, ag_mlp_t *out)
+{
+    ag_clear_error();
+    if (!out)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_create: NULL out");
+    if (!ag_stream())
+        return ag_set_error(AG_ERR_NO_DEVICE, "ag_mlp_create: no CUDA device");
+    ag_mlp_s *m = new ag_mlp_s();
+    memset((void *)m, 0, sizeof(*m));
+    const size_t nb = AG_MLP_NPARAM * sizeof(float);
+    cudaError_t e = cudaMalloc((void **)&m->w, nb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->wb, AG_MLP_NPARAM * sizeof(__nv_bfloat16));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->g, nb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->m, nb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->v, nb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&m->loss, sizeof(float));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ag_mlp_release(m);
+        return ag_set_error(AG_ERR_OOM, "ag_mlp_create: %s", cudaGetErrorString(e));
+    }
+    /* He-style uniform init from the counter generator; zero biases */
+    std::vector<float> w(AG_MLP_NPARAM, 0.0f);
+    for (int i = 0; i < AG_MLP_NPARAM; ++i) {
+        float lim = 0.0f;
+        if (i < AG_MLP_OFF_B1)
+            lim = sqrtf(6.0f / AG_MLP_IN);
+        else if (i >= AG_MLP_OFF_W2 && i < AG_MLP_OFF_B2)
+            lim = sqrtf(6.0f / AG_MLP_H);
+        else if (i >= AG_MLP_OFF_W3 && i < AG_MLP_OFF_B3)
+            lim = sqrtf(3.0f / AG_MLP_H);
+        w[i] = lim * (2.0f * ag_u01(ag_draw64(seed, (uint64_t)i, 0)) - 1.0f);
+    }
+    ag_status_t st = ag_mlp_set_params(m, w.data());
+    if (st != AG_OK) {
+        ag_mlp_release(m);
+        return st;
+    }
+    *out = m;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_release(ag_mlp_t m)
+{
+    if (!m)
+        return AG_OK;
+    cudaStreamSynchronize(mlp_stream());
+    cudaFree(m->w);
+    cudaFree(m->wb);
+    cudaFree(m->g);
+    cudaFree(m->m);
+    cudaFree(m->v);
+    cudaFree(m->buf);
+    cudaFree(m->loss);
+    delete m;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_set_params(ag_mlp_t m, const float *params)
+{
+    if (!m || !params)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_set_params: NULL argument");
+    cudaStream_t s = mlp_stream();
+    MCHK(cudaMemcpyAsync(m->w, params, AG_MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, s));
+    MCHK(cudaMemsetAsync(m->m, 0, AG_MLP_NPARAM * sizeof(float), s));
+    MCHK(cudaMemsetAsync(m->v, 0, AG_MLP_NPARAM * sizeof(float), s));
+    ag_mlp_round_kernel<<<8, 1024, 0, s>>>(m->w, m->wb);
+    MCHK(cudaGetLastError());
+    MCHK(cudaStreamSynchronize(s));
+    m->step = 0;
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_get_params(ag_mlp_t m, float *params)
+{
+    if (!m || !params)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_get_params: NULL argument");
+    MCHK(cudaStreamSynchronize(mlp_stream()));
+    MCHK(cudaMemcpy(params, m->w, AG_MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_features(ag_graph_t g, float *features)
+{
+    ag_clear_error();
+    AgGraphView gv;
+    ag_status_t st = ag_rt_graph_view(g, &gv);
+    if (st != AG_OK)
+        return st;
+    if (!features)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_features: NULL output");
+    if (gv.N == 0)
+        return AG_OK;
+    uint64_t blocks = ((uint64_t)gv.N * 32 + 255) / 256;
+    if (blocks > 148 * 16)
+        blocks = 148 * 16;
+    ag_features_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, features);
+    MCHK(cudaGetLastError());
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_forward(ag_mlp_t m, const float *X, uint32_t n, float *Y)
+{
+    ag_clear_error();
+    if (!m || (n && (!X || !Y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_forward: NULL argument");
+    if (n == 0)
+        return AG_OK;
+    uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK;
+    if (blocks > 148 * 16)
+        blocks = 148 * 16;
+    ag_mlp_infer_kernel<<<(unsigned)blocks, AG_MLP_BLK, 0, mlp_stream()>>>(m->wb, X, n, Y);
+    MCHK(cudaGetLastError());
+    return AG_OK;
+}
+
+static ag_status_t mlp_ensure_buf(ag_mlp_t m, uint32_t n)
+{
+    if (m->buf_cap >= n)
+        return AG_OK;
+    cudaFree(m->buf);
+    m->buf = nullptr;
+    m->buf_cap = 0;
+    MCHK(cudaMalloc((void **)&m->buf, (size_t)n * AG_MLP_REC * sizeof(float)));
+    m->buf_cap = n;
+    return AG_OK;
+}
+
+/* gradient of the mean squared error over n samples into m->g (and *loss) */
+static ag_status_t mlp_grad(ag_mlp_t m, const float *X, const float *T, uint32_t n, float *loss)
+{
+    ag_status_t st = mlp_ensure_buf(m, n);
+    if (st != AG_OK)
+        return st;
+    cudaStream_t s = mlp_stream();
+    MCHK(cudaMemsetAsync(m->g, 0, AG_MLP_NPARAM * sizeof(float), s));
+    MCHK(cudaMemsetAsync(m->loss, 0, sizeof(float), s));
+    uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK;
+    if (blocks > 148 * 16)
+        blocks = 148 * 16;
+    ag_mlp_k1<<<(unsigned)blocks, AG_MLP_BLK, 0, s>>>(m->wb, X, T, n, 1.0f / (float)n, m->buf, m->loss);
+    MCHK(cudaGetLastError());
+    const size_t smem = AG_MLP_CHUNK * AG_MLP_REC * sizeof(float);
+    MCHK(cudaFuncSetAttribute(ag_mlp_k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ag_mlp_k2<<<(n + AG_MLP_CHUNK - 1) / AG_MLP_CHUNK, 256, smem, s>>>(m->buf, n, m->g);
+    MCHK(cudaGetLastError());
+    if (loss) {
+        float h = 0.0f;
+        MCHK(cudaMemcpyAsync(&h, m->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+        MCHK(cudaStreamSynchronize(s));
+        *loss = h / (float)n;
+    }
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_gradients(ag_mlp_t m, const float *X, const float *T, uint32_t n, float *grad,
+                                        float *loss)
+{
+    ag_clear_error();
+    if (!m || !X || !T || n == 0)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_gradients: bad argument");
+    ag_status_t st = mlp_grad(m, X, T, n, loss);
+    if (st != AG_OK)
+        return st;
+    if (grad) {
+        MCHK(cudaStreamSynchronize(mlp_stream()));
+        MCHK(cudaMemcpy(grad, m->g, AG_MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_mlp_train(ag_mlp_t m, const float *X, const float *T, uint32_t n, uint32_t epochs,
+                                    uint32_t batch, float lr, float *final_loss)
+{
+    ag_clear_error();
+    if (!m || !X || !T || n == 0 || batch == 0)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_train: bad argument");
+    cudaStream_t s = mlp_stream();
+    float last = 0.0f;
+    for (uint32_t ep = 0; ep < epochs; ++ep) {
+        double sum = 0.0;
+        uint32_t nb = 0;
+        for (uint32_t b0 = 0; b0 < n; b0 += batch) {
+            const uint32_t cnt = std::min<uint32_t>(batch, n - b0);
+            float l = 0.0f;
+            const bool want = (b0 + batch >= n); /* loss of the epoch's last batch */
+            ag_status_t st = mlp_grad(m, X + (size_t)b0 * AG_MLP_IN, T + b0, cnt, want ? &l : nullptr);
+            if (st != AG_OK)
+                return st;
+            m->step++;
+            const float b1t = powf(0.9f, (float)m->step), b2t = powf(0.999f, (float)m->step);
+            ag_mlp_adam_kernel<<<8, 1024, 0, s>>>(m->w, m->wb, m->g, m->m, m->v, lr, b1t, b2t);
+            MCHK(cudaGetLastError());
+            if (want) {
+                sum += l;
+                ++nb;
+            }
+        }
+        last = nb ? (float)(sum / nb) : 0.0f;
+    }
+    MCHK(cudaStreamSynchronize(s));
+    if (final_loss)
+        *final_loss = last;
+    return AG_OK;
+}
+
+/* predicted un-normalised ranks (caller order, host) for a warm start */
+extern "C" ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_ranks)
+{
+    ag_clear_error();
+    AgGraphView gv;
+    ag_status_t st = ag_rt_graph_view(g, &gv);
+    if (st != AG_OK)
+        return st;
+    if (!m || !init_ranks)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_warm_start: NULL argument");
+    if (gv.N == 0)
+        return AG_OK;
+    cudaStream_t s = gv.stream;
+    float *X = nullptr, *Y = nullptr;
+    MCHK(cudaMallocAsync((void **)&X, (size_t)gv.N * AG_MLP_IN * sizeof(float), s));
+    MCHK(cudaMallocAsync((void **)&Y, (size_t)gv.N * sizeof(float), s));
+    st = ag_features(g, X);
+    if (st == AG_OK)
+        st = ag_mlp_forward(m, X, gv.N, Y);
+    if (st == AG_OK) {
+        ag_mlp_to_ranks_kernel<<<148 * 8, 256, 0, s>>>(Y, gv.N, 1.0f - Damp, Y);
+        cudaError_t e = cudaMemcpyAsync(init_ranks, Y, (size_t)gv.N * sizeof(float), cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess)
+            st = ag_set_error(AG_ERR_CUDA, "ag_mlp_warm_start: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(X, s);
+    cudaFreeAsync(Y, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (st == AG_OK && e != cudaSuccess)
+        st = ag_set_error(AG_ERR_CUDA, "ag_mlp_warm_start: %s", cudaGetErrorString(e));
+    return st;
+}

@@ -28,9 +28,9 @@
  *          <= AG_TSEQ edges: bit-identical to the reference's sequential
  *          sum); longer rows are summed by the whole warp (lane-strided
  *          partials + xor tree).  The update runs lane-parallel.
- *   long : one row of AG_WCAP < degree <= AG_WHUB, warp-strided partials
+ *   long : one row of (item cap) < degree <= (hub chunk), warp-strided partials
  *          straight from memory + xor tree.
- *   hub  : rows > AG_WHUB split into AG_WHUB-edge chunks on separate warps;
+ *   hub  : longer rows split into hub-chunk-sized pieces on separate warps;
  *          the last chunk to arrive sums the chunk partials in chunk order.
  * In EXACT order every row is summed in stream order by one lane.
  * All reductions have a fixed order: results do not depend on scheduling.
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             float s = ps.strided_partial(eb, ee, lane, pf);
             s = ag_warp_sum_f(s);
             if (lane == 0) {
-                const uint32_t nch = (deg + AG_WHUB - 1) / AG_WHUB;
+                const uint32_t nch = (deg + p.whub - 1) / p.whub;
                 p.hub_part[pbase + chunk] = s;
                 __threadfence();
                 const uint32_t prev = atomicAdd(&p.hub_cnt[pbase], 1u);

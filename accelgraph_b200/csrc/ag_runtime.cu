@@ -190,6 +190,9 @@ struct ag_graph_s
     float *xbuf, *ybuf;     /* SpMV vectors in device order                  */
     uint32_t hot_n;         /* entries of the shared-memory hot table        */
     uint32_t warm_n;        /* ids below this may allocate L1 lines          */
+    ag_tile_config tiles;   /* work-list and cache shape in use              */
+    uint32_t hot_allowed;   /* 0 when uploaded with AG_UPLOAD_NO_SMEM_CACHE  */
+    std::vector<uint32_t> *gstart_host;
     /* union of independent graphs (ag_multigraph_upload) */
     uint32_t ngraphs;
     uint32_t *gstart;       /* device, ngraphs + 1                           */
@@ -265,6 +268,7 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->gstart);
     dev_free(g->g_u32);
     dev_free(g->g_f64);
+    delete g->gstart_host;
     dev_free(g->out);
     dev_free(g->xbuf);
     dev_free(g->ybuf);
@@ -299,8 +303,8 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
  * holding <= AG_WCAP in-edges.  Heavy items come first so that they start
  * early. */
 static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out,
-                              uint32_t *nparts, uint32_t *nhub, const uint32_t *gstart = nullptr,
-                              uint32_t ngraphs = 0)
+                              uint32_t *nparts, uint32_t *nhub, const uint32_t *gstart, uint32_t ngraphs,
+                              uint32_t cap, uint32_t whub)
 {
     std::vector<uint4> hubs, longs, rows;
     uint32_t pbase = 0, nh = 0;
@@ -310,14 +314,14 @@ static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::
         return ag_set_error(AG_ERR_INVALID_GRAPH, "%u vertices exceed the 2^30 row limit", N);
     while (r < N) {
         const uint32_t d = off[r + 1] - off[r];
-        if (d > AG_WCAP) {
-            if (!exact && d > AG_WHUB) {
-                const uint32_t nch = (d + AG_WHUB - 1) / AG_WHUB;
+        if (d > cap) {
+            if (!exact && d > whub) {
+                const uint32_t nch = (d + whub - 1) / whub;
                 if (nch >= (1u << (32 - AG_SLOT_BITS)) || pbase + nch > AG_SLOT_MASK)
                     return ag_set_error(AG_ERR_UNSUPPORTED, "row %u: %u in-edges exceed the hub split limits", r, d);
                 for (uint32_t c = 0; c < nch; ++c) {
-                    const uint32_t cb = off[r] + c * AG_WHUB;
-                    const uint32_t ce = std::min(off[r + 1], cb + (uint32_t)AG_WHUB);
+                    const uint32_t cb = off[r] + c * whub;
+                    const uint32_t ce = std::min(off[r + 1], cb + whub);
                     hubs.push_back(make_uint4((AG_T_HUB << 30) | r, pbase | (c << AG_SLOT_BITS), cb, ce));
                 }
                 pbase += nch;
@@ -334,7 +338,7 @@ static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::
         const uint32_t limit = (gstart && gnext <= ngraphs) ? gstart[gnext] : N;
         while (r < N && r < limit && r - rb < AG_WROWS) {
             const uint32_t dr = off[r + 1] - off[r];
-            if (dr > AG_WCAP || off[r + 1] - eb > AG_WCAP)
+            if (dr > cap || off[r + 1] - eb > cap)
                 break;
             ++r;
         }
@@ -539,15 +543,22 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         if (ew)
             warm = (uint32_t)strtoul(ew, nullptr, 10);
         hot = std::min<uint32_t>(hot, AG_HOT_MAX);
-        g->hot_n = (flags & AG_UPLOAD_NO_SMEM_CACHE) ? 0u : std::min<uint32_t>(N & ~63u, hot & ~63u);
+        g->hot_allowed = (flags & AG_UPLOAD_NO_SMEM_CACHE) ? 0u : 1u;
+        g->hot_n = g->hot_allowed ? std::min<uint32_t>(N & ~63u, hot & ~63u) : 0u;
         g->warm_n = std::max<uint32_t>(warm, g->hot_n);
+        g->tiles.task_edges = AG_WCAP;
+        g->tiles.hub_chunk = AG_WHUB;
+        g->tiles.hot_entries = g->hot_n;
+        g->tiles.warm_entries = g->warm_n;
     }
 
     std::vector<uint4> tf, te;
     uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
-    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gstart_host, ngraphs);
+    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gstart_host, ngraphs, g->tiles.task_edges,
+                    g->tiles.hub_chunk);
     if (st == AG_OK)
-        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gstart_host, ngraphs);
+        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gstart_host, ngraphs, g->tiles.task_edges,
+                        g->tiles.hub_chunk);
     if (st != AG_OK) {
         ag_graph_release(g);
         return st;
@@ -571,6 +582,7 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
     UP(cudaMemsetAsync(g->hub_cnt, 0, (size_t)nparts * 4 + 16, s));
     if (ngraphs) {
         g->ngraphs = ngraphs;
+        g->gstart_host = new std::vector<uint32_t>(gstart_host, gstart_host + ngraphs + 1);
         g->gstart = (uint32_t *)dev_alloc(g, (size_t)(ngraphs + 1) * 4, &st);
         g->g_u32 = (uint32_t *)dev_alloc(g, (size_t)ngraphs * 4 * 4, &st);
         g->g_f64 = (double *)dev_alloc(g, (size_t)ngraphs * 2 * 8, &st);
@@ -689,6 +701,7 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.out = g->out;
     p.hot_n = g->hot_n;
     p.warm_n = g->warm_n;
+    p.whub = g->tiles.hub_chunk;
     p.ngraphs = g->ngraphs;
     p.gstart = g->gstart;
     if (g->ngraphs) {
@@ -1156,5 +1169,184 @@ extern "C" ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t 
     }
     if (device_ms)
         *device_ms = res.device_ms;
+    return AG_OK;
+}
+
+/* ------------------------------------------------------------ tiles */
+extern "C" ag_status_t ag_graph_get_tiles(ag_graph_t g, ag_tile_config *cfg)
+{
+    if (!g || !cfg)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_get_tiles: NULL argument");
+    *cfg = g->tiles;
+    return AG_OK;
+}
+
+/* re-plan the work lists for a new tile shape; cached launch graphs are
+ * rebuilt on the next launch */
+extern "C" ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cfg)
+{
+    ag_clear_error();
+    if (!g || !cfg)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_set_tiles: NULL argument");
+    if (cfg->task_edges < 32 || cfg->task_edges > AG_WCAP || cfg->hub_chunk < cfg->task_edges ||
+        cfg->hub_chunk > (1u << 20))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_set_tiles: task_edges in [32, %u], hub_chunk in "
+                            "[task_edges, 2^20]", AG_WCAP);
+    cudaStream_t s = g_ctx.stream;
+    ag_status_t st = stream_wait(s, 0);
+    if (st != AG_OK)
+        return st;
+    const uint32_t N = g->N;
+    std::vector<uint32_t> off(N + 1);
+    AG_CUDA(cudaMemcpy(off.data(), g->row_off, (size_t)(N + 1) * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint4> tf, te;
+    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
+    const uint32_t *gs = g->gstart_host ? g->gstart_host->data() : nullptr;
+    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gs, g->ngraphs, cfg->task_edges, cfg->hub_chunk);
+    if (st == AG_OK)
+        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gs, g->ngraphs, cfg->task_edges, cfg->hub_chunk);
+    if (st != AG_OK)
+        return st;
+    uint4 *tdf = nullptr, *tde = nullptr;
+    float *hp = nullptr;
+    uint32_t *hc = nullptr;
+    tdf = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
+    tde = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
+    hp = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    hc = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
+    if (st != AG_OK) {
+        dev_free(tdf);
+        dev_free(tde);
+        dev_free(hp);
+        dev_free(hc);
+        return st;
+    }
+    if (!tf.empty())
+        AG_CUDA(cudaMemcpyAsync(tdf, tf.data(), tf.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    if (!te.empty())
+        AG_CUDA(cudaMemcpyAsync(tde, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    AG_CUDA(cudaMemsetAsync(hc, 0, (size_t)nparts * 4 + 16, s));
+    dev_free(g->tasks_fast);
+    dev_free(g->tasks_exact);
+    dev_free(g->hub_part);
+    dev_free(g->hub_cnt);
+    g->tasks_fast = tdf;
+    g->tasks_exact = tde;
+    g->hub_part = hp;
+    g->hub_cnt = hc;
+    g->ntasks_fast = (uint32_t)tf.size();
+    g->ntasks_exact = (uint32_t)te.size();
+    g->nparts = nparts;
+    g->num_hub_rows = nhub;
+    g->tiles = *cfg;
+    g->hot_n = g->hot_allowed ? std::min<uint32_t>(std::min<uint32_t>(cfg->hot_entries, AG_HOT_MAX), N) & ~63u : 0u;
+    g->warm_n = std::max<uint32_t>(cfg->warm_entries, g->hot_n);
+    g->tiles.hot_entries = g->hot_n;
+    g->tiles.warm_entries = g->warm_n;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            if (g->have_exe[a][b]) {
+                free_exec(&g->exe[a][b]);
+                g->have_exe[a][b] = 0;
+            }
+    return stream_wait(s, 0);
+}
+
+/* Time each candidate tile shape on this graph (FP32, FAST order, a fixed
+ * number of passes that never stop early) and keep the fastest.  Candidates:
+ * item caps {128, 256}, hub chunks {1024, 2048, 4096}, and, when the
+ * shared-memory table is allowed, table sizes {0, 8K, 16K, 24K} entries.
+ * With AG_TUNE_CACHE naming a file, results are read from and appended to it
+ * (one line per graph shape: N E max-in-degree device cap chunk hot warm us). */
+extern "C" ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, double *best_pass_us)
+{
+    ag_clear_error();
+    if (!g)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_autotune: NULL graph");
+    if (passes == 0)
+        passes = 8;
+    char dev_name[256] = "unknown";
+    {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, g_ctx.device) == cudaSuccess) {
+            snprintf(dev_name, sizeof(dev_name), "%s", prop.name);
+            for (char *c = dev_name; *c; ++c)
+                if (*c == ' ')
+                    *c = '_';
+        }
+    }
+    const char *cache = getenv("AG_TUNE_CACHE");
+    if (cache) {
+        FILE *f = fopen(cache, "r");
+        if (f) {
+            unsigned n, e, md, cap, chunk, hot, warm;
+            double us;
+            char dn[256];
+            while (fscanf(f, "%u %u %u %255s %u %u %u %u %lf", &n, &e, &md, dn, &cap, &chunk, &hot, &warm, &us) == 9) {
+                if (n == g->N && e == g->E && md == g->max_in_degree && strcmp(dn, dev_name) == 0) {
+                    ag_tile_config c = {cap, chunk, hot, warm};
+                    fclose(f);
+                    ag_status_t st = ag_graph_set_tiles(g, &c);
+                    if (st == AG_OK) {
+                        if (best)
+                            *best = g->tiles;
+                        if (best_pass_us)
+                            *best_pass_us = us;
+                    }
+                    return st;
+                }
+            }
+            fclose(f);
+        }
+    }
+    std::vector<ag_tile_config> cands;
+    const uint32_t caps[2] = {128, 256};
+    const uint32_t chunks[3] = {1024, 2048, 4096};
+    const uint32_t hots[4] = {0, 8192, 16384, 24576};
+    const int nh = g->hot_allowed ? 4 : 1;
+    for (uint32_t c : caps)
+        for (uint32_t h : chunks)
+            for (int k = 0; k < nh; ++k)
+                cands.push_back({c, h, hots[k], std::max<uint32_t>(65536u, hots[k])});
+    ag_tile_config bestc = g->tiles;
+    double bestus = 1e300;
+    ag_pr_opts o;
+    ag_pr_opts_init(&o);
+    o.quiet = 1;
+    for (const ag_tile_config &c : cands) {
+        ag_status_t st = ag_graph_set_tiles(g, &c);
+        if (st != AG_OK)
+            return st;
+        ag_pr_result r;
+        double us = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            st = ag_pagerank_launch(g, passes, 0.0, &o);
+            if (st == AG_OK)
+                st = ag_pagerank_fetch(g, nullptr, &r, nullptr, nullptr, nullptr, 0);
+            if (st != AG_OK)
+                return st;
+            if (rep == 1 && r.passes)
+                us = r.device_ms * 1e3 / r.passes;
+        }
+        if (us < bestus) {
+            bestus = us;
+            bestc = g->tiles;
+        }
+    }
+    ag_status_t st = ag_graph_set_tiles(g, &bestc);
+    if (st != AG_OK)
+        return st;
+    if (cache) {
+        FILE *f = fopen(cache, "a");
+        if (f) {
+            fprintf(f, "%u %u %u %s %u %u %u %u %.3f\n", g->N, g->E, g->max_in_degree, dev_name, bestc.task_edges,
+                    bestc.hub_chunk, bestc.hot_entries, bestc.warm_entries, bestus);
+            fclose(f);
+        }
+    }
+    if (best)
+        *best = g->tiles;
+    if (best_pass_us)
+        *best_pass_us = bestus;
     return AG_OK;
 }

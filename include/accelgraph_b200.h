@@ -125,12 +125,30 @@ typedef struct ag_graph_info
     uint64_t device_bytes;   /* device memory held by the handle              */
 } ag_graph_info;
 
+/* Work-list and cache shape of a device graph (see ag_autotune). */
+typedef struct ag_tile_config
+{
+    uint32_t task_edges;   /* in-edges per warp item of consecutive rows (32..256) */
+    uint32_t hub_chunk;    /* in-edges per warp for rows split across warps        */
+    uint32_t hot_entries;  /* contributions kept in shared memory per pass          */
+    uint32_t warm_entries; /* contributions below this id may take L1 lines        */
+} ag_tile_config;
+
 /* Copy the inverse CSR (and forward out-degrees) of `graph` to the device
  * and plan the kernel work list.  The handle stays valid until released;
  * the host graph may be freed after the call returns. */
 ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out);
 ag_status_t ag_graph_release(ag_graph_t g);
 ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info);
+ag_status_t ag_graph_get_tiles(ag_graph_t g, ag_tile_config *cfg);
+/* Re-plan the work list for another tile shape (results are unchanged in
+ * EXACT order; FAST-order sums of rows split differently may differ in the
+ * last bits). */
+ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cfg);
+/* Autotuner: time each candidate tile shape for `passes` pull passes on this
+ * graph and keep the fastest; *best and *best_pass_us (may be NULL) receive
+ * it.  AG_TUNE_CACHE names an optional cache file of earlier results. */
+ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, double *best_pass_us);
 
 /* --------------------------------------------------------------- PageRank */
 #define AG_PREC_FP32 0   /* contributions stored in binary32 (reference)     */
@@ -225,6 +243,38 @@ ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t *iterations
  * |r' - r| over all pairs of the last pass. */
 ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32_t k, uint32_t max_iterations,
                         double epsilon, float *ranks, ag_pr_result *result);
+
+/* ------------------------------------------------------- learned warm start */
+/* A small MLP (8 -> 64 -> 64 -> 1, ReLU; bfloat16 weights, binary32
+ * accumulation) that predicts log(un-normalised rank) from per-vertex degree
+ * features, trained and run by this library's own kernels.  Its predictions
+ * only choose the starting ranks: the solve still iterates to the same
+ * epsilon, and uniform starting ranks remain the default. */
+typedef struct ag_mlp_s *ag_mlp_t;
+/* number of binary32 parameters: W1[64][8] b1[64] W2[64][64] b2[64] w3[64] b3 */
+uint32_t ag_mlp_num_params(void);
+ag_status_t ag_mlp_create(uint64_t seed, ag_mlp_t *out);
+ag_status_t ag_mlp_release(ag_mlp_t m);
+ag_status_t ag_mlp_set_params(ag_mlp_t m, const float *params);   /* host array */
+ag_status_t ag_mlp_get_params(ag_mlp_t m, float *params);          /* host array */
+/* Device array of num_vertices x 8 features in caller vertex order:
+ * log1p of in-degree, out-degree, sum of in-neighbours' in-degrees, sum of
+ * their out-degrees, min and max of their out-degrees, sum of their
+ * 1/out-degree, max of their in-degrees. */
+ag_status_t ag_features(ag_graph_t g, float *features);
+/* Y[i] = MLP(X[i]) for n samples; X (n x 8) and Y (n) are device arrays. */
+ag_status_t ag_mlp_forward(ag_mlp_t m, const float *X, uint32_t n, float *Y);
+/* Gradient of the mean squared error of MLP(X) against T (device arrays)
+ * with respect to the parameters (host array of ag_mlp_num_params()
+ * values, may be NULL) and the loss (may be NULL). */
+ag_status_t ag_mlp_gradients(ag_mlp_t m, const float *X, const float *T, uint32_t n, float *grad, float *loss);
+/* Adam on mini-batches of `batch` consecutive samples for `epochs` epochs
+ * (the caller shuffles); *final_loss receives the last batch's loss. */
+ag_status_t ag_mlp_train(ag_mlp_t m, const float *X, const float *T, uint32_t n, uint32_t epochs, uint32_t batch,
+                         float lr, float *final_loss);
+/* Predicted starting ranks for ag_pr_opts.init_ranks (host array of
+ * num_vertices, caller order; never below 1 - damp). */
+ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_ranks);
 
 /* ------------------------------------------------------------------- SpMV */
 #define AG_SPMV_GRAPH_WEIGHTS 0u /* w = uploaded inverse weights (0.0001f if none) */
