@@ -97,7 +97,7 @@ class SPMVStats(C.Structure):
 class PROpts(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("precision", C.c_int32), ("order", C.c_int32), ("quiet", C.c_int32),
-        ("switch_residual", C.c_double), ("init_ranks", f32p),
+        ("switch_residual", C.c_double), ("init_ranks", f32p), ("init_on_device", C.c_int32),
     ]
 
 
@@ -153,6 +153,7 @@ SIGNATURES = [
     ("ag_version", C.c_char_p, []),
     ("ag_init", C.c_int32, [C.c_int]),
     ("ag_stream", C.c_void_p, []),
+    ("ag_set_stream", C.c_int32, [C.c_void_p]),
     ("ag_synchronize", C.c_int32, [C.c_double]),
     ("ag_num_sms", C.c_int, []),
     ("ag_graph_from_edges", GraphP, [C.c_uint32, C.c_uint64, u32p, u32p, f32p, C.c_uint32]),
@@ -191,6 +192,12 @@ SIGNATURES = [
     ("ag_mlp_train", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                  f32p]),
     ("ag_mlp_warm_start", C.c_int32, [C.c_void_p, C.c_void_p, f32p]),
+    ("ag_mlp_warm_start_device", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ag_graph_upload_rows", C.c_int32, [GraphP, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                         C.POINTER(C.c_void_p)]),
+    ("ag_partition_init", C.c_int32, [C.c_void_p, C.c_void_p]),
+    ("ag_partition_pass", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    ("ag_partition_fetch", C.c_int32, [C.c_void_p, f32p]),
     ("ag_ppr_spmm", C.c_int32, [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_double, f32p, C.POINTER(PRResult)]),
     ("ag_spmv_pull_noalloc", C.c_int32, [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_uint32, C.c_void_p]),
@@ -533,9 +540,14 @@ def make_opts(precision=AG_PREC_FP32, order=AG_ORDER_FAST, init_ranks=None, swit
     o.quiet = int(quiet)
     o.switch_residual = switch_residual
     if init_ranks is not None:
-        arr = np.ascontiguousarray(init_ranks, np.float32)
-        o.init_ranks = arr.ctypes.data_as(f32p)
-        o._keep = arr
+        if hasattr(init_ranks, "data_ptr"):  # a device tensor
+            o.init_ranks = C.cast(C.c_void_p(init_ranks.data_ptr()), f32p)
+            o.init_on_device = 1
+            o._keep = init_ranks
+        else:
+            arr = np.ascontiguousarray(init_ranks, np.float32)
+            o.init_ranks = arr.ctypes.data_as(f32p)
+            o._keep = arr
     return o
 
 

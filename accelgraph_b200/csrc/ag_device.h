@@ -108,6 +108,7 @@ typedef struct AgControl
     uint32_t low_passes;      /* passes that read 16-bit contributions      */
     uint32_t stop;            /* 1 once the loop is over (stream launches)  */
     uint32_t fault;           /* nonzero: a bounded device wait ran out     */
+    double last_err_sum;      /* sum of |r' - r| of the last closed pass    */
     uint32_t hist_active[AG_MAX_HISTORY];
     double hist_err[AG_MAX_HISTORY];
     unsigned long long hist_t[AG_MAX_HISTORY];
@@ -134,6 +135,9 @@ typedef struct AgPullParams
     float *rank;           /* PR: ranks; SpMV: y                               */
     const float *x;        /* SpMV input                                       */
     uint32_t whub;         /* in-edges per hub chunk of this work list         */
+    uint32_t c_base;       /* row r's contribution is written at c_base + r
+                              (a rank's slice of a partitioned solve)          */
+    uint32_t norm_n;       /* vertex count ranks are normalised by (0: N)      */
     float *c32_0, *c32_1;
     uint16_t *c16_0, *c16_1;
     float *hub_part;
@@ -146,6 +150,7 @@ typedef struct AgPullParams
     uint32_t use_cond;     /* 1: launched by the CUDA graph's WHILE node      */
     uint32_t hot_n;        /* contributions (ids < hot_n) served from shared
                               memory; a multiple of 64                         */
+    uint32_t hot_n16;      /* entries of the same table in 16-bit passes       */
     uint32_t warm_n;       /* gathers of ids in [hot_n, warm_n) may take L1
                               lines; colder ones bypass L1                     */
     const uint32_t *perm;  /* device row i is caller vertex perm[i]            */

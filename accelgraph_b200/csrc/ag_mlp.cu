@@ -512,6 +512,34 @@ extern "C" ag_status_t ag_mlp_train(ag_mlp_t m, const float *X, const float *T, 
     return AG_OK;
 }
 
+/* predicted un-normalised ranks into a device array (caller order) */
+extern "C" ag_status_t ag_mlp_warm_start_device(ag_graph_t g, ag_mlp_t m, float *init_dev)
+{
+    ag_clear_error();
+    AgGraphView gv;
+    ag_status_t st = ag_rt_graph_view(g, &gv);
+    if (st != AG_OK)
+        return st;
+    if (!m || !init_dev)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_warm_start_device: NULL argument");
+    if (gv.N == 0)
+        return AG_OK;
+    cudaStream_t s = gv.stream;
+    float *X = nullptr;
+    MCHK(cudaMallocAsync((void **)&X, (size_t)gv.N * AG_MLP_IN * sizeof(float), s));
+    st = ag_features(g, X);
+    if (st == AG_OK)
+        st = ag_mlp_forward(m, X, gv.N, init_dev);
+    if (st == AG_OK) {
+        ag_mlp_to_ranks_kernel<<<148 * 8, 256, 0, s>>>(init_dev, gv.N, 1.0f - Damp, init_dev);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            st = ag_set_error(AG_ERR_CUDA, "ag_mlp_warm_start_device: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(X, s);
+    return st;
+}
+
 /* predicted un-normalised ranks (caller order, host) for a warm start */
 extern "C" ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_ranks)
 {

@@ -328,7 +328,7 @@ struct AgPass
         if (PREC != 0 && write_low)
             ag_st_keep_u16(c_out16 + r, ag_f32_to_low<PREC>(c), pol_last);
         else
-            ag_st_keep_f32(c_out32 + r, c, pol_last);
+            ag_st_keep_f32(c_out32 + p.c_base + r, c, pol_last);
     }
 
     /* two 16-byte groups of in-edges per lane: quads qa and qa + 32 (ids and,
@@ -489,7 +489,9 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
      * copy per 32 KB, completing on an mbarrier that every thread waits on
      * (bounded; a wait that runs out is reported through ctl->fault) */
     if (p.hot_n) {
-        const uint32_t bytes = p.hot_n * ps.gather_elem_bytes();
+        /* 16-bit passes hold twice the entries in the same bytes */
+        const uint32_t hn = ps.gather_elem_bytes() == 2 ? p.hot_n16 : p.hot_n;
+        const uint32_t bytes = hn * ps.gather_elem_bytes();
         if (tid == 0) {
             ag_mbar_init(&s_bar, 1);
             ag_mbar_expect_tx(&s_bar, bytes);
@@ -507,7 +509,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         }
         ps.hot32 = reinterpret_cast<const float *>(hot);
         ps.hot16 = reinterpret_cast<const uint16_t *>(hot);
-        ps.hot_n = p.hot_n;
+        ps.hot_n = hn;
     }
 
     /* each warp walks its tasks with a stride of all warps; the first id
@@ -767,6 +769,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 c->switch_pass = P + 1;
         }
         c->prev_err = err;
+        c->last_err_sum = vc->err_acc;
         c->iter = P + 1;
         c->converged = conv ? 1u : 0u;
         const bool cont = !conv && (P + 1 < vc->max_iter);
@@ -794,7 +797,7 @@ __global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams
         if (PREC != 0)
             ag_st_keep_u16(p.c16_0 + v, ag_f32_to_low<PREC>(c), pol_last);
         else
-            ag_st_keep_f32(p.c32_0 + v, c, pol_last);
+            ag_st_keep_f32(p.c32_0 + p.c_base + v, c, pol_last);
     }
     for (uint32_t g = blockIdx.x * AG_SBLK + threadIdx.x; g < p.ngraphs; g += gridDim.x * AG_SBLK) {
         p.g_active[g] = 0;
@@ -834,8 +837,9 @@ __global__ void __launch_bounds__(AG_SBLK) ag_normalize_kernel(const AgPullParam
     __shared__ double sh[AG_SNW];
     const float fN = __uint2float_rn(p.N);
     double s = 0.0;
+    const float fNn = p.norm_n ? __uint2float_rn(p.norm_n) : fN;
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
-        float div = fN;
+        float div = fNn;
         if (p.ngraphs) {
             /* each graph of a union is normalised by its own vertex count */
             uint32_t lo = 0, hi = p.ngraphs;

@@ -94,6 +94,21 @@ extern "C" void *ag_stream(void)
     return (void *)g_ctx.stream;
 }
 
+/* launch on a caller-owned stream from now on (NULL: back to the library's
+ * own stream); the caller keeps the stream alive while the library uses it */
+static cudaStream_t g_own_stream = nullptr;
+extern "C" ag_status_t ag_set_stream(void *stream)
+{
+    ag_status_t st = ctx_ensure(-1);
+    if (st != AG_OK)
+        return st;
+    AG_CUDA(cudaStreamSynchronize(g_ctx.stream));
+    if (!g_own_stream)
+        g_own_stream = g_ctx.stream;
+    g_ctx.stream = stream ? (cudaStream_t)stream : g_own_stream;
+    return AG_OK;
+}
+
 extern "C" int ag_num_sms(void)
 {
     if (ctx_ensure(-1) != AG_OK)
@@ -192,6 +207,8 @@ struct ag_graph_s
     uint32_t warm_n;        /* ids below this may allocate L1 lines          */
     ag_tile_config tiles;   /* work-list and cache shape in use              */
     uint32_t hot_allowed;   /* 0 when uploaded with AG_UPLOAD_NO_SMEM_CACHE  */
+    uint32_t c_base;        /* partitioned solve: this rank's slice offset    */
+    uint32_t norm_n;        /* partitioned solve: global vertex count         */
     std::vector<uint32_t> *gstart_host;
     /* union of independent graphs (ag_multigraph_upload) */
     uint32_t ngraphs;
@@ -355,15 +372,16 @@ static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::
 }
 
 static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
-                               uint32_t ngraphs, ag_graph_t *out);
+                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out);
 
 extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out)
 {
-    return upload_impl(graph, flags, nullptr, 0, out);
+    return upload_impl(graph, flags, nullptr, 0, 0, out);
 }
 
+/* gather_n: length of the vector the in-edges index (0: num_vertices) */
 static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
-                               uint32_t ngraphs, ag_graph_t *out)
+                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out)
 {
     ag_clear_error();
     if (!graph || !out)
@@ -499,11 +517,12 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
     /* every in-edge must name a vertex < N before anything reads through it */
     if (!(flags & AG_UPLOAD_TRUSTED)) {
         uint32_t hflag[2] = {0, 0};
-        UP(ag_validate_ids(ids_old, E, N, g->flag, s));
+        UP(ag_validate_ids(ids_old, E, gather_n ? gather_n : N, g->flag, s));
         UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
         UP(cudaStreamSynchronize(s));
         if (hflag[0]) {
-            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1], N);
+            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1],
+                              gather_n ? gather_n : N);
             if (relabel) {
                 dev_free(off_old);
                 dev_free(ids_old);
@@ -700,6 +719,9 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.inv = g->inv;
     p.out = g->out;
     p.hot_n = g->hot_n;
+    p.c_base = g->c_base;
+    p.norm_n = g->norm_n;
+    p.hot_n16 = std::min<uint32_t>(2 * g->hot_n, g->N & ~63u);
     p.warm_n = g->warm_n;
     p.whub = g->tiles.hub_chunk;
     p.ngraphs = g->ngraphs;
@@ -822,7 +844,8 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
     AgExec *x = &g->exe[prec][exact];
     cudaStream_t s = g_ctx.stream;
     if (o.init_ranks && g->N)
-        AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4, cudaMemcpyHostToDevice, s));
+        AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4,
+                                o.init_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     AgRunConfig run;
     memset(&run, 0, sizeof(run));
     run.max_iter = std::min<uint32_t>(max_iterations, AG_MAX_HISTORY);
@@ -1139,7 +1162,7 @@ extern "C" ag_status_t ag_multigraph_upload(const struct GraphCSR *const *graphs
     u.inverse_sorted_edges_array = &iel;
     /* vertices stay grouped by graph; the union is L2-resident at the sizes
      * it is meant for, so no shared-memory table */
-    return upload_impl(&u, flags | AG_UPLOAD_KEEP_ORDER | AG_UPLOAD_NO_SMEM_CACHE, gstart.data(), count, out);
+    return upload_impl(&u, flags | AG_UPLOAD_KEEP_ORDER | AG_UPLOAD_NO_SMEM_CACHE, gstart.data(), count, 0, out);
 }
 
 extern "C" ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t *iterations, uint32_t *passes,
@@ -1348,5 +1371,164 @@ extern "C" ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config
         *best = g->tiles;
     if (best_pass_us)
         *best_pass_us = bestus;
+    return AG_OK;
+}
+
+/* --------------------------------------------- row-partitioned solves */
+extern "C" ag_status_t ag_graph_upload_rows(const struct GraphCSR *graph, const uint32_t *bounds, uint32_t nranks,
+                                            uint32_t rank, uint32_t slice, uint32_t flags, ag_graph_t *out)
+{
+    ag_clear_error();
+    if (!graph || !bounds || !out || nranks == 0 || rank >= nranks)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_upload_rows: bad argument");
+    const uint32_t N = graph->num_vertices;
+    if (bounds[0] != 0 || bounds[nranks] != N)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_upload_rows: bounds must run from 0 to num_vertices");
+    for (uint32_t r = 0; r < nranks; ++r)
+        if (bounds[r] > bounds[r + 1] || bounds[r + 1] - bounds[r] > slice)
+            return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_upload_rows: range %u exceeds the slice %u", r, slice);
+    if ((uint64_t)slice * nranks > AG_ROW_MASK)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_upload_rows: padded vector too long");
+    const uint32_t rb = bounds[rank], re = bounds[rank + 1], n = re - rb;
+    const struct Vertex *iv = graph->inverse_vertices;
+    const struct EdgeList *iel = graph->inverse_sorted_edges_array;
+    /* padded id of vertex u: owner rank's slice start + offset in the range */
+    std::vector<uint32_t> owner_base(N);
+    for (uint32_t r = 0; r < nranks; ++r)
+        for (uint32_t u = bounds[r]; u < bounds[r + 1]; ++u)
+            owner_base[u] = r * slice + (u - bounds[r]);
+    uint64_t e = 0;
+    for (uint32_t v = rb; v < re; ++v)
+        e += iv->out_degree[v];
+    if (e >= 0xFFFFFFF0ull)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_upload_rows: too many edges in one range");
+    std::vector<uint32_t> indeg(n), idx(n), outdeg(n), nb(e);
+    uint64_t pos = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t v = rb + i, d = iv->out_degree[v], b = iv->edges_idx[v];
+        if ((uint64_t)b + d > graph->num_edges)
+            return ag_set_error(AG_ERR_INVALID_GRAPH, "row %u exceeds the edge array", v);
+        indeg[i] = d;
+        idx[i] = (uint32_t)pos;
+        outdeg[i] = graph->vertices->out_degree[v];
+        for (uint32_t j = 0; j < d; ++j) {
+            const uint32_t u = iel->edges_array_dest[b + j];
+            if (u >= N)
+                return ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge names vertex %u >= %u", u, N);
+            nb[pos + j] = owner_base[u];
+        }
+        pos += d;
+    }
+    struct Vertex fv = {outdeg.data(), indeg.data(), nullptr};
+    struct Vertex lv = {indeg.data(), outdeg.data(), idx.data()};
+    struct EdgeList lel;
+    memset(&lel, 0, sizeof(lel));
+    lel.num_edges = (uint32_t)e;
+    lel.num_vertices = n;
+    lel.edges_array_dest = nb.data();
+    struct GraphCSR lg;
+    memset(&lg, 0, sizeof(lg));
+    lg.num_vertices = n;
+    lg.num_edges = (uint32_t)e;
+    lg.vertices = &fv;
+    lg.inverse_vertices = &lv;
+    lg.inverse_sorted_edges_array = &lel;
+    ag_graph_t g = nullptr;
+    ag_status_t st = upload_impl(&lg, flags | AG_UPLOAD_KEEP_ORDER | AG_UPLOAD_NO_SMEM_CACHE, nullptr, 0,
+                                 slice * nranks, &g);
+    if (st != AG_OK)
+        return st;
+    g->c_base = rank * slice;
+    g->norm_n = N;
+    *out = g;
+    return AG_OK;
+}
+
+/* first contributions of this rank's rows into its slice of c_full
+ * (ranks start at base_pr) */
+extern "C" ag_status_t ag_partition_init(ag_graph_t g, float *c_full)
+{
+    ag_clear_error();
+    if (!g || !c_full || !g->norm_n)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_init: not a row partition");
+    AgPullParams p = base_params(g, 0);
+    p.c32_0 = c_full;
+    AgRunConfig run;
+    memset(&run, 0, sizeof(run));
+    run.max_iter = AG_MAX_HISTORY;
+    run.eps = 0.0;
+    void *args[2] = {&p, &run};
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8));
+    AG_CUDA(cudaLaunchKernel(ag_init_kernel_ptr(0), dim3(grid), dim3(AG_SBLK), args, 0, g_ctx.stream));
+    return AG_OK;
+}
+
+__global__ void ag_partition_setup_kernel(AgControl *c, double eps)
+{
+    c->iter = 0;
+    c->max_iter = AG_MAX_HISTORY;
+    c->active_acc = 0;
+    c->done_ctas = 0;
+    c->err_acc = 0.0;
+    c->eps = eps;
+    c->stop = 0;
+    c->mode_read = 0;
+    c->mode_write = 0;
+}
+
+__global__ void ag_partition_stats_kernel(const AgControl *c, double *stats)
+{
+    stats[0] = (double)c->hist_active[0];
+    stats[1] = c->last_err_sum;
+}
+
+/* one pull pass over this rank's rows: gathers from c_in_full (all ranks'
+ * slices), writes this rank's slice of c_out_full; stats_dev[0] = active
+ * rows, stats_dev[1] = sum of |r' - r| (device doubles, for the caller's
+ * all-reduce).  Enqueued on ag_stream() without waiting. */
+extern "C" ag_status_t ag_partition_pass(ag_graph_t g, const float *c_in_full, float *c_out_full, double epsilon,
+                                         double *stats_dev)
+{
+    ag_clear_error();
+    if (!g || !c_in_full || !c_out_full || !stats_dev || !g->norm_n)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_pass: not a row partition / NULL argument");
+    cudaStream_t s = g_ctx.stream;
+    ag_partition_setup_kernel<<<1, 1, 0, s>>>(g->ctl, epsilon);
+    AG_CUDA(cudaGetLastError());
+    if (g->N) {
+        AgPullParams p = base_params(g, 0);
+        p.c32_0 = const_cast<float *>(c_in_full);
+        p.c32_1 = c_out_full;
+        p.use_cond = 0;
+        const void *k = ag_pull_kernel_ptr(AG_MODE_PR, 0, 0);
+        const unsigned grid = pull_grid(k, p.ntasks, pull_smem(g));
+        void *args[1] = {&p};
+        AG_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, pull_smem(g), s));
+    }
+    ag_partition_stats_kernel<<<1, 1, 0, s>>>(g->ctl, stats_dev);
+    AG_CUDA(cudaGetLastError());
+    return AG_OK;
+}
+
+/* this rank's ranks divided by the global vertex count (host array) */
+extern "C" ag_status_t ag_partition_fetch(ag_graph_t g, float *ranks_local)
+{
+    ag_clear_error();
+    if (!g || !g->norm_n)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_fetch: not a row partition");
+    if (g->N == 0)
+        return AG_OK;
+    AgPullParams p = base_params(g, 0);
+    AG_CUDA(cudaMemsetAsync(&g->ctl->rank_sum, 0, sizeof(double), g_ctx.stream));
+    void *args[1] = {&p};
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8));
+    AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), dim3(grid), dim3(AG_SBLK), args, 0, g_ctx.stream));
+    ag_status_t st = stream_wait(g_ctx.stream, 0);
+    if (st != AG_OK)
+        return st;
+    if (ranks_local)
+        AG_CUDA(cudaMemcpy(ranks_local, g->out, (size_t)g->N * 4, cudaMemcpyDeviceToHost));
     return AG_OK;
 }

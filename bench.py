@@ -52,6 +52,14 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--workload", default="pagerank",
+                   choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart"],
+                   help="pagerank: the headline line (driver contract); the others measure the other forms")
+    p.add_argument("--graphs", type=int, default=256, help="multigraph: number of graphs")
+    p.add_argument("--train-graphs", type=int, default=200, help="warmstart: training graphs")
+    p.add_argument("--k", type=int, default=64, help="ppr: sources")
+    p.add_argument("--mode", default="replicas", choices=["replicas", "rows"],
+                   help="N > 1: independent graphs per rank (replicas) or one graph split by rows (rows)")
     return p.parse_args()
 
 
@@ -319,12 +327,233 @@ def run_b200(a):
         torch.distributed.destroy_process_group()
 
 
+# ---------------------------------------------------------------- forms
+def _gpu_setup():
+    import torch
+    import accelgraph_b200 as ag
+    torch.cuda.set_device(0)
+    ag.check(ag.lib.ag_init(0), "ag_init")
+    return ag
+
+
+def _rel(a, b):
+    import numpy as np
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)), float(np.abs(a - b).max())
+
+
+def run_spmv(a):
+    """SpMV pull, FP32 weights and x uniform in [0,1), one multiply per edge."""
+    import torch
+    ag = _gpu_setup()
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED, flags=ag.AG_BUILD_DEDUPE | ag.AG_BUILD_WEIGHTS)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g, weights=True)
+    x = torch.empty(N, dtype=torch.float32, device="cuda")
+    y = torch.empty(N, dtype=torch.float32, device="cuda")
+    xh = __import__("numpy").empty(N, "float32")
+    ag.lib.ag_fill_uniform(xh.ctypes.data_as(ag.f32p), N, SEED + 1)
+    x.copy_(torch.from_numpy(xh))
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ag.lib.ag_stream(), device=torch.device("cuda", 0))
+    for _ in range(a.warmup):
+        ag.check(ag.lib.ag_spmv_pull_device(dg.h, x.data_ptr(), y.data_ptr(), 0), "spmv")
+    ag.lib.ag_synchronize(0.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps * 10):
+        ag.check(ag.lib.ag_spmv_pull_device(dg.h, x.data_ptr(), y.data_ptr(), 0), "spmv")
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / (a.steps * 10)
+    peak, kind = peak_hbm()
+    alg = 8 * E + 12 * N
+    import oracle
+    yo = oracle.spmv_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.in_weights(), xh)
+    rl, mx = _rel(y.cpu().numpy(), yo)
+    print(json.dumps({"workload": f"spmv pull FP32 weighted, RMAT s{a.scale} ef{a.edge_factor}", "N": N, "E": E,
+                      "ms_per_product": ms, "gteps": E / ms / 1e6, "roofline": {"bytes": alg,
+                      "achieved_gbs": alg / ms / 1e6, "peak": peak, "frac": alg / ms / 1e6 / peak,
+                      "peak_kind": kind}, "rel_l1_vs_oracle": rl, "max_abs_vs_oracle": mx}), flush=True)
+
+
+def run_precision(a):
+    """Time to epsilon and error against the FP64 GPU oracle: FP32 plain vs the
+    BF16 and FP16 contribution forms (switching to FP32 storage)."""
+    ag = _gpu_setup()
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g)
+    r64, p64 = dg.pagerank_f64(5000, 1e-13)
+    out = {"workload": f"PageRank pull to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}", "N": N, "E": E,
+           "fp64_passes": p64}
+    peak, kind = peak_hbm()
+    for name, prec in (("fp32", 0), ("bf16", 1), ("fp16", 2)):
+        dg.launch(a.iterations, a.epsilon, precision=prec)
+        dg.fetch()
+        best = None
+        for _ in range(max(1, a.steps)):
+            r, res, _ = dg.pagerank(a.iterations, a.epsilon, precision=prec)
+            if best is None or res.device_ms < best[1].device_ms:
+                best = (r, res)
+        r, res = best
+        rl, mx = _rel(r, r64)
+        alg = 4 * E + (24 if prec == 0 else 20) * N
+        out[name] = {"device_ms_to_eps": res.device_ms, "passes": res.passes, "iterations": res.iterations,
+                     "switch_pass": res.switch_pass, "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx,
+                     "pass_us": res.device_ms * 1e3 / res.passes,
+                     "roofline_frac": alg / (res.device_ms * 1e-3 / res.passes) / 1e9 / peak}
+    out["speedup_vs_fp32"] = {k: out["fp32"]["device_ms_to_eps"] / out[k]["device_ms_to_eps"]
+                              for k in ("bf16", "fp16")}
+    print(json.dumps(out), flush=True)
+
+
+def run_ppr(a):
+    """k personalized PageRanks as one SpMM per pass (Erdos-Renyi, avg degree
+    16) vs solving the same graph's plain PageRank once per source."""
+    import numpy as np
+    ag = _gpu_setup()
+    n = 1 << a.scale
+    g = ag.Graph.er(n, 16, seed=SEED)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g)
+    rng = np.random.default_rng(SEED + 1000)
+    src = rng.choice(N, size=a.k, replace=False).astype(np.uint32)
+    dg.ppr(src[:2], iterations=3, epsilon=a.epsilon, want_ranks=False)
+    _, res = dg.ppr(src, iterations=a.iterations, epsilon=a.epsilon, want_ranks=False)
+    dg.launch(a.iterations, a.epsilon)
+    dg.fetch()
+    _, res1, _ = dg.pagerank(a.iterations, a.epsilon)
+    peak, kind = peak_hbm()
+    alg = 4 * E + 8 * N + 16 * a.k * N
+    print(json.dumps({"workload": f"personalized PageRank, k={a.k} sources, ER n=2^{a.scale} avg degree 16",
+                      "N": N, "E": E, "ppr_passes": res.passes, "ppr_device_ms": res.device_ms,
+                      "ppr_ms_per_pass": res.device_ms / max(res.passes, 1),
+                      "gteps_all_sources": a.k * E * res.passes / res.device_ms / 1e6,
+                      "per_source_ms": res.device_ms / a.k,
+                      "plain_single_ms": res1.device_ms, "plain_single_passes": res1.passes,
+                      "speedup_per_source_vs_plain": res1.device_ms / (res.device_ms / a.k),
+                      "roofline_model_frac": alg / (res.device_ms * 1e-3 / res.passes) / 1e9 / peak,
+                      "gathered_row_bytes_per_pass": 256 * E}), flush=True)
+
+
+def run_multigraph(a):
+    """Many uneven R-MAT graphs in one launch vs one launch per graph."""
+    import numpy as np
+    ag = _gpu_setup()
+    rng = np.random.default_rng(SEED + 2)
+    gs = []
+    for i in range(a.graphs):
+        gs.append(ag.Graph.rmat(int(rng.integers(10, 17)), int(rng.integers(8, 33)), seed=SEED + 10 + i))
+    E = sum(g.num_edges for g in gs)
+    mg = ag.MultiGraph(gs)
+    best, us = mg.autotune(passes=6)
+    mg.pagerank(a.iterations, a.epsilon)
+    parts, info = mg.pagerank(a.iterations, a.epsilon)
+    one_ms = info["device_ms"]
+    seq_ms = 0.0
+    seq_passes = 0
+    for g in gs:
+        dg = ag.DeviceGraph(g)
+        dg.pagerank(a.iterations, a.epsilon)
+        _, res, _ = dg.pagerank(a.iterations, a.epsilon)
+        seq_ms += res.device_ms
+        seq_passes += res.passes
+        dg.release()
+    print(json.dumps({"workload": f"{a.graphs} R-MAT graphs, scale U[10,16], edge factor U[8,32], eps {a.epsilon:g}",
+                      "total_edges": E, "union_device_ms": one_ms, "union_passes": int(info["passes"].max()),
+                      "sequential_device_ms": seq_ms, "speedup": seq_ms / one_ms,
+                      "edge_passes": int(sum(g.num_edges * int(p) for g, p in zip(gs, info["passes"]))),
+                      "gteps_union": sum(g.num_edges * int(p) for g, p in zip(gs, info["passes"])) / one_ms / 1e6,
+                      "all_converged": bool(info["converged"].all()),
+                      "tiles": {"task_edges": best.task_edges, "hub_chunk": best.hub_chunk}}), flush=True)
+
+
+def run_warmstart(a):
+    """Train the warm-start MLP on this GPU's PageRank results of seeded
+    graphs (scales 14-18), evaluate on a held-out RMAT graph."""
+    import time
+    import numpy as np
+    ag = _gpu_setup()
+    from accelgraph_b200 import warmstart as ws
+    t0 = time.perf_counter()
+    specs = ws.training_graph_specs(count=a.train_graphs, scales=(14, 18), seed=SEED)
+    X, T = ws.build_training_set(specs, per_graph=4096)
+    t_data = time.perf_counter() - t0
+    m = ws.MLP(seed=1)
+    _, loss0 = m.gradients(X, T)
+    t1 = time.perf_counter()
+    loss = m.train(X, T, epochs=60, batch=4096, lr=2e-3)
+    t_train = time.perf_counter() - t1
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=9999)
+    dg = ag.DeviceGraph(g)
+    ws.compare(dg, m, a.iterations, a.epsilon)
+    c = ws.compare(dg, m, a.iterations, a.epsilon)
+    r64, _ = dg.pagerank_f64(5000, 1e-13)
+    eu = _rel(c["ranks_uniform"], r64)
+    ew = _rel(c["ranks_warm"], r64)
+    ei = _rel(c["init"] / g.num_vertices, r64)
+    print(json.dumps({"workload": f"learned warm start, eval RMAT s{a.scale} ef{a.edge_factor} (seed 9999), "
+                                  f"trained on {a.train_graphs} graphs s14-18", "N": g.num_vertices,
+                      "E": g.num_edges, "train_samples": int(X.shape[0]), "loss_initial": loss0,
+                      "loss_final": loss, "data_s": t_data, "train_s": t_train,
+                      "uniform": c["uniform"], "warm": c["warm"],
+                      "speedup_time_to_eps": c["uniform"]["device_ms"] / (c["warm"]["device_ms"] +
+                                                                          c["warm"]["predict_ms"]),
+                      "rel_l1_vs_fp64": {"uniform": eu[0], "warm": ew[0], "prediction_alone": ei[0]}}),
+          flush=True)
+
+
+def run_rows(a):
+    """One graph split by rows over all ranks (NCCL all-gather per pass);
+    strong scaling: the whole job solves one graph."""
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import accelgraph_b200 as ag
+    from accelgraph_b200 import distributed as agd
+    ag.check(ag.lib.ag_init(local), "ag_init")
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
+    for _ in range(max(1, a.warmup)):
+        agd.pagerank_rows_gpu(g, a.iterations, a.epsilon)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    passes = 0
+    for _ in range(a.steps):
+        _, _, info = agd.pagerank_rows_gpu(g, a.iterations, a.epsilon)
+        passes += info["passes"]
+    torch.cuda.synchronize()
+    dist.barrier()
+    t, _ = reduce_time_work(time.perf_counter() - t0, 0.0, device="cuda")
+    value = g.num_edges * passes / t / 1e9
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                          "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": dict(workload_config(a, world), parallelism=f"rows{world}"),
+                          "passes_per_solve": passes // a.steps, "timing": "host clock around whole solves"}),
+              flush=True)
+    dist.destroy_process_group()
+
+
 def main():
     a = parse()
+    if a.impl != "reference" and a.workload == "pagerank" and a.mode == "rows":
+        run_rows(a)
+        return
     if a.impl == "reference":
         run_reference(a)
-    else:
+    elif a.workload == "pagerank":
         run_b200(a)
+    else:
+        {"spmv": run_spmv, "precision": run_precision, "ppr": run_ppr, "multigraph": run_multigraph,
+         "warmstart": run_warmstart}[a.workload](a)
 
 
 if __name__ == "__main__":

@@ -56,6 +56,9 @@ const char *ag_version(void);
 ag_status_t ag_init(int device);
 /* The cudaStream_t (as void*) every launch of this library goes to. */
 void *ag_stream(void);
+/* Make every later launch of this library go to the caller's stream (NULL:
+ * back to the library's own); waits for work already queued. */
+ag_status_t ag_set_stream(void *stream);
 /* Wait for the library stream, polling with a deadline (seconds; <=0 means
  * the AG_WAIT_TIMEOUT_S environment variable, default 600).  Returns
  * AG_ERR_TIMEOUT when the deadline passes with work still queued. */
@@ -170,8 +173,9 @@ typedef struct ag_pr_opts
                                   once a pass's error_total falls below this
                                   (<= 0: 1e-4), or when the residual stops
                                   falling                                     */
-    const float *init_ranks;   /* warm start: num_vertices un-normalised ranks,
-                                  host pointer; NULL = base_pr everywhere     */
+    const float *init_ranks;   /* warm start: num_vertices un-normalised ranks
+                                  in caller order; NULL = base_pr everywhere  */
+    int32_t init_on_device;    /* nonzero: init_ranks is a device pointer     */
 } ag_pr_opts;
 
 typedef struct ag_pr_result
@@ -232,6 +236,27 @@ ag_status_t ag_multigraph_upload(const struct GraphCSR *const *graphs, uint32_t 
 ag_status_t ag_multigraph_fetch(ag_graph_t g, float *ranks, uint32_t *iterations, uint32_t *passes,
                                 uint32_t *converged, double *error_total, double *device_ms);
 
+/* ------------------------------------------------- row-partitioned solves */
+/* One GPU's share of a PageRank solve over several GPUs: the caller's rows
+ * are cut into nranks contiguous ranges bounds[r] .. bounds[r+1] (bounds has
+ * nranks + 1 entries, from 0 to num_vertices; every range at most `slice`
+ * rows), and vertex u of range r is addressed as r * slice + (u - bounds[r])
+ * in the contribution vector of nranks * slice floats that every rank holds
+ * in full.  Each pass reads that vector and writes this rank's slice of the
+ * next one; the caller all-gathers the slices (e.g. NCCL) and all-reduces the
+ * pass statistics between passes.  Row sums are those of a one-GPU solve. */
+ag_status_t ag_graph_upload_rows(const struct GraphCSR *graph, const uint32_t *bounds, uint32_t nranks,
+                                 uint32_t rank, uint32_t slice, uint32_t flags, ag_graph_t *out);
+/* ranks start at base_pr; writes this rank's first contributions into its
+ * slice of c_full (device) */
+ag_status_t ag_partition_init(ag_graph_t g, float *c_full);
+/* one pass; stats_dev (device, 2 doubles) receives this rank's active count
+ * and sum of |r' - r| */
+ag_status_t ag_partition_pass(ag_graph_t g, const float *c_in_full, float *c_out_full, double epsilon,
+                              double *stats_dev);
+/* this rank's ranks / num_vertices (host array of bounds[r+1] - bounds[r]) */
+ag_status_t ag_partition_fetch(ag_graph_t g, float *ranks_local);
+
 /* ------------------------------------------------- batched personalized PR */
 /* Personalized PageRank of k <= 64 source vertices (caller ids) solved
  * together: one pass is one sparse x dense (N x 64) product.  Column i
@@ -275,6 +300,9 @@ ag_status_t ag_mlp_train(ag_mlp_t m, const float *X, const float *T, uint32_t n,
 /* Predicted starting ranks for ag_pr_opts.init_ranks (host array of
  * num_vertices, caller order; never below 1 - damp). */
 ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_ranks);
+/* The same into a device array, enqueued on ag_stream() without waiting:
+ * pass it on with ag_pr_opts.init_on_device = 1. */
+ag_status_t ag_mlp_warm_start_device(ag_graph_t g, ag_mlp_t m, float *init_ranks_device);
 
 /* ------------------------------------------------------------------- SpMV */
 #define AG_SPMV_GRAPH_WEIGHTS 0u /* w = uploaded inverse weights (0.0001f if none) */

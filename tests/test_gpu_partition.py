@@ -1,0 +1,34 @@
+"""Row-partitioned solve on the GPU (NCCL, world size 1 on the one GPU this
+suite has): the partition kernels and the NCCL all-gather plumbing against
+the oracle.  The two-rank loop itself is covered on CPU (test_multirank)."""
+import datetime
+import socket
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_rows_partition_single_rank_matches_oracle(gpu, oracle):
+    ag = gpu
+    import torch
+    import torch.distributed as dist
+
+    from accelgraph_b200 import distributed as agd
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        g = ag.Graph.rmat(13, 16)
+        ranks, (rb, re), info = agd.pagerank_rows_gpu(g, iterations=60, epsilon=1e-4)
+        ref = oracle.pagerank_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(), 60, 1e-4)
+        assert (rb, re) == (0, g.num_vertices)
+        assert info["iterations"] == ref["iterations"]
+        assert np.abs(ranks.astype(np.float64) - ref["ranks"]).sum() / ref["ranks"].sum() <= 1e-5
+    finally:
+        dist.destroy_process_group()
