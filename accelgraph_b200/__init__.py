@@ -156,6 +156,7 @@ SIGNATURES = [
     ("ag_set_stream", C.c_int32, [C.c_void_p]),
     ("ag_synchronize", C.c_int32, [C.c_double]),
     ("ag_num_sms", C.c_int, []),
+    ("ag_probe_gather_rates", C.c_int32, [f64p]),
     ("ag_graph_from_edges", GraphP, [C.c_uint32, C.c_uint64, u32p, u32p, f32p, C.c_uint32]),
     ("ag_graph_rmat", GraphP, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                C.c_uint32]),
@@ -167,6 +168,7 @@ SIGNATURES = [
     ("ag_graph_release", C.c_int32, [C.c_void_p]),
     ("ag_graph_get_info", C.c_int32, [C.c_void_p, C.POINTER(GraphInfo)]),
     ("ag_graph_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
+    ("ag_graph_get_tasks", C.c_int32, [C.c_void_p, C.c_int, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("ag_graph_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
     ("ag_autotune", C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(TileConfig), f64p]),
     ("ag_pr_opts_init", None, [C.POINTER(PROpts)]),
@@ -425,6 +427,10 @@ class DeviceGraph:
         check(lib.ag_graph_get_tiles(self.h, C.byref(t)), "ag_graph_get_tiles")
         return t
 
+    def tasks(self, exact: bool = False) -> np.ndarray:
+        """The pull kernel's work list (items x 4 words, device row numbering)."""
+        return _tasks(self.h, exact)
+
     def set_tiles(self, task_edges=256, hub_chunk=2048, hot_entries=16384, warm_entries=65536) -> None:
         t = TileConfig(task_edges, hub_chunk, hot_entries, warm_entries)
         check(lib.ag_graph_set_tiles(self.h, C.byref(t)), "ag_graph_set_tiles")
@@ -485,6 +491,15 @@ class DeviceGraph:
         return y
 
 
+def _tasks(h, exact: bool) -> np.ndarray:
+    n = C.c_uint32()
+    check(lib.ag_graph_get_tasks(h, int(exact), None, 0, C.byref(n)), "ag_graph_get_tasks")
+    out = np.zeros((n.value, 4), np.uint32)
+    check(lib.ag_graph_get_tasks(h, int(exact), out.ctypes.data_as(u32p), n.value, C.byref(n)),
+          "ag_graph_get_tasks")
+    return out
+
+
 class MultiGraph:
     """Many independent graphs solved in one launch (ag_multigraph_*)."""
 
@@ -513,6 +528,10 @@ class MultiGraph:
         us = C.c_double()
         check(lib.ag_autotune(self.h, passes, C.byref(t), C.byref(us)), "ag_autotune")
         return t, us.value
+
+    def tasks(self, exact: bool = False) -> np.ndarray:
+        """The union's work list (items x 4 words)."""
+        return _tasks(self.h, exact)
 
     def pagerank(self, iterations=100, epsilon=1e-6, order=AG_ORDER_FAST):
         o = make_opts(order=order)

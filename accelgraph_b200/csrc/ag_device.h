@@ -176,9 +176,34 @@ typedef struct AgGraphView
     cudaStream_t stream;
 } AgGraphView;
 
+/* device planner of the work lists (ag_plan.cu): hub chunks, long rows not
+ * split, row items, split rows */
+typedef struct AgPlanTotals
+{
+    uint32_t hub_items, long_items, row_items, hub_rows;
+} AgPlanTotals;
+
+typedef struct AgPlanState
+{
+    const uint32_t *row_off, *gstart;
+    uint32_t n, cap, whub, ngraphs, nseg;
+    void *scratch;
+    uint32_t *scan;
+} AgPlanState;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* count items per segment and copy the four totals to totals_host (the copy
+ * is stream-ordered: wait on the stream before reading them) */
+cudaError_t ag_plan_count(const uint32_t *row_off, uint32_t n, uint32_t cap, uint32_t whub, const uint32_t *gstart,
+                          uint32_t ngraphs, AgPlanState *ps, uint32_t *totals_host, cudaStream_t s);
+/* write both lists: fast holds hub + long + row items, exact holds
+ * long + split rows + row items */
+cudaError_t ag_plan_write(AgPlanState *ps, const uint32_t *totals, uint4 *fast, uint4 *exact, cudaStream_t s);
+void ag_plan_release(AgPlanState *ps, cudaStream_t s);
+cudaError_t ag_set_u32(uint32_t *p, uint32_t v, cudaStream_t s);
 
 struct ag_graph_s;
 int32_t ag_rt_graph_view(struct ag_graph_s *g, AgGraphView *v);

@@ -388,32 +388,58 @@ struct AgPass
         v[7] = in[7] ? gather(q.b.w, q.wb.w) : 0.f;
     }
 
+    /* first round of a warp stage, issued ahead of its use: the lane's
+     * values of quads (eb >> 2) + lane and + 32 (zero outside [eb, ee)) */
+    __device__ __forceinline__ void stage_issue(const Pair &first, uint32_t eb, uint32_t ee, uint32_t lane,
+                                                float *v) const
+    {
+        bool in[8];
+        gather8(first, (eb >> 2) + lane, eb, ee, v, in);
+    }
+
     /* warp stage: vals[j - eb] = gathered value of in-edge j, j in [eb, ee).
-     * `first` holds the lane's first pair (loaded a task ahead); a lane
-     * gathers all eight values of a pair before it stores any of them. */
-    __device__ __forceinline__ void stage(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
-                                          const Pair &first) const
+     * `v` holds the lane's first round (stage_issue); the later rounds, if
+     * any, load their ids and gather here.  A lane gathers all eight values
+     * of a round before it stores any of them. */
+    __device__ __forceinline__ void stage_commit(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
+                                                 const float *v) const
     {
         const uint32_t q1 = (ee + 3u) >> 2;
         uint32_t qa = (eb >> 2) + lane;
-        Pair cur = first;
-        while (qa < q1) {
-            float v[8];
+        {
+            const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (ja + k >= eb && ja + k < ee)
+                    vals[ja + k - eb] = v[k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (jb + k >= eb && jb + k < ee)
+                    vals[jb + k - eb] = v[4 + k];
+        }
+        for (qa += 64; qa < q1; qa += 64) {
+            const Pair cur = load_pair(qa, q1);
+            float w[8];
             bool in[8];
-            gather8(cur, qa, eb, ee, v, in);
+            gather8(cur, qa, eb, ee, w, in);
             const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
                 if (in[k])
-                    vals[ja + k - eb] = v[k];
+                    vals[ja + k - eb] = w[k];
 #pragma unroll
             for (int k = 0; k < 4; ++k)
                 if (in[4 + k])
-                    vals[jb + k - eb] = v[4 + k];
-            qa += 64;
-            if (qa < q1)
-                cur = load_pair(qa, q1);
+                    vals[jb + k - eb] = w[4 + k];
         }
+    }
+
+    __device__ __forceinline__ void stage(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
+                                          const Pair &first) const
+    {
+        float v[8];
+        stage_issue(first, eb, ee, lane, v);
+        stage_commit(vals, eb, ee, lane, v);
     }
 
     /* warp-strided partial sum of in-edges [eb, ee) straight from memory;
@@ -422,21 +448,48 @@ struct AgPass
     __device__ __forceinline__ float strided_partial(uint32_t eb, uint32_t ee, uint32_t lane,
                                                      const Pair &first) const
     {
+        /* two rounds of gathers in flight: the values of round k are added
+         * while those of round k + 1 travel and the ids of round k + 2 load.
+         * In-edges outside [eb, ee) gather nothing and add +0.0, which leaves
+         * this (tree-ordered) partial sum unchanged. */
         const uint32_t q1 = (ee + 3u) >> 2;
         uint32_t qa = (eb >> 2) + lane;
-        Pair cur = first;
         float s = 0.0f;
-        while (qa < q1) {
-            const Pair nxt = load_pair(qa + 64, q1);
-            float v[8];
-            bool in[8];
-            gather8(cur, qa, eb, ee, v, in);
+        if (MODE == AG_MODE_SPMV) {
+            /* weighted pairs take twice the registers: one round in flight */
+            Pair cur = first;
+            while (qa < q1) {
+                const Pair nx = load_pair(qa + 64, q1);
+                float v[8];
+                bool in[8];
+                gather8(cur, qa, eb, ee, v, in);
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                if (in[k])
-                    s = __fadd_rn(s, v[k]);
-            cur = nxt;
-            qa += 64;
+                for (int k = 0; k < 8; ++k)
+                    if (in[k])
+                        s = __fadd_rn(s, v[k]);
+                cur = nx;
+                qa += 64;
+            }
+            return s;
+        }
+        if (qa >= q1)
+            return s;
+        float v[8];
+        bool in[8];
+        gather8(first, qa, eb, ee, v, in);
+        Pair nxt = load_pair(qa + 64, q1);
+        while (qa < q1) {
+            const uint32_t qn = qa + 64;
+            const Pair nn = load_pair(qn + 64, q1);
+            float vn[8];
+            gather8(nxt, qn, eb, ee, vn, in);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                s = __fadd_rn(s, v[k]);
+                v[k] = vn[k];
+            }
+            nxt = nn;
+            qa = qn;
         }
         return s;
     }

@@ -313,61 +313,74 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     return AG_OK;
 }
 
-/* Work list of the fused pull kernel (one item per warp).  FAST order:
- * rows longer than AG_WCAP run on their own warp, rows longer than AG_WHUB
- * are split into AG_WHUB-edge chunks; EXACT order keeps every long row on one
- * warp.  Everything else is packed into items of <= AG_WROWS consecutive rows
- * holding <= AG_WCAP in-edges.  Heavy items come first so that they start
- * early. */
-static ag_status_t plan_tasks(const uint32_t *off, uint32_t N, bool exact, std::vector<uint4> &out,
-                              uint32_t *nparts, uint32_t *nhub, const uint32_t *gstart, uint32_t ngraphs,
-                              uint32_t cap, uint32_t whub)
+/* Work lists of the fused pull kernel (one item per warp), planned on the
+ * device from the device row offsets (ag_plan.cu).  FAST order: rows longer
+ * than `cap` in-edges run on their own warp, rows longer than `whub` are split
+ * into whub-edge chunks; EXACT order keeps every long row on one warp.  Other
+ * rows are packed into items of <= AG_WROWS consecutive rows holding <= cap
+ * in-edges.  Heavy items come first so that they start early.  On success the
+ * lists replace the graph's current ones. */
+static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
 {
-    std::vector<uint4> hubs, longs, rows;
-    uint32_t pbase = 0, nh = 0;
-    uint32_t r = 0;
-    uint32_t gnext = 0; /* rows items never cross the start of a graph */
+    const uint32_t N = g->N;
     if (N > AG_ROW_MASK)
         return ag_set_error(AG_ERR_INVALID_GRAPH, "%u vertices exceed the 2^30 row limit", N);
-    while (r < N) {
-        const uint32_t d = off[r + 1] - off[r];
-        if (d > cap) {
-            if (!exact && d > whub) {
-                const uint32_t nch = (d + whub - 1) / whub;
-                if (nch >= (1u << (32 - AG_SLOT_BITS)) || pbase + nch > AG_SLOT_MASK)
-                    return ag_set_error(AG_ERR_UNSUPPORTED, "row %u: %u in-edges exceed the hub split limits", r, d);
-                for (uint32_t c = 0; c < nch; ++c) {
-                    const uint32_t cb = off[r] + c * whub;
-                    const uint32_t ce = std::min(off[r + 1], cb + whub);
-                    hubs.push_back(make_uint4((AG_T_HUB << 30) | r, pbase | (c << AG_SLOT_BITS), cb, ce));
-                }
-                pbase += nch;
-                ++nh;
-            } else {
-                longs.push_back(make_uint4((AG_T_LONG << 30) | r, r + 1, off[r], off[r + 1]));
-            }
-            ++r;
-            continue;
-        }
-        const uint32_t rb = r, eb = off[r];
-        while (gstart && gnext <= ngraphs && gstart[gnext] <= rb)
-            ++gnext;
-        const uint32_t limit = (gstart && gnext <= ngraphs) ? gstart[gnext] : N;
-        while (r < N && r < limit && r - rb < AG_WROWS) {
-            const uint32_t dr = off[r + 1] - off[r];
-            if (dr > cap || off[r + 1] - eb > cap)
-                break;
-            ++r;
-        }
-        rows.push_back(make_uint4((AG_T_ROWS << 30) | rb, r, eb, off[r]));
+    if (((uint64_t)g->max_in_degree + whub - 1) / whub >= (1u << (32 - AG_SLOT_BITS)))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "a row of %u in-edges exceeds the hub split limits",
+                            g->max_in_degree);
+    cudaStream_t s = g_ctx.stream;
+    AgPlanState ps;
+    uint32_t tot[4] = {0, 0, 0, 0};
+    cudaError_t e = ag_plan_count(g->row_off, N, cap, whub, g->gstart, g->ngraphs, &ps, tot, s);
+    ag_status_t st = AG_OK;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ag_plan_release(&ps, s);
+        return ag_set_error(AG_ERR_CUDA, "work-list planning failed: %s", cudaGetErrorString(e));
     }
-    out.clear();
-    out.reserve(hubs.size() + longs.size() + rows.size());
-    out.insert(out.end(), hubs.begin(), hubs.end());
-    out.insert(out.end(), longs.begin(), longs.end());
-    out.insert(out.end(), rows.begin(), rows.end());
-    *nparts = pbase;
-    *nhub = nh;
+    st = stream_wait(s, 0);
+    if (st != AG_OK) {
+        ag_plan_release(&ps, s);
+        return st;
+    }
+    if (tot[0] > AG_SLOT_MASK) {
+        ag_plan_release(&ps, s);
+        return ag_set_error(AG_ERR_UNSUPPORTED, "%u hub chunks exceed the hub split limits", tot[0]);
+    }
+    const uint32_t nf = tot[0] + tot[1] + tot[2], ne = tot[1] + tot[3] + tot[2];
+    uint4 *tdf = (uint4 *)dev_alloc(g, (size_t)nf * sizeof(uint4), &st);
+    uint4 *tde = (uint4 *)dev_alloc(g, (size_t)ne * sizeof(uint4), &st);
+    float *hp = (float *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
+    uint32_t *hc = (uint32_t *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
+    if (st == AG_OK) {
+        e = ag_plan_write(&ps, tot, tdf, tde, s);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(hc, 0, (size_t)tot[0] * 4 + 16, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = ag_set_error(AG_ERR_CUDA, "work-list planning failed: %s", cudaGetErrorString(e));
+        }
+    }
+    ag_plan_release(&ps, s);
+    if (st != AG_OK) {
+        dev_free(tdf);
+        dev_free(tde);
+        dev_free(hp);
+        dev_free(hc);
+        return st;
+    }
+    dev_free(g->tasks_fast);
+    dev_free(g->tasks_exact);
+    dev_free(g->hub_part);
+    dev_free(g->hub_cnt);
+    g->tasks_fast = tdf;
+    g->tasks_exact = tde;
+    g->hub_part = hp;
+    g->hub_cnt = hc;
+    g->ntasks_fast = nf;
+    g->ntasks_exact = ne;
+    g->nparts = tot[0];
+    g->num_hub_rows = tot[3];
     return AG_OK;
 }
 
@@ -404,7 +417,6 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
 
     /* host view of the inverse rows: contiguous rows are uploaded as they
      * are; any other layout (gaps, overlap, reordering) is repacked */
-    std::vector<uint32_t> off(N + 1);
     bool contiguous = true;
     uint64_t total = 0;
     uint32_t maxd = 0;
@@ -415,7 +427,6 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         if ((uint64_t)iv->edges_idx[v] + d > E)
             return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: row %u [%u, +%u) exceeds %u edges", v,
                                 iv->edges_idx[v], d, E);
-        off[v] = (uint32_t)total;
         total += d;
         if (d > maxd)
             maxd = d;
@@ -423,7 +434,18 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
     if (total != E)
         return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: in-degrees sum to %llu, expected %u edges",
                             (unsigned long long)total, E);
-    off[N] = E;
+    /* row starts: the caller's own array when its rows are contiguous (its
+     * N entries plus E), else a packed copy */
+    std::vector<uint32_t> off;
+    if (!contiguous) {
+        off.resize((size_t)N + 1);
+        uint32_t o = 0;
+        for (uint32_t v = 0; v < N; ++v) {
+            off[v] = o;
+            o += iv->out_degree[v];
+        }
+        off[N] = E;
+    }
 
     ag_graph_s *g = new ag_graph_s();
     memset((void *)g, 0, sizeof(*g));
@@ -485,7 +507,13 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
             return st;                                                                           \
         }                                                                                        \
     } while (0)
-    UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
+    if (contiguous) {
+        if (N)
+            UP(cudaMemcpyAsync(off_old, iv->edges_idx, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        UP(ag_set_u32(off_old + N, E, s));
+    } else {
+        UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
+    }
     UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
     if (contiguous) {
         if (E)
@@ -539,9 +567,6 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
             UP(cudaMemsetAsync(g->w + E, 0, (size_t)(g->E4 - E) * 4, s));
         UP(ag_relabel_by_out_degree(off_old, ids_old, w_old, outdeg_old, N, E, g->perm, g->inv, g->row_off, g->ids,
                                     g->w, g->outdeg, s));
-        /* the planner walks the device row offsets */
-        UP(cudaMemcpyAsync(off.data(), g->row_off, (size_t)(N + 1) * 4, cudaMemcpyDeviceToHost, s));
-        UP(cudaStreamSynchronize(s));
         dev_free(off_old);
         dev_free(ids_old);
         dev_free(outdeg_old);
@@ -571,34 +596,6 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         g->tiles.warm_entries = g->warm_n;
     }
 
-    std::vector<uint4> tf, te;
-    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
-    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gstart_host, ngraphs, g->tiles.task_edges,
-                    g->tiles.hub_chunk);
-    if (st == AG_OK)
-        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gstart_host, ngraphs, g->tiles.task_edges,
-                        g->tiles.hub_chunk);
-    if (st != AG_OK) {
-        ag_graph_release(g);
-        return st;
-    }
-    g->ntasks_fast = (uint32_t)tf.size();
-    g->ntasks_exact = (uint32_t)te.size();
-    g->nparts = nparts;
-    g->num_hub_rows = nhub;
-    g->tasks_fast = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
-    g->tasks_exact = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
-    g->hub_part = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
-    g->hub_cnt = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
-    if (st != AG_OK) {
-        ag_graph_release(g);
-        return st;
-    }
-    if (!tf.empty())
-        UP(cudaMemcpyAsync(g->tasks_fast, tf.data(), tf.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
-    if (!te.empty())
-        UP(cudaMemcpyAsync(g->tasks_exact, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
-    UP(cudaMemsetAsync(g->hub_cnt, 0, (size_t)nparts * 4 + 16, s));
     if (ngraphs) {
         g->ngraphs = ngraphs;
         g->gstart_host = new std::vector<uint32_t>(gstart_host, gstart_host + ngraphs + 1);
@@ -610,6 +607,11 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
             return st;
         }
         UP(cudaMemcpyAsync(g->gstart, gstart_host, (size_t)(ngraphs + 1) * 4, cudaMemcpyHostToDevice, s));
+    }
+    st = plan_device(g, g->tiles.task_edges, g->tiles.hub_chunk);
+    if (st != AG_OK) {
+        ag_graph_release(g);
+        return st;
     }
     UP(cudaEventCreate(&g->ev0));
     UP(cudaEventCreate(&g->ev1));
@@ -1204,6 +1206,25 @@ extern "C" ag_status_t ag_graph_get_tiles(ag_graph_t g, ag_tile_config *cfg)
     return AG_OK;
 }
 
+extern "C" ag_status_t ag_graph_get_tasks(ag_graph_t g, int exact, uint32_t *items, uint32_t capacity,
+                                         uint32_t *count)
+{
+    ag_clear_error();
+    if (!g || !count || (capacity && !items))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_get_tasks: NULL argument");
+    const uint32_t n = exact ? g->ntasks_exact : g->ntasks_fast;
+    *count = n;
+    const uint32_t k = std::min(n, capacity);
+    if (k) {
+        ag_status_t st = stream_wait(g_ctx.stream, 0);
+        if (st != AG_OK)
+            return st;
+        AG_CUDA(cudaMemcpy(items, exact ? g->tasks_exact : g->tasks_fast, (size_t)k * sizeof(uint4),
+                           cudaMemcpyDeviceToHost));
+    }
+    return AG_OK;
+}
+
 /* re-plan the work lists for a new tile shape; cached launch graphs are
  * rebuilt on the next launch */
 extern "C" ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cfg)
@@ -1220,47 +1241,9 @@ extern "C" ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cf
     if (st != AG_OK)
         return st;
     const uint32_t N = g->N;
-    std::vector<uint32_t> off(N + 1);
-    AG_CUDA(cudaMemcpy(off.data(), g->row_off, (size_t)(N + 1) * 4, cudaMemcpyDeviceToHost));
-    std::vector<uint4> tf, te;
-    uint32_t nparts = 0, nhub = 0, np2 = 0, nh2 = 0;
-    const uint32_t *gs = g->gstart_host ? g->gstart_host->data() : nullptr;
-    st = plan_tasks(off.data(), N, false, tf, &nparts, &nhub, gs, g->ngraphs, cfg->task_edges, cfg->hub_chunk);
-    if (st == AG_OK)
-        st = plan_tasks(off.data(), N, true, te, &np2, &nh2, gs, g->ngraphs, cfg->task_edges, cfg->hub_chunk);
+    st = plan_device(g, cfg->task_edges, cfg->hub_chunk);
     if (st != AG_OK)
         return st;
-    uint4 *tdf = nullptr, *tde = nullptr;
-    float *hp = nullptr;
-    uint32_t *hc = nullptr;
-    tdf = (uint4 *)dev_alloc(g, tf.size() * sizeof(uint4), &st);
-    tde = (uint4 *)dev_alloc(g, te.size() * sizeof(uint4), &st);
-    hp = (float *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
-    hc = (uint32_t *)dev_alloc(g, (size_t)nparts * 4 + 16, &st);
-    if (st != AG_OK) {
-        dev_free(tdf);
-        dev_free(tde);
-        dev_free(hp);
-        dev_free(hc);
-        return st;
-    }
-    if (!tf.empty())
-        AG_CUDA(cudaMemcpyAsync(tdf, tf.data(), tf.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
-    if (!te.empty())
-        AG_CUDA(cudaMemcpyAsync(tde, te.data(), te.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
-    AG_CUDA(cudaMemsetAsync(hc, 0, (size_t)nparts * 4 + 16, s));
-    dev_free(g->tasks_fast);
-    dev_free(g->tasks_exact);
-    dev_free(g->hub_part);
-    dev_free(g->hub_cnt);
-    g->tasks_fast = tdf;
-    g->tasks_exact = tde;
-    g->hub_part = hp;
-    g->hub_cnt = hc;
-    g->ntasks_fast = (uint32_t)tf.size();
-    g->ntasks_exact = (uint32_t)te.size();
-    g->nparts = nparts;
-    g->num_hub_rows = nhub;
     g->tiles = *cfg;
     g->hot_n = g->hot_allowed ? std::min<uint32_t>(std::min<uint32_t>(cfg->hot_entries, AG_HOT_MAX), N) & ~63u : 0u;
     g->warm_n = std::max<uint32_t>(cfg->warm_entries, g->hot_n);

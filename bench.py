@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--workload", default="pagerank",
-                   choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart"],
+                   choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe"],
                    help="pagerank: the headline line (driver contract); the others measure the other forms")
     p.add_argument("--graphs", type=int, default=256, help="multigraph: number of graphs")
     p.add_argument("--train-graphs", type=int, default=200, help="warmstart: training graphs")
@@ -542,6 +542,21 @@ def run_rows(a):
     dist.destroy_process_group()
 
 
+def run_gather_probe(a):
+    """Random 4-byte gather rates of this device (ag_probe_gather_rates)."""
+    import numpy as np
+    ag = _gpu_setup()
+    r = np.zeros(6)
+    ag.check(ag.lib.ag_probe_gather_rates(r.ctypes.data_as(ag.f64p)), "ag_probe_gather_rates")
+    names = ["shared_64KB", "global_L1_256KB", "global_L2_64MB", "global_HBM_256MB", "texture_L2_64MB",
+             "cluster_shared_8x160KB"]
+    sms = ag.lib.ag_num_sms()
+    print(json.dumps({"workload": "random 4-byte gathers, 1024 threads/SM, 8 in flight per thread",
+                      "gathers_per_s": dict(zip(names, r.tolist())),
+                      "per_clock_per_sm_at_1.9GHz": dict(zip(names, (r / sms / 1.9e9).round(3).tolist()))}),
+          flush=True)
+
+
 def main():
     a = parse()
     if a.impl != "reference" and a.workload == "pagerank" and a.mode == "rows":
@@ -553,7 +568,7 @@ def main():
         run_b200(a)
     else:
         {"spmv": run_spmv, "precision": run_precision, "ppr": run_ppr, "multigraph": run_multigraph,
-         "warmstart": run_warmstart}[a.workload](a)
+         "warmstart": run_warmstart, "gather-probe": run_gather_probe}[a.workload](a)
 
 
 if __name__ == "__main__":

@@ -65,6 +65,11 @@ ag_status_t ag_set_stream(void *stream);
 ag_status_t ag_synchronize(double timeout_s);
 /* Number of streaming multiprocessors of the library's device (0 if none). */
 int ag_num_sms(void);
+/* Device probe of random 4-byte gather rates (gathers per second), the
+ * quantity that bounds a pull pass: rates[0..5] = shared memory, L1-resident,
+ * L2-resident, HBM-resident, L2-resident through textures, distributed shared
+ * memory of an 8-CTA cluster.  Allocates and frees 256 MB. */
+ag_status_t ag_probe_gather_rates(double *rates);
 
 /* ------------------------------------------------- host graph substrate */
 #define AG_BUILD_DEDUPE   1u  /* drop self loops and duplicate edges; implies SORT */
@@ -144,6 +149,12 @@ ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_gra
 ag_status_t ag_graph_release(ag_graph_t g);
 ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info);
 ag_status_t ag_graph_get_tiles(ag_graph_t g, ag_tile_config *cfg);
+/* Copy a work list of the pull kernel (exact = 0: FAST order, 1: EXACT
+ * order) into `items` as 4 words per item (kind << 30 | first row, end row
+ * or hub slot, first in-edge, end in-edge), in device row numbering;
+ * *count receives the list's length.  At most `capacity` items are copied
+ * (items may be NULL with capacity 0 to ask for the length). */
+ag_status_t ag_graph_get_tasks(ag_graph_t g, int exact, uint32_t *items, uint32_t capacity, uint32_t *count);
 /* Re-plan the work list for another tile shape (results are unchanged in
  * EXACT order; FAST-order sums of rows split differently may differ in the
  * last bits). */
