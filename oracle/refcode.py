@@ -1,0 +1,111 @@
+"""ctypes binding of the reference's own pull calls, compiled here
+(oracle/_ref/libref_pagerank.so; TEST INFRASTRUCTURE ONLY).
+
+`make -C oracle ref` compiles the reference's unmodified
+02_capi_graph/src/algorithms/capi/pageRank.c and SPMV.c against stand-ins
+for the absent OpenGraph and libcxl headers (oracle/refstubs/) and links
+them with a CPU emulation of the accelerator's pull gather
+(oracle/refstubs/afu_emulator.c).  pageRankPullGraphCSR and SPMVPullGraphCSR
+then run the reference's own host code: its starting ranks, contribution
+loop, update, residual, stop test, normalisation, SpMV input vector and
+checksum, with the gather done by the emulation (stream-order binary32 sums,
+the compute units' semantics).  The library is built where the reference
+source is present; elsewhere `available()` is False and the tests that use
+it skip.  The GraphCSR and Arguments structures are the ones the reference
+headers declare, which this repository's include/ mirrors field for field.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_ref" / "libref_pagerank.so"
+REF_SOURCE = Path("/root/reference/02_capi_graph/src/algorithms/capi/pageRank.c")
+
+
+class _PageRankStats(C.Structure):
+    _fields_ = [("damp", C.c_float), ("base_pr", C.c_float), ("iterations", C.c_uint32),
+                ("num_vertices", C.c_uint32), ("activeVertices", C.c_uint32),
+                ("realRanks", C.POINTER(C.c_uint32)), ("pageRanks", C.POINTER(C.c_float)),
+                ("time_total", C.c_double), ("error_total", C.c_double)]
+
+
+class _SPMVStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("arguments", C.c_void_p), ("num_vertices", C.c_uint32),
+                ("vector_output", C.POINTER(C.c_float)), ("vector_input", C.POINTER(C.c_float)),
+                ("time_total", C.c_double)]
+
+
+def build() -> bool:
+    """Compile the library when the reference source is present and the
+    library is missing or older than its recipe; True when it exists."""
+    if REF_SOURCE.exists():
+        deps = [HERE / "Makefile", HERE / "refstubs" / "afu_emulator.c", HERE / "refstubs" / "exports.map",
+                *sorted((HERE / "refstubs").glob("*.h"))]
+        if not LIB.exists() or LIB.stat().st_mtime < max(p.stat().st_mtime for p in deps):
+            subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    return LIB.exists()
+
+
+_lib = None
+
+
+def available() -> bool:
+    return _load() is not None
+
+
+def _load():
+    global _lib
+    if _lib is None and build():
+        lib = C.CDLL(str(LIB))
+        lib.pageRankPullGraphCSR.restype = C.POINTER(_PageRankStats)
+        lib.pageRankPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
+        lib.freePageRankStats.argtypes = [C.POINTER(_PageRankStats)]
+        lib.SPMVPullGraphCSR.restype = C.POINTER(_SPMVStats)
+        lib.SPMVPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
+        lib.freeSPMVStats.argtypes = [C.POINTER(_SPMVStats)]
+        lib.refemu_set_kernel.argtypes = [C.c_int]
+        lib.refemu_gathers.restype = C.c_uint64
+        _lib = lib
+    return _lib
+
+
+def pagerank_pull(arguments_ptr, graph_ptr, num_vertices: int):
+    """Run the reference's pageRankPullGraphCSR on a GraphCSR (pointer) with
+    a struct Arguments (pointer).  Returns ranks (normalised, float32),
+    iterations (the reference's stats->iterations), error_total, and the
+    number of gathers the emulated accelerator ran."""
+    import numpy as np
+    lib = _load()
+    lib.refemu_set_kernel(0)
+    g0 = lib.refemu_gathers()
+    st = lib.pageRankPullGraphCSR(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
+    try:
+        s = st.contents
+        ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
+            np.zeros(0, np.float32)
+        out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total),
+               "gathers": int(lib.refemu_gathers() - g0), "damp": float(s.damp), "base_pr": float(s.base_pr)}
+    finally:
+        lib.freePageRankStats(st)
+    return out
+
+
+def spmv_pull(arguments_ptr, graph_ptr, num_vertices: int):
+    """Run the reference's SPMVPullGraphCSR: returns its input vector, its
+    output vector and its iteration count."""
+    import numpy as np
+    lib = _load()
+    lib.refemu_set_kernel(1)
+    st = lib.SPMVPullGraphCSR(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
+    try:
+        s = st.contents
+        n = num_vertices
+        out = {"x": np.ctypeslib.as_array(s.vector_input, shape=(n,)).copy() if n else np.zeros(0, np.float32),
+               "y": np.ctypeslib.as_array(s.vector_output, shape=(n,)).copy() if n else np.zeros(0, np.float32),
+               "iterations": int(s.iterations)}
+    finally:
+        lib.freeSPMVStats(st)
+    return out

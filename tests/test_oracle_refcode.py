@@ -1,0 +1,57 @@
+"""The oracle against the reference's own host code.
+
+oracle/refcode runs the reference's unmodified pageRankPullGraphCSR and
+SPMVPullGraphCSR (pageRank.c:942-1109, SPMV.c:622-751, compiled here with a
+CPU emulation of the accelerator gather).  The oracle's restatement of those
+loops must give the same ranks bit for bit and the same iteration counts; the
+SpMV input vector and product must match bit for bit too.  Skipped where the
+reference source was not available to compile the library."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def refcode():
+    from oracle import refcode as rc
+    if not rc.available():
+        pytest.skip("reference pull calls not compiled (reference source absent)")
+    return rc
+
+
+def _graphs(ag):
+    yield "rmat10_ef16", ag.Graph.rmat(10, 16, seed=3)
+    yield "rmat12_ef8", ag.Graph.rmat(12, 8, seed=4)
+    yield "er4096_d8", ag.Graph.er(4096, 8, seed=5)
+    # a graph with isolated vertices, sinks and sources
+    src = np.array([0, 0, 1, 2, 2, 3, 5, 5, 5, 7, 8, 8], np.uint32)
+    dst = np.array([1, 2, 2, 0, 3, 3, 1, 2, 4, 7, 9, 0], np.uint32)
+    yield "small_mixed", ag.Graph.from_edges(11, src, dst)
+
+
+@pytest.mark.parametrize("iterations,epsilon", [(20, 1e-4), (200, 1e-6), (3, 1e-12), (300, 0.0)])
+def test_oracle_pagerank_equals_reference_code(ag, oracle, refcode, iterations, epsilon):
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(iterations, epsilon)
+        ref = refcode.pagerank_pull(C.byref(args), g.ptr, g.num_vertices)
+        mine = oracle.pagerank_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(),
+                                    iterations, epsilon)
+        assert ref["damp"] == np.float32(0.85) and ref["base_pr"] == np.float32(1.0) - np.float32(0.85)
+        assert ref["iterations"] == mine["iterations"], name
+        assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
+        # the reference sums the residual with an OpenMP reduction (any order)
+        assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
+        # one gather per pass run: the converging pass counts
+        assert ref["gathers"] == mine["passes"], name
+
+
+def test_oracle_spmv_equals_reference_code(ag, oracle, refcode):
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(1, 1e-4)
+        ref = refcode.spmv_pull(C.byref(args), g.ptr, g.num_vertices)
+        x = oracle.spmv_input(g.out_degree())
+        assert np.array_equal(ref["x"].view(np.uint32), x.view(np.uint32)), name
+        y = oracle.spmv_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), None, x)
+        assert np.array_equal(ref["y"].view(np.uint32), y.view(np.uint32)), name
+        assert ref["iterations"] == 1
