@@ -161,6 +161,9 @@ SIGNATURES = [
     ("ag_graph_rmat", GraphP, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                C.c_uint32]),
     ("ag_graph_er", GraphP, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32]),
+    ("ag_graph_build_csr", GraphP, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    ("ag_graph_build", C.c_int32, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                   C.c_uint32, C.POINTER(C.c_void_p)]),
     ("ag_graph_read_edge_file", GraphP, [C.c_char_p, C.c_int, C.c_uint32]),
     ("ag_graph_free", None, [GraphP]),
     ("ag_fill_uniform", None, [f32p, C.c_uint64, C.c_uint64]),
@@ -278,6 +281,24 @@ def _f32(ptr, n) -> np.ndarray:
     return np.ctypeslib.as_array(ptr, shape=(n,))
 
 
+def _edge_ptrs(src, dst, weight):
+    """Raw pointers of edge arrays given as numpy arrays (converted to
+    contiguous uint32/float32) or CUDA tensors (used in place)."""
+    out, keep = [], []
+    for a, dt in ((src, np.uint32), (dst, np.uint32), (weight, np.float32)):
+        if a is None:
+            out.append(None)
+            keep.append(None)
+        elif hasattr(a, "data_ptr"):
+            out.append(a.data_ptr())
+            keep.append(a)
+        else:
+            arr = np.ascontiguousarray(a, dt)
+            out.append(arr.ctypes.data)
+            keep.append(arr)
+    return out, keep
+
+
 class Graph:
     """A struct GraphCSR plus numpy views of its arrays.
 
@@ -309,6 +330,14 @@ class Graph:
         w = None if weight is None else np.ascontiguousarray(weight, np.float32)
         ptr = lib.ag_graph_from_edges(num_vertices, len(src), src.ctypes.data_as(u32p), dst.ctypes.data_as(u32p),
                                       None if w is None else w.ctypes.data_as(f32p), flags)
+        return cls(ptr, True)
+
+    @classmethod
+    def build_gpu(cls, num_vertices: int, src, dst, weight=None, flags=0) -> "Graph":
+        """ag_graph_build_csr: the from_edges CSR built on the GPU.  src, dst,
+        weight: numpy arrays or CUDA tensors."""
+        (ps, pd, pw), keep = _edge_ptrs(src, dst, weight)
+        ptr = lib.ag_graph_build_csr(num_vertices, len(keep[0]), ps, pd, pw, flags)
         return cls(ptr, True)
 
     @classmethod
@@ -405,6 +434,23 @@ class DeviceGraph:
         self.h = h
         self.num_vertices = graph.num_vertices
         self.num_edges = graph.num_edges
+
+    @classmethod
+    def from_edges(cls, num_vertices: int, src, dst, weight=None, build_flags=AG_BUILD_DEDUPE,
+                   flags: int = 0) -> "DeviceGraph":
+        """ag_graph_build: edge list to device graph, CSR built on the GPU."""
+        (ps, pd, pw), keep = _edge_ptrs(src, dst, weight)
+        m = len(keep[0]) if keep[0] is not None else 0
+        h = C.c_void_p()
+        if weight is not None:
+            flags |= AG_UPLOAD_WEIGHTS
+        check(lib.ag_graph_build(num_vertices, m, ps, pd, pw, build_flags, flags, C.byref(h)), "ag_graph_build")
+        self = cls.__new__(cls)
+        self.h = h
+        self.num_vertices = num_vertices
+        inf = self.info()
+        self.num_edges = inf.num_edges
+        return self
 
     def info(self) -> GraphInfo:
         inf = GraphInfo()

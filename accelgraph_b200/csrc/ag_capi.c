@@ -53,6 +53,9 @@ struct PageRankStats *newPageRankStatsGraphCSR(struct GraphCSR *graph)
         free(stats);
         return NULL;
     }
+    /* first touch of the two arrays spread over the host threads, as the
+     * reference does (pageRank.c:68-73) */
+#pragma omp parallel for schedule(static)
     for (v = 0; v < n; v++) {
         stats->pageRanks[v] = stats->base_pr;
         stats->realRanks[v] = v;

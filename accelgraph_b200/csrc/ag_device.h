@@ -191,9 +191,30 @@ typedef struct AgPlanState
     uint32_t *scan;
 } AgPlanState;
 
+/* forward and inverse CSR in device memory, caller vertex order (ag_build.cu) */
+typedef struct AgDevCSR
+{
+    uint32_t N, E;
+    uint32_t *out_deg, *in_deg;   /* N                                       */
+    uint32_t *fwd_idx, *inv_idx;  /* N + 1 row starts                        */
+    uint32_t *fwd_src, *fwd_dst;  /* E, sorted by source                     */
+    uint32_t *inv_src, *inv_dst;  /* E, sorted by destination: inv_src holds
+                                     the row (destination), inv_dst the
+                                     in-neighbour (source)                   */
+    float *fwd_w, *inv_w;         /* E or NULL                               */
+    float max_w;
+    uint32_t max_in_degree;
+} AgDevCSR;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
+
+/* build both CSRs from a device edge list (m < 2^31 edges); a bad endpoint
+ * returns cudaErrorInvalidValue with *bad_edge = its lowest edge index */
+cudaError_t ag_csr_build_device(uint32_t n, uint32_t m, const uint32_t *src, const uint32_t *dst, const float *w,
+                                uint32_t flags, AgDevCSR *out, uint32_t *bad_edge, cudaStream_t s);
+void ag_csr_free_device(AgDevCSR *c, cudaStream_t s);
 
 /* count items per segment and copy the four totals to totals_host (the copy
  * is stream-ordered: wait on the stream before reading them) */

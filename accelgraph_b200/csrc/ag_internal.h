@@ -24,6 +24,10 @@ void ag_clear_error(void);
 void *ag_rt_host_alloc(size_t bytes, int pinned, int *got_pinned);
 void ag_rt_host_free(void *ptr, int pinned);
 
+/* an empty host graph of the builder's layout (all arrays allocated, page-
+ * locked when requested); NULL on allocation failure */
+struct GraphCSR *ag_host_graph_new(uint32_t N, uint32_t E, int weighted, int pinned);
+
 /* wall clock in seconds (CLOCK_MONOTONIC) */
 double ag_wall_seconds(void);
 

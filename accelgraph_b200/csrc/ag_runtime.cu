@@ -174,14 +174,111 @@ extern "C" void *ag_rt_host_alloc(size_t bytes, int pinned, int *got_pinned)
     return malloc(bytes);
 }
 
+/* frees either kind: a graph whose page-locked allocations ran out part way
+ * holds both, so the kind is asked per pointer, `pinned` being a hint */
 extern "C" void ag_rt_host_free(void *ptr, int pinned)
 {
     if (!ptr)
         return;
-    if (pinned)
+    bool page_locked = false;
+    if (g_ctx.ready) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, ptr) == cudaSuccess)
+            page_locked = at.type == cudaMemoryTypeHost;
+        else
+            cudaGetLastError();
+    } else {
+        page_locked = pinned != 0;
+    }
+    if (page_locked)
         cudaFreeHost(ptr);
     else
         free(ptr);
+}
+
+/* ------------------------------------------------ device-to-host copies */
+#define AG_STAGE_CHUNK ((size_t)4 << 20)
+
+static struct
+{
+    unsigned char *buf; /* two page-locked chunks */
+    cudaEvent_t ev[2];
+    int state;          /* 0: not set up, 1: ready, -1: unavailable */
+} g_stage = {nullptr, {nullptr, nullptr}, 0};
+
+static ag_status_t event_wait(cudaEvent_t ev, double timeout_s)
+{
+    const double limit = wait_limit_s(timeout_s);
+    const double t0 = ag_wall_seconds();
+    unsigned spins = 0;
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess)
+            return AG_OK;
+        if (e != cudaErrorNotReady)
+            return ag_set_error(AG_ERR_CUDA, "device copy failed: %s", cudaGetErrorString(e));
+        if (ag_wall_seconds() - t0 > limit)
+            return ag_set_error(AG_ERR_TIMEOUT, "device copy did not finish within %.1f s", limit);
+        if (++spins > 64) {
+            struct timespec ts = {0, 5000};
+            nanosleep(&ts, nullptr);
+        }
+    }
+}
+
+/* Copy `bytes` of device memory to host memory `dst` on the library stream
+ * and wait for it (bounded).  A page-locked destination is copied directly;
+ * a pageable one goes through two page-locked chunks, so that the device
+ * copy of one chunk overlaps the host copy of the other. */
+static ag_status_t copy_to_host(void *dst, const void *src, size_t bytes)
+{
+    cudaStream_t s = g_ctx.stream;
+    if (!bytes)
+        return AG_OK;
+    cudaPointerAttributes at;
+    bool pinned = false;
+    if (cudaPointerGetAttributes(&at, dst) == cudaSuccess)
+        pinned = at.type == cudaMemoryTypeHost;
+    else
+        cudaGetLastError();
+    if (!pinned && bytes >= ((size_t)1 << 20) && g_stage.state == 0) {
+        g_stage.state = -1;
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, 2 * AG_STAGE_CHUNK, cudaHostAllocDefault) == cudaSuccess) {
+            if (cudaEventCreateWithFlags(&g_stage.ev[0], cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&g_stage.ev[1], cudaEventDisableTiming) == cudaSuccess) {
+                g_stage.buf = (unsigned char *)p;
+                g_stage.state = 1;
+            } else {
+                cudaFreeHost(p);
+            }
+        }
+        cudaGetLastError();
+    }
+    if (pinned || bytes < ((size_t)1 << 20) || g_stage.state != 1) {
+        AG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        return stream_wait(s, 0);
+    }
+    unsigned char *d = (unsigned char *)dst;
+    const unsigned char *sp = (const unsigned char *)src;
+    const size_t nch = (bytes + AG_STAGE_CHUNK - 1) / AG_STAGE_CHUNK;
+    auto len = [&](size_t k) { return std::min(AG_STAGE_CHUNK, bytes - k * AG_STAGE_CHUNK); };
+    auto issue = [&](size_t k) -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(g_stage.buf + (k & 1) * AG_STAGE_CHUNK, sp + k * AG_STAGE_CHUNK, len(k),
+                                        cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? cudaEventRecord(g_stage.ev[k & 1], s) : e;
+    };
+    AG_CUDA(issue(0));
+    for (size_t k = 0; k < nch; ++k) {
+        /* chunk k + 1 reuses the buffer chunk k - 1 was copied out of */
+        if (k + 1 < nch)
+            AG_CUDA(issue(k + 1));
+        ag_status_t st = event_wait(g_stage.ev[k & 1], 0);
+        if (st != AG_OK)
+            return st;
+        memcpy(d + k * AG_STAGE_CHUNK, g_stage.buf + (k & 1) * AG_STAGE_CHUNK, len(k));
+    }
+    return AG_OK;
 }
 
 /* ------------------------------------------------------- graph handle */
@@ -385,74 +482,45 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
 }
 
 static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
-                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out);
+                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out, const AgDevCSR *dev = nullptr);
 
 extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out)
 {
     return upload_impl(graph, flags, nullptr, 0, 0, out);
 }
 
-/* gather_n: length of the vector the in-edges index (0: num_vertices) */
+/* gather_n: length of the vector the in-edges index (0: num_vertices).
+ * dev: the graph's CSR already in device memory (built by ag_graph_build);
+ * `graph` is then unused, and the device arrays are copied, not checked. */
 static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, const uint32_t *gstart_host,
-                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out)
+                               uint32_t ngraphs, uint32_t gather_n, ag_graph_t *out, const AgDevCSR *dev)
 {
     ag_clear_error();
-    if (!graph || !out)
+    if ((!graph && !dev) || !out)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_upload: NULL argument");
     *out = nullptr;
     ag_status_t st = ctx_ensure(-1);
     if (st != AG_OK)
         return st;
-    const uint32_t N = graph->num_vertices, E = graph->num_edges;
-    const struct Vertex *iv = graph->inverse_vertices;
-    const struct Vertex *fv = graph->vertices;
-    const struct EdgeList *iel = graph->inverse_sorted_edges_array;
-    if (N > 0 && (!iv || !iv->out_degree || !iv->edges_idx || !fv || !fv->out_degree))
+    const uint32_t N = dev ? dev->N : graph->num_vertices, E = dev ? dev->E : graph->num_edges;
+    const struct Vertex *iv = dev ? nullptr : graph->inverse_vertices;
+    const struct Vertex *fv = dev ? nullptr : graph->vertices;
+    const struct EdgeList *iel = dev ? nullptr : graph->inverse_sorted_edges_array;
+    if (!dev && N > 0 && (!iv || !iv->out_degree || !iv->edges_idx || !fv || !fv->out_degree))
         return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: missing vertex arrays");
-    if (E > 0 && (!iel || !iel->edges_array_dest))
+    if (!dev && E > 0 && (!iel || !iel->edges_array_dest))
         return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: missing inverse edge array");
     if (E >= 0xFFFFFFF0u)
         return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: too many edges");
-    const bool want_w = (flags & AG_UPLOAD_WEIGHTS) && iel && iel->edges_array_weight;
-
-    /* host view of the inverse rows: contiguous rows are uploaded as they
-     * are; any other layout (gaps, overlap, reordering) is repacked */
-    bool contiguous = true;
-    uint64_t total = 0;
-    uint32_t maxd = 0;
-    for (uint32_t v = 0; v < N; ++v) {
-        const uint32_t d = iv->out_degree[v];
-        if (iv->edges_idx[v] != total)
-            contiguous = false;
-        if ((uint64_t)iv->edges_idx[v] + d > E)
-            return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: row %u [%u, +%u) exceeds %u edges", v,
-                                iv->edges_idx[v], d, E);
-        total += d;
-        if (d > maxd)
-            maxd = d;
-    }
-    if (total != E)
-        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: in-degrees sum to %llu, expected %u edges",
-                            (unsigned long long)total, E);
-    /* row starts: the caller's own array when its rows are contiguous (its
-     * N entries plus E), else a packed copy */
-    std::vector<uint32_t> off;
-    if (!contiguous) {
-        off.resize((size_t)N + 1);
-        uint32_t o = 0;
-        for (uint32_t v = 0; v < N; ++v) {
-            off[v] = o;
-            o += iv->out_degree[v];
-        }
-        off[N] = E;
-    }
+    if (dev)
+        flags |= AG_UPLOAD_TRUSTED; /* the builder checked every endpoint */
+    const bool want_w = (flags & AG_UPLOAD_WEIGHTS) && (dev ? dev->inv_w != nullptr : iel && iel->edges_array_weight);
 
     ag_graph_s *g = new ag_graph_s();
     memset((void *)g, 0, sizeof(*g));
     g->N = N;
     g->E = E;
     g->E4 = ((E + 3u) & ~3u) + 4u;
-    g->max_in_degree = maxd;
 
     cudaStream_t s = g_ctx.stream;
     const bool relabel = !(flags & AG_UPLOAD_KEEP_ORDER) && N > 0;
@@ -507,38 +575,110 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
             return st;                                                                           \
         }                                                                                        \
     } while (0)
-    if (contiguous) {
-        if (N)
-            UP(cudaMemcpyAsync(off_old, iv->edges_idx, (size_t)N * 4, cudaMemcpyHostToDevice, s));
-        UP(ag_set_u32(off_old + N, E, s));
-    } else {
-        UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
-    }
-    UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
-    if (contiguous) {
+#define UPFAIL(status)                                                                           \
+    do {                                                                                         \
+        st = (status);                                                                           \
+        if (relabel) {                                                                           \
+            dev_free(off_old);                                                                   \
+            dev_free(ids_old);                                                                   \
+            dev_free(outdeg_old);                                                                \
+            dev_free(w_old);                                                                     \
+        }                                                                                        \
+        ag_graph_release(g);                                                                     \
+        return st;                                                                               \
+    } while (0)
+    if (dev) {
+        g->max_in_degree = dev->max_in_degree;
+        UP(cudaMemcpyAsync(off_old, dev->inv_idx, (size_t)(N + 1) * 4, cudaMemcpyDeviceToDevice, s));
+        UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
         if (E)
-            UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
-        if (want_w && E)
-            UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
-    } else {
-        std::vector<uint32_t> packed(E);
-        std::vector<float> packw(want_w ? E : 0);
-        for (uint32_t v = 0; v < N; ++v) {
-            const uint32_t d = iv->out_degree[v], b = iv->edges_idx[v];
-            memcpy(packed.data() + off[v], iel->edges_array_dest + b, (size_t)d * 4);
-            if (want_w)
-                memcpy(packw.data() + off[v], iel->edges_array_weight + b, (size_t)d * 4);
+            UP(cudaMemcpyAsync(ids_old, dev->inv_dst, (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
+        if (want_w) {
+            if (E)
+                UP(cudaMemcpyAsync(w_old, dev->inv_w, (size_t)E * 4, cudaMemcpyDeviceToDevice, s));
+            UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, s));
         }
-        if (E)
-            UP(cudaMemcpyAsync(ids_old, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
-        if (want_w && E)
-            UP(cudaMemcpyAsync(w_old, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
-        UP(cudaStreamSynchronize(s)); /* the packed copies are stack-owned */
+        if (N)
+            UP(cudaMemcpyAsync(outdeg_old, dev->out_deg, (size_t)N * 4, cudaMemcpyDeviceToDevice, s));
+    } else {
+        /* The bulk copies start first, assuming the usual layout of contiguous
+         * rows; the host checks the rows while they run.  A layout that is not
+         * contiguous is repacked and copied again (ordered after the first copy
+         * on the same stream).  Every error path below waits for the stream
+         * before the caller's arrays can be freed (ag_graph_release does). */
+        const bool guess_contiguous = N == 0 || iv->edges_idx[0] == 0;
+        if (guess_contiguous) {
+            if (E)
+                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            if (want_w && E)
+                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+        }
+        if (N)
+            UP(cudaMemcpyAsync(outdeg_old, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+        /* host view of the inverse rows: contiguous rows are uploaded as they
+         * are; any other layout (gaps, overlap, reordering) is repacked */
+        bool contiguous = true;
+        uint64_t total = 0;
+        uint32_t maxd = 0;
+        for (uint32_t v = 0; v < N; ++v) {
+            const uint32_t d = iv->out_degree[v];
+            if (iv->edges_idx[v] != total)
+                contiguous = false;
+            if ((uint64_t)iv->edges_idx[v] + d > E)
+                UPFAIL(ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: row %u [%u, +%u) exceeds %u edges", v,
+                                    iv->edges_idx[v], d, E));
+            total += d;
+            if (d > maxd)
+                maxd = d;
+        }
+        if (total != E)
+            UPFAIL(ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_upload: in-degrees sum to %llu, expected %u edges",
+                                (unsigned long long)total, E));
+        g->max_in_degree = maxd;
+        /* row starts: the caller's own array when its rows are contiguous (its
+         * N entries plus E), else a packed copy */
+        std::vector<uint32_t> off;
+        if (!contiguous) {
+            off.resize((size_t)N + 1);
+            uint32_t o = 0;
+            for (uint32_t v = 0; v < N; ++v) {
+                off[v] = o;
+                o += iv->out_degree[v];
+            }
+            off[N] = E;
+        }
+
+        if (contiguous) {
+            if (N)
+                UP(cudaMemcpyAsync(off_old, iv->edges_idx, (size_t)N * 4, cudaMemcpyHostToDevice, s));
+            UP(ag_set_u32(off_old + N, E, s));
+        } else {
+            UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
+        }
+        UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
+        if (contiguous) {
+            if (!guess_contiguous && E)
+                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            if (!guess_contiguous && want_w && E)
+                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+        } else {
+            std::vector<uint32_t> packed(E);
+            std::vector<float> packw(want_w ? E : 0);
+            for (uint32_t v = 0; v < N; ++v) {
+                const uint32_t d = iv->out_degree[v], b = iv->edges_idx[v];
+                memcpy(packed.data() + off[v], iel->edges_array_dest + b, (size_t)d * 4);
+                if (want_w)
+                    memcpy(packw.data() + off[v], iel->edges_array_weight + b, (size_t)d * 4);
+            }
+            if (E)
+                UP(cudaMemcpyAsync(ids_old, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            if (want_w && E)
+                UP(cudaMemcpyAsync(w_old, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+            UP(cudaStreamSynchronize(s)); /* the packed copies are stack-owned */
+        }
+        if (want_w)
+            UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, s));
     }
-    if (want_w)
-        UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, s));
-    if (N)
-        UP(cudaMemcpyAsync(outdeg_old, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
     UP(cudaMemsetAsync(g->ctl, 0, sizeof(AgControl), s));
     UP(cudaMemsetAsync(g->flag, 0, 4, s));
     UP(cudaMemsetAsync(g->flag + 1, 0xFF, 4, s));
@@ -622,6 +762,7 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         return st;
     }
 #undef UP
+#undef UPFAIL
     *out = g;
     return AG_OK;
 }
@@ -905,10 +1046,10 @@ extern "C" ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_resul
         return ag_set_error(AG_ERR_CUDA, "control readback failed: %s", cudaGetErrorString(e));
     }
     if (ranks && g->N) {
-        e = cudaMemcpy(ranks, g->out, (size_t)g->N * 4, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) {
+        st = copy_to_host(ranks, g->out, (size_t)g->N * 4);
+        if (st != AG_OK) {
             free(hc);
-            return ag_set_error(AG_ERR_CUDA, "rank readback failed: %s", cudaGetErrorString(e));
+            return st;
         }
     }
     const uint32_t passes = hc->iter;
@@ -993,11 +1134,8 @@ extern "C" ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint
     AG_CUDA(cudaMallocAsync((void **)&dy, (size_t)g->N * 4, s));
     AG_CUDA(cudaMemcpyAsync(dx, x, (size_t)g->N * 4, cudaMemcpyHostToDevice, s));
     st = ag_spmv_pull_device(g, dx, dy, mode);
-    if (st == AG_OK) {
-        cudaError_t e = cudaMemcpyAsync(y, dy, (size_t)g->N * 4, cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess)
-            st = ag_set_error(AG_ERR_CUDA, "y readback failed: %s", cudaGetErrorString(e));
-    }
+    if (st == AG_OK)
+        st = copy_to_host(y, dy, (size_t)g->N * 4);
     cudaFreeAsync(dx, s);
     cudaFreeAsync(dy, s);
     ag_status_t w = stream_wait(s, 0);
@@ -1514,4 +1652,135 @@ extern "C" ag_status_t ag_partition_fetch(ag_graph_t g, float *ranks_local)
     if (ranks_local)
         AG_CUDA(cudaMemcpy(ranks_local, g->out, (size_t)g->N * 4, cudaMemcpyDeviceToHost));
     return AG_OK;
+}
+
+/* ------------------------------------------------ device graph build */
+/* device copy of an input array: device memory is used in place, host
+ * memory (pageable or page-locked) is copied on the library stream */
+static ag_status_t stage_in(const void *p, size_t bytes, const void **dev, void **owned)
+{
+    *dev = nullptr;
+    *owned = nullptr;
+    if (!p)
+        return AG_OK;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess &&
+        (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged)) {
+        *dev = p;
+        return AG_OK;
+    }
+    cudaGetLastError();
+    void *d = nullptr;
+    AG_CUDA(cudaMallocAsync(&d, bytes ? bytes : 16, g_ctx.stream));
+    if (bytes) {
+        cudaError_t e = cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, g_ctx.stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeAsync(d, g_ctx.stream);
+            return ag_set_error(AG_ERR_CUDA, "edge list copy failed: %s", cudaGetErrorString(e));
+        }
+    }
+    *dev = d;
+    *owned = d;
+    return AG_OK;
+}
+
+static ag_status_t build_device_csr(uint32_t N, uint64_t m, const uint32_t *src, const uint32_t *dst,
+                                    const float *w, uint32_t flags, AgDevCSR *csr)
+{
+    memset(csr, 0, sizeof(*csr));
+    if (m > 0 && (!src || !dst))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_build: NULL edge arrays");
+    if (m >= (1ull << 31))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_build: %llu edges exceed the 2^31 device build limit",
+                            (unsigned long long)m);
+    if (N > AG_ROW_MASK)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_build: %u vertices exceed the 2^30 row limit", N);
+    ag_status_t st = ctx_ensure(-1);
+    if (st != AG_OK)
+        return st;
+    cudaStream_t s = g_ctx.stream;
+    const void *ds = nullptr, *dd = nullptr, *dw = nullptr;
+    void *os = nullptr, *od = nullptr, *ow = nullptr;
+    st = stage_in(src, (size_t)m * 4, &ds, &os);
+    if (st == AG_OK)
+        st = stage_in(dst, (size_t)m * 4, &dd, &od);
+    if (st == AG_OK && w)
+        st = stage_in(w, (size_t)m * 4, &dw, &ow);
+    if (st == AG_OK) {
+        uint32_t bad = UINT32_MAX;
+        cudaError_t e = ag_csr_build_device(N, (uint32_t)m, (const uint32_t *)ds, (const uint32_t *)dd,
+                                            (const float *)dw, flags, csr, &bad, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (bad != UINT32_MAX)
+                st = ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_build: edge %u has an endpoint outside %u vertices",
+                                  bad, N);
+            else
+                st = ag_set_error(AG_ERR_CUDA, "ag_graph_build: device build failed: %s", cudaGetErrorString(e));
+        }
+    }
+    if (os)
+        cudaFreeAsync(os, s);
+    if (od)
+        cudaFreeAsync(od, s);
+    if (ow)
+        cudaFreeAsync(ow, s);
+    return st;
+}
+
+extern "C" struct GraphCSR *ag_graph_build_csr(uint32_t num_vertices, uint64_t num_edges, const uint32_t *src,
+                                              const uint32_t *dst, const float *weight, uint32_t flags)
+{
+    ag_clear_error();
+    AgDevCSR c;
+    if (build_device_csr(num_vertices, num_edges, src, dst, weight, flags, &c) != AG_OK)
+        return nullptr;
+    const uint32_t N = c.N, E = c.E;
+    struct GraphCSR *g = ag_host_graph_new(N, E, weight != nullptr, (flags & AG_BUILD_PINNED) ? 1 : 0);
+    ag_status_t st = g ? AG_OK : ag_set_error(AG_ERR_OOM, "ag_graph_build_csr: host allocation failed");
+    struct
+    {
+        void *h;
+        const void *d;
+        size_t bytes;
+    } cp[] = {{g ? g->vertices->out_degree : nullptr, c.out_deg, (size_t)N * 4},
+              {g ? g->vertices->in_degree : nullptr, c.in_deg, (size_t)N * 4},
+              {g ? g->vertices->edges_idx : nullptr, c.fwd_idx, ((size_t)N + 1) * 4},
+              {g ? g->inverse_vertices->edges_idx : nullptr, c.inv_idx, ((size_t)N + 1) * 4},
+              {g ? g->sorted_edges_array->edges_array_src : nullptr, c.fwd_src, (size_t)E * 4},
+              {g ? g->sorted_edges_array->edges_array_dest : nullptr, c.fwd_dst, (size_t)E * 4},
+              {g ? g->inverse_sorted_edges_array->edges_array_src : nullptr, c.inv_src, (size_t)E * 4},
+              {g ? g->inverse_sorted_edges_array->edges_array_dest : nullptr, c.inv_dst, (size_t)E * 4},
+              {g ? g->sorted_edges_array->edges_array_weight : nullptr, c.fwd_w, (size_t)E * 4},
+              {g ? g->inverse_sorted_edges_array->edges_array_weight : nullptr, c.inv_w, (size_t)E * 4}};
+    for (auto &x : cp)
+        if (st == AG_OK && x.h && x.d)
+            st = copy_to_host(x.h, x.d, x.bytes);
+    const float max_w = c.max_w;
+    ag_csr_free_device(&c, g_ctx.stream);
+    if (st != AG_OK) {
+        ag_graph_free(g);
+        return nullptr;
+    }
+    g->max_weight = g->sorted_edges_array->max_weight = g->inverse_sorted_edges_array->max_weight = max_w;
+    return g;
+}
+
+extern "C" ag_status_t ag_graph_build(uint32_t num_vertices, uint64_t num_edges, const uint32_t *src,
+                                      const uint32_t *dst, const float *weight, uint32_t build_flags,
+                                      uint32_t upload_flags, ag_graph_t *out)
+{
+    ag_clear_error();
+    if (!out)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_build: NULL output");
+    *out = nullptr;
+    AgDevCSR c;
+    ag_status_t st = build_device_csr(num_vertices, num_edges, src, dst, weight, build_flags, &c);
+    if (st != AG_OK)
+        return st;
+    st = upload_impl(nullptr, upload_flags, nullptr, 0, 0, out, &c);
+    ag_csr_free_device(&c, g_ctx.stream);
+    ag_status_t w = stream_wait(g_ctx.stream, 0);
+    return st != AG_OK ? st : w;
 }

@@ -120,6 +120,48 @@ void ag_graph_free(struct GraphCSR *graph)
     free(h);
 }
 
+/* an empty host graph with every array of the builder's layout allocated:
+ * row starts of N + 1 entries, inverse degrees aliasing the forward ones */
+struct GraphCSR *ag_host_graph_new(uint32_t N, uint32_t E, int weighted, int pinned)
+{
+    ag_host_graph *h = (ag_host_graph *)calloc(1, sizeof(*h));
+    if (!h)
+        return NULL;
+    h->magic = AG_GRAPH_MAGIC;
+    h->pinned = pinned;
+    h->g.num_vertices = N;
+    h->g.num_edges = E;
+    h->g.avg_degree = N ? E / N : 0;
+    h->g.vertices = &h->v;
+    h->g.inverse_vertices = &h->iv;
+    h->g.sorted_edges_array = &h->el;
+    h->g.inverse_sorted_edges_array = &h->iel;
+    h->el.num_edges = h->iel.num_edges = E;
+    h->el.num_vertices = h->iel.num_vertices = N;
+    h->el.avg_degree = h->iel.avg_degree = h->g.avg_degree;
+    h->v.out_degree = (uint32_t *)halloc((size_t)N * 4, pinned, &h->pinned);
+    h->v.in_degree = (uint32_t *)halloc((size_t)N * 4, pinned, &h->pinned);
+    h->v.edges_idx = (uint32_t *)halloc((size_t)N * 4 + 4, pinned, &h->pinned);
+    h->iv.edges_idx = (uint32_t *)halloc((size_t)N * 4 + 4, pinned, &h->pinned);
+    h->el.edges_array_src = (uint32_t *)halloc((size_t)E * 4, pinned, &h->pinned);
+    h->el.edges_array_dest = (uint32_t *)halloc((size_t)E * 4, pinned, &h->pinned);
+    h->iel.edges_array_src = (uint32_t *)halloc((size_t)E * 4, pinned, &h->pinned);
+    h->iel.edges_array_dest = (uint32_t *)halloc((size_t)E * 4, pinned, &h->pinned);
+    if (weighted) {
+        h->el.edges_array_weight = (float *)halloc((size_t)E * 4, pinned, &h->pinned);
+        h->iel.edges_array_weight = (float *)halloc((size_t)E * 4, pinned, &h->pinned);
+    }
+    h->iv.out_degree = h->v.in_degree;
+    h->iv.in_degree = h->v.out_degree;
+    if (!h->v.out_degree || !h->v.in_degree || !h->v.edges_idx || !h->iv.edges_idx || !h->el.edges_array_src ||
+        !h->el.edges_array_dest || !h->iel.edges_array_src || !h->iel.edges_array_dest ||
+        (weighted && (!h->el.edges_array_weight || !h->iel.edges_array_weight))) {
+        ag_graph_free(&h->g);
+        return NULL;
+    }
+    return &h->g;
+}
+
 /* ------------------------------------------------------- radix sort */
 static int bits_for(uint64_t max_value)
 {

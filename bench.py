@@ -2,7 +2,7 @@
 
 Workload (default): plain FP32 PageRank pull on a seeded R-MAT graph of
 scale 22, edge factor 16 (a,b,c = 0.57,0.19,0.19; self loops and duplicates
-removed; uint32 ids), damping 0.85, run to epsilon 1e-6 (iteration cap 100).
+removed; uint32 ids), damping 0.85, run to epsilon 1e-6 (iteration cap 300).
 A step is one complete solve: init, pull passes until no vertex changes by
 >= epsilon, normalisation.  The metric is GTEPS = edges x passes / time.
 
@@ -16,8 +16,12 @@ A step is one complete solve: init, pull passes until no vertex changes by
          bounded number of passes of the same graph, all host threads.
 
 --impl reference times that CPU restatement alone, as the reference arm.
---gpus N (torchrun): every rank solves its own graph (seed + rank), no data
-exchange; value = all ranks' edges x passes / max-over-ranks time.
+--gpus N (torchrun): by default every rank solves its own graph (seed + rank),
+no data exchange, value = all ranks' edges x passes / max-over-ranks time
+(weak scaling); --mode rows splits one graph by rows across the ranks with
+an all-gather of contributions per pass (strong scaling).
+--workload selects the other forms (SpMV, precision, PPR, many graphs, warm
+start, gather-rate probe); each prints its own JSON line.
 """
 from __future__ import annotations
 
@@ -68,6 +72,18 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def profiled_traffic(scale: int, edge_factor: int):
+    """DRAM bytes (read + write) of one pull pass from the committed ncu
+    summary of this workload (profiles/ag_pull_kernel_rmat<scale>.md, row
+    `dram__bytes_read.sum + write | R + W MB`), or None without one."""
+    import re
+    f = ROOT / "profiles" / f"ag_pull_kernel_rmat{scale}.md"
+    if edge_factor != 16 or not f.exists():
+        return None
+    m = re.search(r"\|\s*dram__bytes_read\.sum \+ write\s*\|\s*([0-9.]+) \+ ([0-9.]+) MB", f.read_text())
+    return None if not m else (float(m.group(1)) + float(m.group(2))) * 1e6
 
 
 def reduce_time_work(seconds_or_ms: float, work: float, device=None):
@@ -273,15 +289,7 @@ def run_b200(a):
             "traffic": None, "peak_kind": peak_kind, "kernel": "ag_pull_kernel<PR,fp32,fast>",
             "bytes_per_pass": alg_bytes, "pass_us": pass_s * 1e6,
             "pass_us_device_timer_median": float(np.median(dev_pass[1:]) * 1e6) if len(dev_pass) > 1 else None}
-    traffic_file = ROOT / "profiles" / "traffic.json"
-    if traffic_file.exists():
-        try:
-            tr = json.loads(traffic_file.read_text())
-            key = f"rmat{a.scale}_ef{a.edge_factor}"
-            if key in tr:
-                roof["traffic"] = tr[key]["dram_bytes_per_pass"]
-        except Exception:
-            pass
+    roof["traffic"] = profiled_traffic(a.scale, a.edge_factor)
 
     # -------- end to end through the C ABI (host buffers, pinned)
     args = ag.default_arguments(a.iterations, a.epsilon)

@@ -95,6 +95,22 @@ struct GraphCSR *ag_graph_rmat(uint32_t scale, uint32_t edge_factor,
  * independent uniform endpoints. */
 struct GraphCSR *ag_graph_er(uint32_t num_vertices, uint32_t avg_degree,
                              uint64_t seed, uint32_t flags);
+/* The same CSR as ag_graph_from_edges (bit for bit, same flags), built on
+ * the GPU by device radix sorts and copied back to a host graph (free it
+ * with ag_graph_free).  src, dst and weight may be host (pageable or
+ * page-locked) or device arrays; num_edges < 2^31, num_vertices <= 2^30.
+ * Replaces OpenGraph's CSR construction, which the reference calls from
+ * 02_capi_graph/src/main/accel-graph.c:345 (generateGraphDataStructure). */
+struct GraphCSR *ag_graph_build_csr(uint32_t num_vertices, uint64_t num_edges,
+                                    const uint32_t *src, const uint32_t *dst,
+                                    const float *weight, uint32_t flags);
+struct ag_graph_s;
+/* Edge list straight to a device graph (ag_graph_t): the CSR is built on the
+ * GPU as ag_graph_build_csr builds it and stays there; upload_flags as for
+ * ag_graph_upload.  No host CSR is made. */
+ag_status_t ag_graph_build(uint32_t num_vertices, uint64_t num_edges, const uint32_t *src,
+                           const uint32_t *dst, const float *weight, uint32_t build_flags,
+                           uint32_t upload_flags, struct ag_graph_s **out);
 /* Binary edge list: 8 bytes per edge (uint32 src, uint32 dst), or 12 bytes
  * (..., float weight) when weighted != 0.  num_vertices = max id + 1. */
 struct GraphCSR *ag_graph_read_edge_file(const char *path, int weighted, uint32_t flags);
