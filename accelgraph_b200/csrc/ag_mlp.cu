@@ -148,19 +148,43 @@ __device__ __forceinline__ float ag_mlp_out(const float *sw, const float *h2)
     return y;
 }
 
+/* Inference: one sample per thread and no loop over samples, so that the
+ * compiler cannot hoist the shared-memory weights into registers across
+ * samples.  The first hidden layer stays in registers (its loops are fully
+ * unrolled, every index a constant) and the output layer is folded into the
+ * loop over the second layer's units, so no activation array lives in local
+ * memory.  Sums run in the same order as ag_mlp_hidden / ag_mlp_out. */
 __global__ void __launch_bounds__(AG_MLP_BLK) ag_mlp_infer_kernel(const __nv_bfloat16 *wb, const float *X, uint32_t n,
                                                                   float *Y)
 {
-    __shared__ float sw[AG_MLP_NPARAM];
+    __shared__ __align__(16) float sw[AG_MLP_NPARAM];
     ag_mlp_load_weights(wb, sw);
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-        float x[AG_MLP_IN], h1[AG_MLP_H], h2[AG_MLP_H];
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    float x[AG_MLP_IN];
+#pragma unroll
+    for (int i = 0; i < AG_MLP_IN; ++i)
+        x[i] = X[(size_t)s * AG_MLP_IN + i];
+    float h1[AG_MLP_H];
+#pragma unroll
+    for (int j = 0; j < AG_MLP_H; ++j) {
+        float a = sw[AG_MLP_OFF_B1 + j];
 #pragma unroll
         for (int i = 0; i < AG_MLP_IN; ++i)
-            x[i] = X[(size_t)s * AG_MLP_IN + i];
-        ag_mlp_hidden(sw, x, h1, h2);
-        Y[s] = ag_mlp_out(sw, h2);
+            a = fmaf(sw[AG_MLP_OFF_W1 + j * AG_MLP_IN + i], x[i], a);
+        h1[j] = fmaxf(a, 0.0f);
     }
+    float y = sw[AG_MLP_OFF_B3];
+#pragma unroll 1
+    for (int k = 0; k < AG_MLP_H; ++k) {
+        float a = sw[AG_MLP_OFF_B2 + k];
+#pragma unroll
+        for (int j = 0; j < AG_MLP_H; ++j)
+            a = fmaf(sw[AG_MLP_OFF_W2 + k * AG_MLP_H + j], h1[j], a);
+        y = fmaf(sw[AG_MLP_OFF_W3 + k], fmaxf(a, 0.0f), y);
+    }
+    Y[s] = y;
 }
 
 /* per-sample training signals; buf layout per sample (stride 2 + 4*64 + 8):
@@ -414,9 +438,7 @@ extern "C" ag_status_t ag_mlp_forward(ag_mlp_t m, const float *X, uint32_t n, fl
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_forward: NULL argument");
     if (n == 0)
         return AG_OK;
-    uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK;
-    if (blocks > 148 * 16)
-        blocks = 148 * 16;
+    const uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK; /* one sample per thread */
     ag_mlp_infer_kernel<<<(unsigned)blocks, AG_MLP_BLK, 0, mlp_stream()>>>(m->wb, X, n, Y);
     MCHK(cudaGetLastError());
     return AG_OK;
