@@ -126,7 +126,8 @@ class GraphInfo(C.Structure):
 AG_OK = 0
 AG_ERR_INVALID_ARG, AG_ERR_INVALID_GRAPH, AG_ERR_CUDA, AG_ERR_OOM = -1, -2, -3, -4
 AG_ERR_TIMEOUT, AG_ERR_NO_DEVICE, AG_ERR_UNSUPPORTED = -5, -6, -7
-AG_BUILD_DEDUPE, AG_BUILD_SORT, AG_BUILD_PINNED, AG_BUILD_WEIGHTS = 1, 2, 4, 8
+AG_BUILD_DEDUPE, AG_BUILD_SORT, AG_BUILD_PINNED, AG_BUILD_WEIGHTS, AG_BUILD_SYMMETRIC = 1, 2, 4, 8, 16
+AG_FILE_TEXT, AG_FILE_BINARY, AG_FILE_CSR = 0, 1, 2
 AG_UPLOAD_WEIGHTS, AG_UPLOAD_VALIDATE, AG_UPLOAD_TRUSTED = 1, 2, 4
 AG_UPLOAD_KEEP_ORDER, AG_UPLOAD_NO_SMEM_CACHE = 8, 16
 AG_PREC_FP32, AG_PREC_BF16, AG_PREC_FP16 = 0, 1, 2
@@ -165,6 +166,8 @@ SIGNATURES = [
     ("ag_graph_build", C.c_int32, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                    C.c_uint32, C.POINTER(C.c_void_p)]),
     ("ag_graph_read_edge_file", GraphP, [C.c_char_p, C.c_int, C.c_uint32]),
+    ("ag_graph_read", GraphP, [C.c_char_p, C.c_int, C.c_int, C.c_uint32]),
+    ("ag_graph_write", C.c_int32, [GraphP, C.c_char_p, C.c_int]),
     ("ag_graph_free", None, [GraphP]),
     ("ag_fill_uniform", None, [f32p, C.c_uint64, C.c_uint64]),
     ("ag_graph_upload", C.c_int32, [GraphP, C.c_uint32, C.POINTER(C.c_void_p)]),
@@ -339,6 +342,17 @@ class Graph:
         (ps, pd, pw), keep = _edge_ptrs(src, dst, weight)
         ptr = lib.ag_graph_build_csr(num_vertices, len(keep[0]), ps, pd, pw, flags)
         return cls(ptr, True)
+
+    @classmethod
+    def read(cls, path, format=AG_FILE_BINARY, weighted=False, flags=0) -> "Graph":
+        """ag_graph_read: text or binary edge list, or a serialised CSR."""
+        ptr = lib.ag_graph_read(str(path).encode(), format, int(weighted), flags)
+        if not ptr:
+            raise AGError(AG_ERR_INVALID_ARG, "ag_graph_read: " + lib.ag_last_error().decode())
+        return cls(ptr, True)
+
+    def write(self, path, format=AG_FILE_CSR) -> None:
+        check(lib.ag_graph_write(self.ptr, str(path).encode(), format), "ag_graph_write")
 
     @classmethod
     def read_edge_file(cls, path, weighted=False, flags=0) -> "Graph":

@@ -1691,9 +1691,10 @@ static ag_status_t build_device_csr(uint32_t N, uint64_t m, const uint32_t *src,
     memset(csr, 0, sizeof(*csr));
     if (m > 0 && (!src || !dst))
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_build: NULL edge arrays");
-    if (m >= (1ull << 31))
+    const bool sym = (flags & AG_BUILD_SYMMETRIC) != 0;
+    if ((sym ? 2 * m : m) >= (1ull << 31))
         return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_build: %llu edges exceed the 2^31 device build limit",
-                            (unsigned long long)m);
+                            (unsigned long long)(sym ? 2 * m : m));
     if (N > AG_ROW_MASK)
         return ag_set_error(AG_ERR_UNSUPPORTED, "ag_graph_build: %u vertices exceed the 2^30 row limit", N);
     ag_status_t st = ctx_ensure(-1);
@@ -1707,10 +1708,40 @@ static ag_status_t build_device_csr(uint32_t N, uint64_t m, const uint32_t *src,
         st = stage_in(dst, (size_t)m * 4, &dd, &od);
     if (st == AG_OK && w)
         st = stage_in(w, (size_t)m * 4, &dw, &ow);
+    void *sym_buf = nullptr;
+    if (st == AG_OK && sym) {
+        /* every edge followed, after the input list, by its reverse */
+        const size_t b = (size_t)m * 4;
+        cudaError_t e = cudaMallocAsync(&sym_buf, 6 * b + 16, s);
+        unsigned char *q = (unsigned char *)sym_buf;
+        if (e == cudaSuccess && b) {
+            cudaMemcpyAsync(q, ds, b, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(q + b, dd, b, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(q + 2 * b, dd, b, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(q + 3 * b, ds, b, cudaMemcpyDeviceToDevice, s);
+            if (dw) {
+                cudaMemcpyAsync(q + 4 * b, dw, b, cudaMemcpyDeviceToDevice, s);
+                cudaMemcpyAsync(q + 5 * b, dw, b, cudaMemcpyDeviceToDevice, s);
+            }
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = ag_set_error(AG_ERR_CUDA, "ag_graph_build: reverse edges: %s", cudaGetErrorString(e));
+        } else {
+            ds = q;
+            dd = q + 2 * b;
+            if (dw)
+                dw = q + 4 * b;
+            m *= 2;
+        }
+    }
     if (st == AG_OK) {
         uint32_t bad = UINT32_MAX;
         cudaError_t e = ag_csr_build_device(N, (uint32_t)m, (const uint32_t *)ds, (const uint32_t *)dd,
-                                            (const float *)dw, flags, csr, &bad, s);
+                                            (const float *)dw, flags & ~AG_BUILD_SYMMETRIC, csr, &bad, s);
+        if (sym && bad != UINT32_MAX)
+            bad = bad % (uint32_t)(m / 2); /* report the input edge */
         if (e != cudaSuccess) {
             cudaGetLastError();
             if (bad != UINT32_MAX)
@@ -1726,6 +1757,8 @@ static ag_status_t build_device_csr(uint32_t N, uint64_t m, const uint32_t *src,
         cudaFreeAsync(od, s);
     if (ow)
         cudaFreeAsync(ow, s);
+    if (sym_buf)
+        cudaFreeAsync(sym_buf, s);
     return st;
 }
 

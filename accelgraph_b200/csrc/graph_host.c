@@ -294,6 +294,42 @@ struct GraphCSR *ag_graph_from_edges(uint32_t num_vertices, uint64_t num_edges,
         }
     }
 
+    if (flags & AG_BUILD_SYMMETRIC) {
+        /* every edge followed, after the input list, by its reverse */
+        struct GraphCSR *sg = NULL;
+        uint64_t m2 = 2 * num_edges;
+        uint32_t *s2, *d2;
+        float *w2 = NULL;
+        if (m2 >= 0xFFFFFFF0ull) {
+            ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_from_edges: %llu edges with their reverses exceed the "
+                         "uint32 edge index", (unsigned long long)num_edges);
+            return NULL;
+        }
+        s2 = (uint32_t *)malloc((m2 ? m2 : 1) * 4);
+        d2 = (uint32_t *)malloc((m2 ? m2 : 1) * 4);
+        if (weighted)
+            w2 = (float *)malloc((m2 ? m2 : 1) * 4);
+        if (s2 && d2 && (!weighted || w2)) {
+            if (num_edges) {
+                memcpy(s2, src, num_edges * 4);
+                memcpy(s2 + num_edges, dst, num_edges * 4);
+                memcpy(d2, dst, num_edges * 4);
+                memcpy(d2 + num_edges, src, num_edges * 4);
+                if (weighted) {
+                    memcpy(w2, weight, num_edges * 4);
+                    memcpy(w2 + num_edges, weight, num_edges * 4);
+                }
+            }
+            sg = ag_graph_from_edges(N, m2, s2, d2, w2, flags & ~AG_BUILD_SYMMETRIC);
+        } else {
+            ag_set_error(AG_ERR_OOM, "ag_graph_from_edges: host allocation failed");
+        }
+        free(s2);
+        free(d2);
+        free(w2);
+        return sg;
+    }
+
     h = (ag_host_graph *)calloc(1, sizeof(*h));
     if (!h) {
         ag_set_error(AG_ERR_OOM, "ag_graph_from_edges: host allocation failed");
@@ -629,4 +665,265 @@ void ag_fill_uniform(float *out, uint64_t n, uint64_t seed)
 #pragma omp parallel for schedule(static)
     for (uint64_t i = 0; i < n; i++)
         out[i] = ag_u01(ag_draw64(seed, i, 0));
+}
+
+/* ---------------------------------------------------------- graph files */
+/* text edge list: "src dst [weight]" per line, blanks between fields */
+static struct GraphCSR *read_text_edges(const char *path, int weighted, uint32_t flags)
+{
+    FILE *f = fopen(path, "r");
+    char line[512];
+    uint64_t m = 0, cap = 1u << 16, lineno = 0;
+    uint32_t *src = NULL, *dst = NULL, maxid = 0;
+    float *w = NULL;
+    struct GraphCSR *g = NULL;
+    if (!f) {
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: cannot open %s: %s", path, strerror(errno));
+        return NULL;
+    }
+    src = (uint32_t *)malloc(cap * 4);
+    dst = (uint32_t *)malloc(cap * 4);
+    w = weighted ? (float *)malloc(cap * 4) : NULL;
+    if (!src || !dst || (weighted && !w))
+        goto oom;
+    while (fgets(line, sizeof(line), f)) {
+        char *p = line, *end;
+        unsigned long long a, b;
+        ++lineno;
+        if (!strchr(line, '\n') && !feof(f)) {
+            ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: %s:%llu: line too long", path,
+                         (unsigned long long)lineno);
+            goto fail;
+        }
+        while (*p == ' ' || *p == '\t' || *p == '\r')
+            ++p;
+        if (*p == '\n' || *p == '\0' || *p == '#' || *p == '%')
+            continue;
+        errno = 0;
+        a = strtoull(p, &end, 10);
+        if (end == p || errno)
+            goto bad;
+        p = end;
+        b = strtoull(p, &end, 10);
+        if (end == p || errno)
+            goto bad;
+        p = end;
+        if (a > 0xFFFFFFFEull || b > 0xFFFFFFFEull)
+            goto bad;
+        if (m == cap) {
+            uint32_t *ns, *nd;
+            float *nw = NULL;
+            cap *= 2;
+            ns = (uint32_t *)realloc(src, cap * 4);
+            if (ns)
+                src = ns;
+            nd = (uint32_t *)realloc(dst, cap * 4);
+            if (nd)
+                dst = nd;
+            if (weighted) {
+                nw = (float *)realloc(w, cap * 4);
+                if (nw)
+                    w = nw;
+            }
+            if (!ns || !nd || (weighted && !nw))
+                goto oom;
+        }
+        if (weighted) {
+            float x = strtof(p, &end);
+            if (end == p)
+                goto bad;
+            w[m] = x;
+            p = end;
+        }
+        while (*p == ' ' || *p == '\t' || *p == '\r')
+            ++p;
+        if (*p != '\n' && *p != '\0')
+            goto bad;
+        src[m] = (uint32_t)a;
+        dst[m] = (uint32_t)b;
+        if (src[m] > maxid)
+            maxid = src[m];
+        if (dst[m] > maxid)
+            maxid = dst[m];
+        ++m;
+        if (m >= 0xFFFFFFF0ull) {
+            ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: %s: too many edges", path);
+            goto fail;
+        }
+    }
+    g = ag_graph_from_edges(m ? maxid + 1 : 0, m, src, dst, w, flags);
+    goto fail; /* common exit */
+bad:
+    ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: %s:%llu: expected \"src dst%s\"", path,
+                 (unsigned long long)lineno, weighted ? " weight" : "");
+    goto fail;
+oom:
+    ag_set_error(AG_ERR_OOM, "ag_graph_read: allocation failed");
+fail:
+    fclose(f);
+    free(src);
+    free(dst);
+    free(w);
+    return g;
+}
+
+/* serialised CSR: header, then every array of the graph, little endian */
+static const char csr_magic[8] = {'A', 'G', 'C', 'S', 'R', '1', 0, 0};
+
+struct csr_header
+{
+    char magic[8];
+    uint32_t num_vertices, num_edges, weighted, avg_degree;
+    float max_weight;
+    uint32_t reserved[3];
+};
+
+static int write_all(FILE *f, const void *p, size_t bytes)
+{
+    return bytes == 0 || fwrite(p, 1, bytes, f) == bytes;
+}
+
+static int read_all(FILE *f, void *p, size_t bytes)
+{
+    return bytes == 0 || fread(p, 1, bytes, f) == bytes;
+}
+
+static struct GraphCSR *read_csr(const char *path, uint32_t flags)
+{
+    FILE *f = fopen(path, "rb");
+    struct csr_header hd;
+    struct GraphCSR *g;
+    long size;
+    uint64_t N, E, need;
+    int ok;
+    if (!f) {
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: cannot open %s: %s", path, strerror(errno));
+        return NULL;
+    }
+    if (!read_all(f, &hd, sizeof(hd)) || memcmp(hd.magic, csr_magic, sizeof(csr_magic)) != 0 || hd.weighted > 1) {
+        fclose(f);
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: %s is not a serialised CSR", path);
+        return NULL;
+    }
+    N = hd.num_vertices;
+    E = hd.num_edges;
+    need = sizeof(hd) + 4 * (2 * N + 2 * (N + 1) + 4 * E + (hd.weighted ? 2 * E : 0));
+    fseek(f, 0, SEEK_END);
+    size = ftell(f);
+    fseek(f, (long)sizeof(hd), SEEK_SET);
+    if (size < 0 || (uint64_t)size != need) {
+        fclose(f);
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: %s holds %ld bytes, its header needs %llu", path, size,
+                     (unsigned long long)need);
+        return NULL;
+    }
+    g = ag_host_graph_new((uint32_t)N, (uint32_t)E, (int)hd.weighted, (flags & AG_BUILD_PINNED) ? 1 : 0);
+    if (!g) {
+        fclose(f);
+        ag_set_error(AG_ERR_OOM, "ag_graph_read: allocation failed");
+        return NULL;
+    }
+    ok = read_all(f, g->vertices->out_degree, N * 4) && read_all(f, g->vertices->in_degree, N * 4) &&
+         read_all(f, g->vertices->edges_idx, (N + 1) * 4) && read_all(f, g->inverse_vertices->edges_idx, (N + 1) * 4) &&
+         read_all(f, g->sorted_edges_array->edges_array_src, E * 4) &&
+         read_all(f, g->sorted_edges_array->edges_array_dest, E * 4) &&
+         read_all(f, g->inverse_sorted_edges_array->edges_array_src, E * 4) &&
+         read_all(f, g->inverse_sorted_edges_array->edges_array_dest, E * 4);
+    if (ok && hd.weighted)
+        ok = read_all(f, g->sorted_edges_array->edges_array_weight, E * 4) &&
+             read_all(f, g->inverse_sorted_edges_array->edges_array_weight, E * 4);
+    fclose(f);
+    if (!ok) {
+        ag_graph_free(g);
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: short read on %s", path);
+        return NULL;
+    }
+    g->avg_degree = g->sorted_edges_array->avg_degree = g->inverse_sorted_edges_array->avg_degree = hd.avg_degree;
+    g->max_weight = g->sorted_edges_array->max_weight = g->inverse_sorted_edges_array->max_weight = hd.max_weight;
+    return g;
+}
+
+struct GraphCSR *ag_graph_read(const char *path, int format, int weighted, uint32_t flags)
+{
+    ag_clear_error();
+    if (!path) {
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: NULL path");
+        return NULL;
+    }
+    switch (format) {
+    case AG_FILE_TEXT:
+        return read_text_edges(path, weighted, flags);
+    case AG_FILE_BINARY:
+        return ag_graph_read_edge_file(path, weighted, flags);
+    case AG_FILE_CSR:
+        return read_csr(path, flags);
+    default:
+        ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_read: unknown format %d", format);
+        return NULL;
+    }
+}
+
+ag_status_t ag_graph_write(const struct GraphCSR *graph, const char *path, int format)
+{
+    FILE *f;
+    const struct EdgeList *el, *iel;
+    uint64_t N, E;
+    int ok = 1, weighted;
+    ag_clear_error();
+    if (!graph || !path)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_write: NULL argument");
+    if (format < AG_FILE_TEXT || format > AG_FILE_CSR)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_write: unknown format %d", format);
+    N = graph->num_vertices;
+    E = graph->num_edges;
+    el = graph->sorted_edges_array;
+    iel = graph->inverse_sorted_edges_array;
+    if ((E && (!el || !el->edges_array_src || !el->edges_array_dest)) || !graph->vertices ||
+        (format == AG_FILE_CSR && (!iel || !graph->inverse_vertices || !graph->vertices->edges_idx ||
+                                   !graph->inverse_vertices->edges_idx || !graph->vertices->out_degree ||
+                                   !graph->vertices->in_degree || (E && (!iel->edges_array_src ||
+                                                                         !iel->edges_array_dest)))))
+        return ag_set_error(AG_ERR_INVALID_GRAPH, "ag_graph_write: the graph lacks arrays this format needs");
+    weighted = el && el->edges_array_weight && (format != AG_FILE_CSR || (iel && iel->edges_array_weight));
+    f = fopen(path, format == AG_FILE_TEXT ? "w" : "wb");
+    if (!f)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_write: cannot open %s: %s", path, strerror(errno));
+    if (format == AG_FILE_TEXT) {
+        for (uint64_t i = 0; i < E && ok; i++) {
+            if (weighted)
+                ok = fprintf(f, "%u %u %.9g\n", el->edges_array_src[i], el->edges_array_dest[i],
+                             (double)el->edges_array_weight[i]) > 0;
+            else
+                ok = fprintf(f, "%u %u\n", el->edges_array_src[i], el->edges_array_dest[i]) > 0;
+        }
+    } else if (format == AG_FILE_BINARY) {
+        for (uint64_t i = 0; i < E && ok; i++) {
+            ok = write_all(f, &el->edges_array_src[i], 4) && write_all(f, &el->edges_array_dest[i], 4);
+            if (ok && weighted)
+                ok = write_all(f, &el->edges_array_weight[i], 4);
+        }
+    } else {
+        /* the first N + 1 row starts: the builder keeps a closing entry; a
+         * graph without one gets E written in its place */
+        struct csr_header hd;
+        uint32_t e32 = (uint32_t)E;
+        memset(&hd, 0, sizeof(hd));
+        memcpy(hd.magic, csr_magic, sizeof(csr_magic));
+        hd.num_vertices = (uint32_t)N;
+        hd.num_edges = (uint32_t)E;
+        hd.weighted = (uint32_t)weighted;
+        hd.avg_degree = graph->avg_degree;
+        hd.max_weight = graph->max_weight;
+        ok = write_all(f, &hd, sizeof(hd)) && write_all(f, graph->vertices->out_degree, N * 4) &&
+             write_all(f, graph->vertices->in_degree, N * 4) && write_all(f, graph->vertices->edges_idx, N * 4) &&
+             write_all(f, &e32, 4) && write_all(f, graph->inverse_vertices->edges_idx, N * 4) &&
+             write_all(f, &e32, 4) && write_all(f, el->edges_array_src, E * 4) &&
+             write_all(f, el->edges_array_dest, E * 4) && write_all(f, iel->edges_array_src, E * 4) &&
+             write_all(f, iel->edges_array_dest, E * 4);
+        if (ok && weighted)
+            ok = write_all(f, el->edges_array_weight, E * 4) && write_all(f, iel->edges_array_weight, E * 4);
+    }
+    if (fclose(f) != 0)
+        ok = 0;
+    return ok ? AG_OK : ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_write: write to %s failed", path);
 }

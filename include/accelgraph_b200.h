@@ -76,6 +76,8 @@ ag_status_t ag_probe_gather_rates(double *rates);
 #define AG_BUILD_SORT     2u  /* rows ordered by neighbour id (radix sort)       */
 #define AG_BUILD_PINNED   4u  /* page-locked host arrays (faster uploads)        */
 #define AG_BUILD_WEIGHTS  8u  /* generators: attach weights uniform in [0,1)     */
+#define AG_BUILD_SYMMETRIC 16u /* add the reverse of every edge (reference -s),
+                                  appended after the input edges             */
 
 /* Build forward and inverse CSR from an edge list (src[i] -> dst[i]).
  * Without SORT, rows keep the input order of their edges (stable counting
@@ -114,6 +116,25 @@ ag_status_t ag_graph_build(uint32_t num_vertices, uint64_t num_edges, const uint
 /* Binary edge list: 8 bytes per edge (uint32 src, uint32 dst), or 12 bytes
  * (..., float weight) when weighted != 0.  num_vertices = max id + 1. */
 struct GraphCSR *ag_graph_read_edge_file(const char *path, int weighted, uint32_t flags);
+
+/* Graph files, in the reference's -z / -c format codes
+ * (02_capi_graph/src/main/accel-graph.c:50-53,114-117):
+ *   AG_FILE_TEXT      text edge list: one edge per line, "src dst" or
+ *                     "src dst weight", any blanks between fields; empty lines
+ *                     and lines starting with '#' or '%' are skipped
+ *   AG_FILE_BINARY    binary edge list (ag_graph_read_edge_file's format)
+ *   AG_FILE_CSR       serialised CSR written by ag_graph_write: every array of
+ *                     the GraphCSR, so a read skips the build (this library's
+ *                     own layout; OpenGraph's is not part of the reference)
+ * Edge-list reads build with `flags` (num_vertices = largest id + 1); a CSR
+ * read ignores them (only AG_BUILD_PINNED applies). */
+#define AG_FILE_TEXT   0
+#define AG_FILE_BINARY 1
+#define AG_FILE_CSR    2
+struct GraphCSR *ag_graph_read(const char *path, int format, int weighted, uint32_t flags);
+/* Write a graph in one of the formats above (edge lists hold the forward
+ * edges in CSR order, with weights when the graph has them). */
+ag_status_t ag_graph_write(const struct GraphCSR *graph, const char *path, int format);
 /* Free a graph returned by one of the builders above. */
 void ag_graph_free(struct GraphCSR *graph);
 /* n values uniform in [0,1) from the library's counter-based generator. */

@@ -50,7 +50,8 @@ def _same(ag, a, b):
 def test_build_csr_matches_host_builder(gpu, n, m, seed):
     ag = gpu
     src, dst, w = _edges(n, m, seed)
-    for flags in (0, ag.AG_BUILD_SORT, ag.AG_BUILD_DEDUPE, ag.AG_BUILD_DEDUPE | ag.AG_BUILD_SORT):
+    for flags in (0, ag.AG_BUILD_SORT, ag.AG_BUILD_DEDUPE, ag.AG_BUILD_DEDUPE | ag.AG_BUILD_SORT,
+                  ag.AG_BUILD_SYMMETRIC, ag.AG_BUILD_DEDUPE | ag.AG_BUILD_SYMMETRIC):
         for weight in (None, w):
             host = ag.Graph.from_edges(n, src, dst, weight, flags)
             dev = ag.Graph.build_gpu(n, src, dst, weight, flags)
