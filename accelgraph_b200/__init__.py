@@ -98,6 +98,7 @@ class PROpts(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("precision", C.c_int32), ("order", C.c_int32), ("quiet", C.c_int32),
         ("switch_residual", C.c_double), ("init_ranks", f32p), ("init_on_device", C.c_int32),
+        ("data_driven", C.c_int32),
     ]
 
 
@@ -502,8 +503,8 @@ class DeviceGraph:
         return t, us.value
 
     def launch(self, iterations=20, epsilon=1e-4, precision=AG_PREC_FP32, order=AG_ORDER_FAST,
-               init_ranks=None, switch_residual=1e-4) -> None:
-        o = make_opts(precision, order, init_ranks, switch_residual)
+               init_ranks=None, switch_residual=1e-4, data_driven=False) -> None:
+        o = make_opts(precision, order, init_ranks, switch_residual, data_driven=data_driven)
         self._keep_init = init_ranks
         check(lib.ag_pagerank_launch(self.h, iterations, epsilon, C.byref(o)), "ag_pagerank_launch")
 
@@ -522,8 +523,8 @@ class DeviceGraph:
         return ranks, res, hist
 
     def pagerank(self, iterations=20, epsilon=1e-4, precision=AG_PREC_FP32, order=AG_ORDER_FAST,
-                 init_ranks=None, switch_residual=1e-4, history=0):
-        self.launch(iterations, epsilon, precision, order, init_ranks, switch_residual)
+                 init_ranks=None, switch_residual=1e-4, history=0, data_driven=False):
+        self.launch(iterations, epsilon, precision, order, init_ranks, switch_residual, data_driven)
         return self.fetch(history)
 
     def pagerank_f64(self, max_iterations=1000, tol=1e-13):
@@ -611,11 +612,12 @@ class MultiGraph:
 
 
 def make_opts(precision=AG_PREC_FP32, order=AG_ORDER_FAST, init_ranks=None, switch_residual=1e-4,
-              quiet=True) -> PROpts:
+              quiet=True, data_driven=False) -> PROpts:
     o = PROpts()
     lib.ag_pr_opts_init(C.byref(o))
     o.precision = precision
     o.order = order
+    o.data_driven = int(data_driven)
     o.quiet = int(quiet)
     o.switch_residual = switch_residual
     if init_ranks is not None:

@@ -103,12 +103,15 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
         printf(" -----------------------------------------------------\n");
         printf("| %-51s | \n", "               ---->>> B200 <<<----");
         printf(" -----------------------------------------------------\n");
-        printf("| %-51s | \n", "Starting Page Rank Pull (tolerance/epsilon)");
+        printf("| %-51s | \n", o.data_driven ? "Starting Page Rank Pull DD (tolerance/epsilon)"
+                                               : "Starting Page Rank Pull (tolerance/epsilon)");
         printf(" -----------------------------------------------------\n");
         printf("| %-51.13lf | \n", arguments->epsilon);
         printf(" -----------------------------------------------------\n");
         printf("| %-10s | %-8s | %-15s | %-9s | \n", "Iteration", "Active", "Error", "Time (S)");
         printf(" -----------------------------------------------------\n");
+        if (o.data_driven) /* every vertex starts on the worklist (pageRank.c:2857-2868) */
+            printf("| %-10s | %-8u | %-15.13lf | %-9f | \n", "Init", graph->num_vertices, 0.0, 0.0);
     }
 
     st = ag_graph_upload(graph, 0, &g);
@@ -172,8 +175,22 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
     return stats;
 }
 
+/* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 is the pull,
+ * 6 the data-driven pull; the other codes (push, fixed-point and quantised
+ * variants) run the FP32 pull, with a note on stderr */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
 {
+    if (arguments && arguments->pushpull == 6) {
+        struct PageRankStats *stats = NULL;
+        ag_pr_opts o;
+        ag_status_t st;
+        ag_pr_opts_init(&o);
+        o.data_driven = 1;
+        st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
+        if (st != AG_OK)
+            fail_exit("pagerank-pull-dd", st);
+        return stats;
+    }
     if (arguments && arguments->pushpull != 0)
         fprintf(stderr, "pageRankGraphCSR: pushpull=%u runs the FP32 pull on the GPU\n", arguments->pushpull);
     return pageRankPullGraphCSR(arguments, graph);

@@ -249,6 +249,7 @@ struct AgPass
     const float *hot32;     /* shared-memory copy of the first hot_n values */
     const uint16_t *hot16;
     uint32_t hot_n;
+    uint8_t *wl_cur, *wl_nxt; /* data-driven mode: this pass's worklist, the next one */
 
     __device__ __forceinline__ AgPass(const AgPullParams &pp) : p(pp)
     {
@@ -265,6 +266,7 @@ struct AgPass
         c_in16 = nullptr;
         c_out32 = nullptr;
         c_out16 = nullptr;
+        wl_cur = wl_nxt = nullptr;
         if (MODE != AG_MODE_SPMV) {
             const uint32_t pass = p.ctl->iter;
             eps = p.ctl->eps;
@@ -277,6 +279,10 @@ struct AgPass
             c_out32 = odd ? p.c32_0 : p.c32_1;
             c_in16 = odd ? p.c16_1 : p.c16_0;
             c_out16 = odd ? p.c16_0 : p.c16_1;
+            if (MODE == AG_MODE_DD) {
+                wl_cur = odd ? p.wl1 : p.wl0;
+                wl_nxt = odd ? p.wl0 : p.wl1;
+            }
         }
     }
 
@@ -329,6 +335,39 @@ struct AgPass
             ag_st_keep_u16(c_out16 + r, ag_f32_to_low<PREC>(c), pol_last);
         else
             ag_st_keep_f32(c_out32 + p.c_base + r, c, pol_last);
+    }
+
+    /* data-driven update of an active row (pageRank.c:2896-2916): the
+     * residual of every active row counts, but the rank and its contribution
+     * are replaced only when it moved by at least epsilon; returns whether
+     * they were (the row's out-neighbours are then activated) */
+    __device__ __forceinline__ bool finish_dd(uint32_t r, float s, float rp, uint32_t od)
+    {
+        const float rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
+        const double err = (double)fabsf(__fsub_rn(rn, rp));
+        my_err += err;
+        if (err >= eps) {
+            p.rank[r] = rn;
+            ag_st_keep_f32(c_out32 + r, od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f, pol_last);
+            ++my_active;
+            return true;
+        }
+        keep_dd(r);
+        return false;
+    }
+
+    /* a row whose rank stays keeps its contribution in the next buffer */
+    __device__ __forceinline__ void keep_dd(uint32_t r) const
+    {
+        ag_st_keep_f32(c_out32 + r, __ldg(c_in32 + r), pol_last);
+    }
+
+    /* the whole warp puts row r's out-neighbours on the next worklist */
+    __device__ __forceinline__ void activate(uint32_t r, uint32_t lane) const
+    {
+        const uint32_t a = __ldg(p.fwd_off + r), b = __ldg(p.fwd_off + r + 1);
+        for (uint32_t j = a + lane; j < b; j += 32)
+            wl_nxt[__ldg(p.fwd_dst + j)] = 1;
     }
 
     /* two 16-byte groups of in-edges per lane: quads qa and qa + 32 (ids and,
@@ -596,7 +635,79 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 continue;
             }
         }
-        if (kind == AG_T_ROWS) {
+        if (MODE == AG_MODE_DD && kind == AG_T_ROWS) {
+            /* data-driven: rows off the worklist keep rank and contribution;
+             * an item without an active row gathers nothing.  Each flag read
+             * is cleared, so this pass's list is empty for the pass after
+             * next, which fills it. */
+            const uint32_t r = r0 + lane;
+            const bool live = r < task.y;
+            bool act = false;
+            if (live) {
+                act = ps.wl_cur[r] != 0;
+                if (act)
+                    ps.wl_cur[r] = 0;
+            }
+            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            if (!__any_sync(0xffffffffu, act)) {
+                if (live)
+                    ps.keep_dd(r);
+            } else {
+                uint32_t o0 = ee, o1 = ee, od = 0;
+                float rp = 0.0f;
+                if (live) {
+                    o0 = ag_ld_row_u32(p.row_off + r);
+                    o1 = ag_ld_row_u32(p.row_off + r + 1);
+                    rp = ag_ld_rank(p.rank + r);
+                    od = ag_ld_row_u32(p.outdeg + r);
+                }
+                ps.stage(vals, eb, ee, lane, pf);
+                __syncwarp();
+                o0 -= eb;
+                o1 -= eb;
+                float s = 0.0f;
+                bool is_long = false;
+                if (act) {
+                    if (EXACT || o1 - o0 <= AG_TSEQ) {
+                        if (o1 > o0) {
+                            s = vals[o0];
+                            for (uint32_t j = o0 + 1; j < o1; ++j)
+                                s = __fadd_rn(s, vals[j]);
+                        }
+                    } else {
+                        is_long = true;
+                    }
+                }
+                if (!EXACT) {
+                    unsigned m = __ballot_sync(0xffffffffu, is_long);
+                    while (m) {
+                        const int src = __ffs(m) - 1;
+                        m &= m - 1;
+                        const uint32_t a = __shfl_sync(0xffffffffu, o0, src);
+                        const uint32_t b = __shfl_sync(0xffffffffu, o1, src);
+                        float tsum = 0.0f;
+                        for (uint32_t j = a + lane; j < b; j += 32)
+                            tsum = __fadd_rn(tsum, vals[j]);
+                        tsum = ag_warp_sum_f(tsum);
+                        if ((int)lane == src)
+                            s = tsum;
+                    }
+                }
+                bool changed = false;
+                if (act)
+                    changed = ps.finish_dd(r, s, rp, od);
+                else if (live)
+                    ps.keep_dd(r);
+                __syncwarp();
+                unsigned m = __ballot_sync(0xffffffffu, changed);
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    m &= m - 1;
+                    ps.activate(__shfl_sync(0xffffffffu, r, src), lane);
+                }
+            }
+            pf = pn;
+        } else if (kind == AG_T_ROWS) {
             /* one row per lane; its bounds, previous rank and out-degree are
              * loaded first so that they arrive while the stage runs */
             const uint32_t r = r0 + lane;
@@ -653,20 +764,36 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         } else if (kind == AG_T_LONG) {
             float rp = 0.0f;
             uint32_t od = 0;
+            const bool act = MODE != AG_MODE_DD || ps.wl_cur[r0] != 0;
             if (MODE != AG_MODE_SPMV && lane == 0) {
                 rp = p.rank[r0];
                 od = p.outdeg[r0];
             }
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
-            float s;
-            if (EXACT) {
-                s = ps.ordered_sum(vals, eb, ee, lane);
+            if (!act) {
+                if (lane == 0)
+                    ps.keep_dd(r0);
             } else {
-                s = ps.strided_partial(eb, ee, lane, pf);
-                s = ag_warp_sum_f(s);
+                float s;
+                if (EXACT) {
+                    s = ps.ordered_sum(vals, eb, ee, lane);
+                } else {
+                    s = ps.strided_partial(eb, ee, lane, pf);
+                    s = ag_warp_sum_f(s);
+                }
+                if (MODE == AG_MODE_DD) {
+                    /* every lane has read the flag before the sum's shuffles */
+                    bool changed = false;
+                    if (lane == 0) {
+                        changed = ps.finish_dd(r0, s, rp, od);
+                        ps.wl_cur[r0] = 0;
+                    }
+                    if (__shfl_sync(0xffffffffu, changed, 0))
+                        ps.activate(r0, lane);
+                } else if (lane == 0) {
+                    ps.finish(r0, s, rp, od);
+                }
             }
-            if (lane == 0)
-                ps.finish(r0, s, rp, od);
             __syncwarp();
             pf = pn;
         } else {
@@ -676,8 +803,23 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             if (lane == 0)
                 deg = p.row_off[r0 + 1] - p.row_off[r0];
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            /* data-driven: a row off the worklist is skipped by all its
+             * chunks (chunk 0 keeps its contribution); the flag of an active
+             * row is cleared by the last chunk to arrive, after every chunk
+             * has read it */
+            const bool act = MODE != AG_MODE_DD || ps.wl_cur[r0] != 0;
+            if (!act) {
+                if (chunk == 0 && lane == 0)
+                    ps.keep_dd(r0);
+                __syncwarp();
+                pf = pn;
+                task = task_n;
+                t = tn;
+                continue;
+            }
             float s = ps.strided_partial(eb, ee, lane, pf);
             s = ag_warp_sum_f(s);
+            bool changed = false;
             if (lane == 0) {
                 const uint32_t nch = (deg + p.whub - 1) / p.whub;
                 p.hub_part[pbase + chunk] = s;
@@ -695,9 +837,16 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                         rp = p.rank[r0];
                         od = p.outdeg[r0];
                     }
-                    ps.finish(r0, tot, rp, od);
+                    if (MODE == AG_MODE_DD) {
+                        changed = ps.finish_dd(r0, tot, rp, od);
+                        ps.wl_cur[r0] = 0;
+                    } else {
+                        ps.finish(r0, tot, rp, od);
+                    }
                 }
             }
+            if (MODE == AG_MODE_DD && __shfl_sync(0xffffffffu, changed, 0))
+                ps.activate(r0, lane);
             __syncwarp();
             pf = pn;
         }
@@ -851,6 +1000,11 @@ __global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams
             ag_st_keep_u16(p.c16_0 + v, ag_f32_to_low<PREC>(c), pol_last);
         else
             ag_st_keep_f32(p.c32_0 + p.c_base + v, c, pol_last);
+        if (p.wl0) {
+            /* data-driven mode: every vertex starts on the worklist */
+            p.wl0[v] = 1;
+            p.wl1[v] = 0;
+        }
     }
     for (uint32_t g = blockIdx.x * AG_SBLK + threadIdx.x; g < p.ngraphs; g += gridDim.x * AG_SBLK) {
         p.g_active[g] = 0;
@@ -979,6 +1133,9 @@ extern "C" const void *ag_pull_kernel_ptr(int mode, int prec, int exact)
     if (mode == AG_MODE_MULTI)
         return exact ? (const void *)ag_pull_kernel<AG_MODE_MULTI, 0, true>
                      : (const void *)ag_pull_kernel<AG_MODE_MULTI, 0, false>;
+    if (mode == AG_MODE_DD)
+        return exact ? (const void *)ag_pull_kernel<AG_MODE_DD, 0, true>
+                     : (const void *)ag_pull_kernel<AG_MODE_DD, 0, false>;
     switch (prec) {
     case 1:
         return exact ? (const void *)ag_pull_kernel<AG_MODE_PR, 1, true> : (const void *)ag_pull_kernel<AG_MODE_PR, 1, false>;

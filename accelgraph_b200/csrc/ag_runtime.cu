@@ -326,6 +326,12 @@ struct ag_graph_s
     uint32_t *flag;
     AgExec exe[3][2];
     int have_exe[3][2];
+    /* data-driven mode: forward CSR in device numbering, two byte worklists,
+     * and its launch graphs (FAST, EXACT) */
+    uint32_t *fwd_off, *fwd_dst;
+    uint8_t *wl;
+    AgExec exe_dd[2];
+    int have_exe_dd[2];
     cudaEvent_t ev0, ev1;
     int launched;
     int last_prec, last_exact;
@@ -365,16 +371,32 @@ static void free_exec(AgExec *x)
     x->graph = nullptr;
 }
 
+/* forget every cached launch graph (they carry buffer pointers and tiles) */
+static void drop_execs(ag_graph_s *g)
+{
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 2; ++b)
+            if (g->have_exe[a][b]) {
+                free_exec(&g->exe[a][b]);
+                g->have_exe[a][b] = 0;
+            }
+    for (int b = 0; b < 2; ++b)
+        if (g->have_exe_dd[b]) {
+            free_exec(&g->exe_dd[b]);
+            g->have_exe_dd[b] = 0;
+        }
+}
+
 extern "C" ag_status_t ag_graph_release(ag_graph_t g)
 {
     if (!g)
         return AG_OK;
     if (g_ctx.ready)
         stream_wait(g_ctx.stream, 0);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 2; ++b)
-            if (g->have_exe[a][b])
-                free_exec(&g->exe[a][b]);
+    drop_execs(g);
+    dev_free(g->fwd_off);
+    dev_free(g->fwd_dst);
+    dev_free(g->wl);
     dev_free(g->row_off);
     dev_free(g->ids);
     dev_free(g->perm);
@@ -882,16 +904,27 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     return p;
 }
 
-static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
+static int pull_mode(const ag_graph_s *g, int dd)
 {
-    AgExec *x = &g->exe[prec][exact];
+    return dd ? AG_MODE_DD : (g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR);
+}
+
+static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
+{
+    AgExec *x = dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
     memset(x, 0, sizeof(*x));
     AG_CUDA(cudaGraphCreate(&x->graph, 0));
     AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
     x->params.use_cond = 1;
-    const void *kpull = ag_pull_kernel_ptr(g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR, prec, exact);
+    if (dd) {
+        x->params.wl0 = g->wl;
+        x->params.wl1 = g->wl + g->N;
+        x->params.fwd_off = g->fwd_off;
+        x->params.fwd_dst = g->fwd_dst;
+    }
+    const void *kpull = ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
     x->grid = pull_grid(kpull, x->params.ntasks, pull_smem(g));
 
     AgRunConfig run;
@@ -934,7 +967,41 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact)
     AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
 
     AG_CUDA(cudaGraphInstantiate(&x->exec, x->graph, 0));
-    g->have_exe[prec][exact] = 1;
+    if (dd)
+        g->have_exe_dd[exact] = 1;
+    else
+        g->have_exe[prec][exact] = 1;
+    return AG_OK;
+}
+
+/* data-driven mode: the forward CSR in device numbering (the transpose of
+ * the inverse rows) and the two worklists, made on first use */
+static ag_status_t ensure_dd(ag_graph_s *g)
+{
+    if (g->fwd_off)
+        return AG_OK;
+    if (g->E >= (1u << 31))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven pull handles fewer than 2^31 edges");
+    ag_status_t st = AG_OK;
+    uint32_t *off = (uint32_t *)dev_alloc(g, ((size_t)g->N + 1) * 4, &st);
+    uint32_t *dst = (uint32_t *)dev_alloc(g, (size_t)g->E * 4 + 16, &st);
+    uint8_t *wl = (uint8_t *)dev_alloc(g, 2 * (size_t)g->N + 16, &st);
+    if (st == AG_OK) {
+        cudaError_t e = ag_csr_transpose_device(g->row_off, g->ids, g->N, g->E, off, dst, g_ctx.stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = ag_set_error(AG_ERR_CUDA, "forward CSR for the data-driven pull: %s", cudaGetErrorString(e));
+        }
+    }
+    if (st != AG_OK) {
+        dev_free(off);
+        dev_free(dst);
+        dev_free(wl);
+        return st;
+    }
+    g->fwd_off = off;
+    g->fwd_dst = dst;
+    g->wl = wl;
     return AG_OK;
 }
 
@@ -961,30 +1028,30 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
     if (o.precision < 0 || o.precision > 2)
         return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
-    if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks))
+    if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks || o.data_driven))
         return ag_set_error(AG_ERR_UNSUPPORTED, "a graph union runs the FP32 form without a warm start");
+    const int dd = o.data_driven ? 1 : 0;
+    if (dd && (o.precision != AG_PREC_FP32 || g->norm_n || g->c_base))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven pull runs in FP32 on a whole graph");
     const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
     ag_status_t st = ensure_buffers(g, prec);
     if (st != AG_OK)
+        return st;
+    if (dd && (st = ensure_dd(g)) != AG_OK)
         return st;
     if (o.init_ranks && !g->init_buf) {
         g->init_buf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
         if (st != AG_OK)
             return st;
         /* rebuild cached graphs: their parameters carry the warm-start pointer */
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 2; ++b)
-                if (g->have_exe[a][b]) {
-                    free_exec(&g->exe[a][b]);
-                    g->have_exe[a][b] = 0;
-                }
+        drop_execs(g);
     }
-    if (!g->have_exe[prec][exact]) {
-        st = build_exec(g, prec, exact);
+    if (dd ? !g->have_exe_dd[exact] : !g->have_exe[prec][exact]) {
+        st = build_exec(g, prec, exact, dd);
         if (st != AG_OK)
             return st;
     }
-    AgExec *x = &g->exe[prec][exact];
+    AgExec *x = dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
     cudaStream_t s = g_ctx.stream;
     if (o.init_ranks && g->N)
         AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4,
@@ -1012,7 +1079,7 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         void *ia[2] = {&sp, &run};
         AG_CUDA(cudaLaunchKernel(ki.func, ki.gridDim, ki.blockDim, ia, 0, s));
         void *pa[1] = {&sp};
-        const void *kpull = ag_pull_kernel_ptr(g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR, prec, exact);
+        const void *kpull = ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
         for (uint32_t i = 0; i < run.max_iter; ++i)
             AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, pull_smem(g), s));
         AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
@@ -1387,12 +1454,7 @@ extern "C" ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cf
     g->warm_n = std::max<uint32_t>(cfg->warm_entries, g->hot_n);
     g->tiles.hot_entries = g->hot_n;
     g->tiles.warm_entries = g->warm_n;
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 2; ++b)
-            if (g->have_exe[a][b]) {
-                free_exec(&g->exe[a][b]);
-                g->have_exe[a][b] = 0;
-            }
+    drop_execs(g);
     return stream_wait(s, 0);
 }
 

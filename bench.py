@@ -57,7 +57,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--workload", default="pagerank",
-                   choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe"],
+                   choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe",
+                            "data-driven"],
                    help="pagerank: the headline line (driver contract); the others measure the other forms")
     p.add_argument("--graphs", type=int, default=256, help="multigraph: number of graphs")
     p.add_argument("--train-graphs", type=int, default=200, help="warmstart: training graphs")
@@ -513,6 +514,40 @@ def run_warmstart(a):
           flush=True)
 
 
+def run_data_driven(a):
+    """Data-driven (worklist) pull, the reference's pushpull 6, against the
+    topology-driven pull on the same graph: time to epsilon on the device,
+    passes, accuracy against the FP64 fixpoint, and the CPU oracle of the
+    worklist pull (all host threads) on the same graph."""
+    import time
+    import oracle
+    ag = _gpu_setup()
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g)
+    r64, _ = dg.pagerank_f64(5000, 1e-13)
+    out = {"workload": f"data-driven PageRank pull to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}",
+           "N": N, "E": E}
+    for name, dd in (("topology", False), ("data_driven", True)):
+        dg.pagerank(a.iterations, a.epsilon, data_driven=dd)
+        best = None
+        for _ in range(max(1, a.steps)):
+            r, res, _ = dg.pagerank(a.iterations, a.epsilon, data_driven=dd)
+            if best is None or res.device_ms < best[1].device_ms:
+                best = (r, res)
+        r, res = best
+        rl, mx = _rel(r, r64)
+        out[name] = {"device_ms_to_eps": res.device_ms, "passes": res.passes, "iterations": res.iterations,
+                     "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx}
+    out["speedup_vs_topology"] = out["topology"]["device_ms_to_eps"] / out["data_driven"]["device_ms_to_eps"]
+    t0 = time.perf_counter()
+    ref = oracle.pagerank_dd(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_edges_idx(),
+                             g.out_degree(), g.out_neighbours(), a.iterations, a.epsilon)
+    out["cpu_oracle"] = {"seconds_to_eps": time.perf_counter() - t0, "iterations": ref["iterations"],
+                         "threads": oracle.lib.oracle_max_threads()}
+    print(json.dumps(out), flush=True)
+
+
 def run_rows(a):
     """One graph split by rows over all ranks (NCCL all-gather per pass);
     strong scaling: the whole job solves one graph."""
@@ -576,7 +611,8 @@ def main():
         run_b200(a)
     else:
         {"spmv": run_spmv, "precision": run_precision, "ppr": run_ppr, "multigraph": run_multigraph,
-         "warmstart": run_warmstart, "gather-probe": run_gather_probe}[a.workload](a)
+         "warmstart": run_warmstart, "gather-probe": run_gather_probe,
+         "data-driven": run_data_driven}[a.workload](a)
 
 
 if __name__ == "__main__":

@@ -224,6 +224,12 @@ typedef struct ag_pr_opts
     const float *init_ranks;   /* warm start: num_vertices un-normalised ranks
                                   in caller order; NULL = base_pr everywhere  */
     int32_t init_on_device;    /* nonzero: init_ranks is a device pointer     */
+    int32_t data_driven;       /* nonzero: data-driven (worklist) pull, the
+                                  reference's pushpull 6 (pageRank.c:2810-2969):
+                                  only vertices on the worklist are recomputed,
+                                  a rank is replaced only when it moves by at
+                                  least epsilon, which activates its
+                                  out-neighbours; FP32, one graph              */
 } ag_pr_opts;
 
 typedef struct ag_pr_result

@@ -37,6 +37,9 @@ def _load() -> C.CDLL:
     lib.oracle_pagerank_pull.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p, f32p,
                                          u32p, f64p, f64p, u32p, f64p, f64p, C.c_int]
     lib.oracle_pagerank_pull.restype = C.c_uint32
+    lib.oracle_pagerank_dd.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double,
+                                       f32p, u32p, f64p, u32p, C.c_int]
+    lib.oracle_pagerank_dd.restype = C.c_uint32
     lib.oracle_pagerank_f64.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f64p, C.c_int]
     lib.oracle_pagerank_f64.restype = C.c_uint32
     lib.oracle_ppr.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, u32p, C.c_uint32, C.c_double, f32p,
@@ -108,6 +111,23 @@ def pagerank_pull(in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4, i
                                       C.byref(et), C.byref(rs), _p(ha, u32p), _p(he, f64p), _p(hs, f64p), threads)
     return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
             "rank_sum": rs.value, "active": ha[:passes], "error": he[:passes], "seconds": hs[:passes]}
+
+
+def pagerank_dd(in_idx, in_deg, in_nb, out_idx, out_deg, out_nb, iterations=20, epsilon=1e-4, threads=0):
+    """Data-driven pull (pageRank.c:2810-2969). Returns dict(ranks,
+    iterations, passes, error_total, active)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_idx, out_deg, out_nb = _csr(out_idx, out_deg, out_nb)
+    n = len(in_deg)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    ha = np.zeros(max(iterations, 1), np.uint32)
+    passes = lib.oracle_pagerank_dd(n, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_idx, u32p),
+                                    _p(out_deg, u32p), _p(out_nb, u32p), iterations, epsilon, _p(ranks, f32p),
+                                    C.byref(it), C.byref(et), _p(ha, u32p), threads)
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "active": ha[:passes]}
 
 
 def pagerank_f64(in_idx, in_deg, in_nb, out_deg, max_iter=1000, tol=1e-13, threads=0):

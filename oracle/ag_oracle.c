@@ -177,6 +177,89 @@ uint32_t oracle_pagerank_pull(uint32_t n, const uint32_t *in_idx, const uint32_t
     return passes;
 }
 
+/* Data-driven (worklist) pull, pageRank.c:2810-2969: every vertex starts
+ * active; in each iteration the contributions of all vertices are formed
+ * from the current ranks, every active vertex v gathers its in-edges in
+ * stream order (accumulator starting at 0.0f) and computes
+ * new = base + damp * sum; the residual |new - old| (binary32 subtract,
+ * binary64 compare) is added to error_total for every active vertex; only
+ * when it reaches epsilon is the rank replaced and every out-neighbour of v
+ * (forward CSR) put on the next worklist.  Stops when no vertex changed
+ * (iterations = that iteration's index) or at the cap; ranks / n at the end. */
+uint32_t oracle_pagerank_dd(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                            const uint32_t *out_idx, const uint32_t *out_deg, const uint32_t *out_nb,
+                            uint32_t iterations, double epsilon, float *ranks_out, uint32_t *iterations_out,
+                            double *error_total_out, uint32_t *hist_active, int threads)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    float *pageRanks = ranks_out;
+    float *riDividedOnDiClause = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    uint8_t *wl_curr = (uint8_t *)calloc(n ? n : 1, 1);
+    uint8_t *wl_next = (uint8_t *)calloc(n ? n : 1, 1);
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v;
+
+    for (v = 0; v < n; v++) {
+        pageRanks[v] = base_pr;
+        wl_curr[v] = 1;
+    }
+    for (it = 0; it < iterations; it++) {
+        uint8_t *t;
+        error_total = 0;
+        activeVertices = 0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++) {
+            if (out_deg[v])
+                riDividedOnDiClause[v] = pageRanks[v] / out_deg[v];
+            else
+                riDividedOnDiClause[v] = 0.0f;
+        }
+#pragma omp parallel for reduction(+ : error_total, activeVertices) schedule(dynamic, 1024) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            if (wl_curr[v]) {
+                uint32_t j, b = in_idx[v], d = in_deg[v];
+                float nodeIncomingPR = 0.0f;
+                for (j = b; j < b + d; j++)
+                    nodeIncomingPR += riDividedOnDiClause[in_nb[j]];
+                float oldPageRank = pageRanks[v];
+                float newPageRank = base_pr + (damp * nodeIncomingPR);
+                double error = fabs(newPageRank - oldPageRank);
+                error_total += error / n;
+                if (error >= epsilon) {
+                    pageRanks[v] = newPageRank;
+                    for (j = out_idx[v]; j < out_idx[v] + out_deg[v]; j++) {
+#pragma omp atomic write
+                        wl_next[out_nb[j]] = 1;
+                    }
+                    activeVertices++;
+                }
+            }
+        }
+        t = wl_curr;
+        wl_curr = wl_next;
+        wl_next = t;
+        memset(wl_next, 0, n);
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (activeVertices == 0)
+            break;
+    }
+#pragma omp parallel for num_threads(nt)
+    for (v = 0; v < n; v++)
+        pageRanks[v] = pageRanks[v] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(riDividedOnDiClause);
+    free(wl_curr);
+    free(wl_next);
+    return passes;
+}
+
 /* FP64 fixpoint with the reference's constants ((double)0.85f and
  * (double)(1.0f - 0.85f)): every operation in binary64, iterated until
  * max |r' - r| <= tol or max_iter passes.  ranks_out receives r / n. */

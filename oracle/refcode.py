@@ -62,6 +62,8 @@ def _load():
         lib = C.CDLL(str(LIB))
         lib.pageRankPullGraphCSR.restype = C.POINTER(_PageRankStats)
         lib.pageRankPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
+        lib.pageRankDataDrivenPullGraphCSR.restype = C.POINTER(_PageRankStats)
+        lib.pageRankDataDrivenPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
         lib.freePageRankStats.argtypes = [C.POINTER(_PageRankStats)]
         lib.SPMVPullGraphCSR.restype = C.POINTER(_SPMVStats)
         lib.SPMVPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
@@ -88,6 +90,22 @@ def pagerank_pull(arguments_ptr, graph_ptr, num_vertices: int):
             np.zeros(0, np.float32)
         out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total),
                "gathers": int(lib.refemu_gathers() - g0), "damp": float(s.damp), "base_pr": float(s.base_pr)}
+    finally:
+        lib.freePageRankStats(st)
+    return out
+
+
+def pagerank_dd(arguments_ptr, graph_ptr, num_vertices: int):
+    """Run the reference's pageRankDataDrivenPullGraphCSR (its CPU worklist
+    pull, pageRank.c:2810-2969, no accelerator involved)."""
+    import numpy as np
+    lib = _load()
+    st = lib.pageRankDataDrivenPullGraphCSR(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
+    try:
+        s = st.contents
+        ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
+            np.zeros(0, np.float32)
+        out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total)}
     finally:
         lib.freePageRankStats(st)
     return out

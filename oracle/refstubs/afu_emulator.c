@@ -20,7 +20,9 @@
  *     unweighted constant 0.0001f (SPMV.c:1206);
  *   - the other runtime calls only check their arguments.
  * It is compiled with -ffp-contract=off so that every product is rounded
- * before it is added.  It also supplies OpenGraph's timer and my_malloc.  The gather runs over
+ * before it is added.  It also supplies OpenGraph's timer, my_malloc and
+ * the two worklist helpers of the data-driven variant (clear a byte list,
+ * swap two list pointers).  The gather runs over
  * vertices with OpenMP, schedule(dynamic, 1024), as the reference's CPU
  * gathers do (pageRank.c:2898-2907).
  */
@@ -34,6 +36,7 @@
 #include "graphConfig.h"
 #include "capienv.h"
 #include "timer.h"
+#include "worklist.h"
 
 static int g_emu_kernel = 0; /* 0: PageRank CU, 1: SpMV CU */
 static struct WEDGraphCSR *g_emu_wed = NULL;
@@ -48,6 +51,15 @@ double Seconds(struct Timer *timer)
 {
     return (double)(timer->end_time.tv_sec - timer->start_time.tv_sec) +
            (double)(timer->end_time.tv_nsec - timer->start_time.tv_nsec) * 1e-9;
+}
+
+void resetWorkList(uint8_t *workList, uint32_t size) { memset(workList, 0, size); }
+
+void swapWorkLists(uint8_t **workList1, uint8_t **workList2)
+{
+    uint8_t *t = *workList1;
+    *workList1 = *workList2;
+    *workList2 = t;
 }
 
 void *my_malloc(size_t size)
