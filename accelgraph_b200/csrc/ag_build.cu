@@ -367,52 +367,3 @@ done:
     }
     return err;
 }
-
-/* row id of every entry: one warp per row, lanes stride over the row */
-__global__ void ag_build_expand_rows_kernel(const uint32_t *row_off, uint32_t n, uint32_t *rows)
-{
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
-        const uint32_t b = row_off[v], e = row_off[v + 1];
-        for (uint32_t j = b + lane; j < e; j += 32)
-            rows[j] = v;
-    }
-}
-
-extern "C" cudaError_t ag_csr_transpose_device(const uint32_t *row_off, const uint32_t *ids, uint32_t n, uint32_t e,
-                                               uint32_t *t_off, uint32_t *t_idx, cudaStream_t s)
-{
-    cudaError_t err = cudaSuccess;
-    const unsigned B = 256;
-    uint32_t *rows = nullptr, *cols = nullptr;
-    void *tmp = nullptr;
-    size_t tmp_bytes = 0;
-    const int nb = bits_for(n > 0 ? (uint64_t)(n - 1) : 0);
-    if (e == 0) {
-        BUILD_CUDA(cudaMemsetAsync(t_off, 0, ((size_t)n + 1) * 4, s));
-        return cudaSuccess;
-    }
-    BUILD_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                               (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)e, 0, nb, s));
-    BUILD_CUDA(cudaMallocAsync(&tmp, tmp_bytes ? tmp_bytes : 16, s));
-    BUILD_CUDA(cudaMallocAsync((void **)&rows, (size_t)e * 4, s));
-    BUILD_CUDA(cudaMallocAsync((void **)&cols, (size_t)e * 4, s));
-    ag_build_expand_rows_kernel<<<grid_for((uint64_t)n * 32, B), B, 0, s>>>(row_off, n, rows);
-    BUILD_CUDA(cudaGetLastError());
-    /* stable by column: within a column, rows keep their increasing order */
-    {
-        size_t tb = tmp_bytes;
-        BUILD_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, ids, cols, rows, t_idx, (int)e, 0, nb, s));
-    }
-    ag_build_row_starts_kernel<<<grid_for((uint64_t)n + 1, B), B, 0, s>>>(cols, e, n, t_off);
-    BUILD_CUDA(cudaGetLastError());
-done:
-    if (tmp)
-        cudaFreeAsync(tmp, s);
-    if (rows)
-        cudaFreeAsync(rows, s);
-    if (cols)
-        cudaFreeAsync(cols, s);
-    return err;
-}

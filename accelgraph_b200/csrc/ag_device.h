@@ -81,10 +81,11 @@
 #define AG_MODE_SPMV 1
 #define AG_MODE_MULTI 2   /* PageRank over a union of independent graphs,
                              each with its own convergence                  */
-#define AG_MODE_DD 3      /* data-driven PageRank: only vertices on the
-                             worklist are recomputed, and only a change of
-                             at least epsilon replaces a rank and puts the
-                             out-neighbours on the next worklist            */
+#define AG_MODE_DD 3      /* data-driven PageRank: a rank is replaced only
+                             when it moves by at least epsilon, and only rows
+                             with a changed in-neighbour (or the first pass)
+                             are updated; a change is signalled by the sign
+                             bit of the contribution written                */
 
 #define AG_SPMV_W_GRAPH 0 /* multiply by the uploaded weight                */
 #define AG_SPMV_W_CONST 1 /* multiply by 0.0001f (graph without weights)    */
@@ -157,11 +158,6 @@ typedef struct AgPullParams
     uint32_t hot_n16;      /* entries of the same table in 16-bit passes       */
     uint32_t warm_n;       /* gathers of ids in [hot_n, warm_n) may take L1
                               lines; colder ones bypass L1                     */
-    /* data-driven mode: byte worklists in device order (pass p reads
-     * wl[p & 1], clearing what it reads, and fills wl[(p + 1) & 1]) and the
-     * forward CSR in device numbering, for the activations */
-    uint8_t *wl0, *wl1;
-    const uint32_t *fwd_off, *fwd_dst;
     const uint32_t *perm;  /* device row i is caller vertex perm[i]            */
     const uint32_t *inv;   /* caller vertex v is device row inv[v]             */
     float *out;            /* normalised ranks in caller order                 */
@@ -224,10 +220,7 @@ extern "C" {
 cudaError_t ag_csr_build_device(uint32_t n, uint32_t m, const uint32_t *src, const uint32_t *dst, const float *w,
                                 uint32_t flags, AgDevCSR *out, uint32_t *bad_edge, cudaStream_t s);
 void ag_csr_free_device(AgDevCSR *c, cudaStream_t s);
-/* transpose of a CSR (n rows, e entries): t_off[n + 1], t_idx[e] list, for
- * every column u, the rows holding u in increasing row order */
-cudaError_t ag_csr_transpose_device(const uint32_t *row_off, const uint32_t *ids, uint32_t n, uint32_t e,
-                                    uint32_t *t_off, uint32_t *t_idx, cudaStream_t s);
+
 
 /* count items per segment and copy the four totals to totals_host (the copy
  * is stream-ordered: wait on the stream before reading them) */

@@ -249,7 +249,7 @@ struct AgPass
     const float *hot32;     /* shared-memory copy of the first hot_n values */
     const uint16_t *hot16;
     uint32_t hot_n;
-    uint8_t *wl_cur, *wl_nxt; /* data-driven mode: this pass's worklist, the next one */
+    bool dd_all;              /* data-driven mode: the first pass, where every row is active */
 
     __device__ __forceinline__ AgPass(const AgPullParams &pp) : p(pp)
     {
@@ -266,7 +266,7 @@ struct AgPass
         c_in16 = nullptr;
         c_out32 = nullptr;
         c_out16 = nullptr;
-        wl_cur = wl_nxt = nullptr;
+        dd_all = false;
         if (MODE != AG_MODE_SPMV) {
             const uint32_t pass = p.ctl->iter;
             eps = p.ctl->eps;
@@ -279,10 +279,8 @@ struct AgPass
             c_out32 = odd ? p.c32_0 : p.c32_1;
             c_in16 = odd ? p.c16_1 : p.c16_0;
             c_out16 = odd ? p.c16_0 : p.c16_1;
-            if (MODE == AG_MODE_DD) {
-                wl_cur = odd ? p.wl1 : p.wl0;
-                wl_nxt = odd ? p.wl0 : p.wl1;
-            }
+            if (MODE == AG_MODE_DD)
+                dd_all = pass == 0;
         }
     }
 
@@ -337,37 +335,34 @@ struct AgPass
             ag_st_keep_f32(c_out32 + p.c_base + r, c, pol_last);
     }
 
-    /* data-driven update of an active row (pageRank.c:2896-2916): the
-     * residual of every active row counts, but the rank and its contribution
-     * are replaced only when it moved by at least epsilon; returns whether
-     * they were (the row's out-neighbours are then activated) */
-    __device__ __forceinline__ bool finish_dd(uint32_t r, float s, float rp, uint32_t od)
+    /* Data-driven mode (the reference's worklist pull, pageRank.c:2810-2969).
+     * A row is on the worklist of a pass when the pass is the first or one of
+     * its in-neighbours changed in the pass before.  A vertex that changes
+     * writes its next contribution with the sign bit set (contributions are
+     * otherwise never negative), so a row learns that from the values it
+     * gathers anyway: it sums their magnitudes, which are the reference's
+     * contributions bit for bit, and ORs their sign bits.  Nothing is
+     * scattered to out-neighbours. */
+    static __device__ __forceinline__ uint32_t dd_neg(float v) { return __float_as_uint(v) >> 31; }
+
+    /* the update of a row (pageRank.c:2896-2916): rows off the worklist and
+     * rows that moved by less than epsilon keep rank and contribution (sign
+     * cleared); an active row's residual always counts */
+    __device__ __forceinline__ void finish_dd(uint32_t r, float s, float rp, uint32_t od, bool act)
     {
-        const float rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
-        const double err = (double)fabsf(__fsub_rn(rn, rp));
-        my_err += err;
-        if (err >= eps) {
-            p.rank[r] = rn;
-            ag_st_keep_f32(c_out32 + r, od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f, pol_last);
-            ++my_active;
-            return true;
+        if (act) {
+            const float rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
+            const double err = (double)fabsf(__fsub_rn(rn, rp));
+            my_err += err;
+            if (err >= eps) {
+                p.rank[r] = rn;
+                const float c = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
+                ag_st_keep_f32(c_out32 + r, __uint_as_float(__float_as_uint(c) | 0x80000000u), pol_last);
+                ++my_active;
+                return;
+            }
         }
-        keep_dd(r);
-        return false;
-    }
-
-    /* a row whose rank stays keeps its contribution in the next buffer */
-    __device__ __forceinline__ void keep_dd(uint32_t r) const
-    {
-        ag_st_keep_f32(c_out32 + r, __ldg(c_in32 + r), pol_last);
-    }
-
-    /* the whole warp puts row r's out-neighbours on the next worklist */
-    __device__ __forceinline__ void activate(uint32_t r, uint32_t lane) const
-    {
-        const uint32_t a = __ldg(p.fwd_off + r), b = __ldg(p.fwd_off + r + 1);
-        for (uint32_t j = a + lane; j < b; j += 32)
-            wl_nxt[__ldg(p.fwd_dst + j)] = 1;
+        ag_st_keep_f32(c_out32 + r, fabsf(__ldg(c_in32 + r)), pol_last);
     }
 
     /* two 16-byte groups of in-edges per lane: quads qa and qa + 32 (ids and,
@@ -485,7 +480,7 @@ struct AgPass
      * the next pair is in flight while the current one is gathered and
      * added (fixed lane assignment, edge order within a lane) */
     __device__ __forceinline__ float strided_partial(uint32_t eb, uint32_t ee, uint32_t lane,
-                                                     const Pair &first) const
+                                                     const Pair &first, uint32_t &neg) const
     {
         /* two rounds of gathers in flight: the values of round k are added
          * while those of round k + 1 travel and the ids of round k + 2 load.
@@ -524,7 +519,12 @@ struct AgPass
             gather8(nxt, qn, eb, ee, vn, in);
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                s = __fadd_rn(s, v[k]);
+                if (MODE == AG_MODE_DD) {
+                    neg |= dd_neg(v[k]);
+                    s = __fadd_rn(s, fabsf(v[k]));
+                } else {
+                    s = __fadd_rn(s, v[k]);
+                }
                 v[k] = vn[k];
             }
             nxt = nn;
@@ -535,7 +535,8 @@ struct AgPass
 
     /* stream-order sum of in-edges [eb, ee) on one warp: stage AG_WCAP
      * values at a time, lane 0 adds them one by one (EXACT order) */
-    __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane) const
+    __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
+                                                 uint32_t &neg) const
     {
         float s = 0.0f;
         for (uint32_t cb = eb; cb < ee; cb += AG_WCAP) {
@@ -546,10 +547,18 @@ struct AgPass
                 uint32_t j = 0;
                 if (cb == eb) {
                     s = vals[0];
+                    if (MODE == AG_MODE_DD) {
+                        neg |= dd_neg(s);
+                        s = fabsf(s);
+                    }
                     j = 1;
                 }
-                for (; j < ce - cb; ++j)
-                    s = __fadd_rn(s, vals[j]);
+                for (; j < ce - cb; ++j) {
+                    const float v = vals[j];
+                    if (MODE == AG_MODE_DD)
+                        neg |= dd_neg(v);
+                    s = __fadd_rn(s, MODE == AG_MODE_DD ? fabsf(v) : v);
+                }
             }
             __syncwarp();
         }
@@ -636,76 +645,66 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             }
         }
         if (MODE == AG_MODE_DD && kind == AG_T_ROWS) {
-            /* data-driven: rows off the worklist keep rank and contribution;
-             * an item without an active row gathers nothing.  Each flag read
-             * is cleared, so this pass's list is empty for the pass after
-             * next, which fills it. */
+            /* data-driven: the sums are those of the plain pull over the
+             * gathered magnitudes; a row is active when the pass is the first
+             * or a gathered value carries the sign of a change */
             const uint32_t r = r0 + lane;
             const bool live = r < task.y;
-            bool act = false;
+            uint32_t o0 = ee, o1 = ee, od = 0;
+            float rp = 0.0f;
             if (live) {
-                act = ps.wl_cur[r] != 0;
-                if (act)
-                    ps.wl_cur[r] = 0;
+                o0 = ag_ld_row_u32(p.row_off + r);
+                o1 = ag_ld_row_u32(p.row_off + r + 1);
+                rp = ag_ld_rank(p.rank + r);
+                od = ag_ld_row_u32(p.outdeg + r);
             }
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
-            if (!__any_sync(0xffffffffu, act)) {
-                if (live)
-                    ps.keep_dd(r);
+            ps.stage(vals, eb, ee, lane, pf);
+            __syncwarp();
+            o0 -= eb;
+            o1 -= eb;
+            float s = 0.0f;
+            uint32_t neg = 0;
+            bool is_long = false;
+            if (EXACT || o1 - o0 <= AG_TSEQ) {
+                if (o1 > o0) {
+                    float v = vals[o0];
+                    neg = ps.dd_neg(v);
+                    s = fabsf(v);
+                    for (uint32_t j = o0 + 1; j < o1; ++j) {
+                        v = vals[j];
+                        neg |= ps.dd_neg(v);
+                        s = __fadd_rn(s, fabsf(v));
+                    }
+                }
             } else {
-                uint32_t o0 = ee, o1 = ee, od = 0;
-                float rp = 0.0f;
-                if (live) {
-                    o0 = ag_ld_row_u32(p.row_off + r);
-                    o1 = ag_ld_row_u32(p.row_off + r + 1);
-                    rp = ag_ld_rank(p.rank + r);
-                    od = ag_ld_row_u32(p.outdeg + r);
-                }
-                ps.stage(vals, eb, ee, lane, pf);
-                __syncwarp();
-                o0 -= eb;
-                o1 -= eb;
-                float s = 0.0f;
-                bool is_long = false;
-                if (act) {
-                    if (EXACT || o1 - o0 <= AG_TSEQ) {
-                        if (o1 > o0) {
-                            s = vals[o0];
-                            for (uint32_t j = o0 + 1; j < o1; ++j)
-                                s = __fadd_rn(s, vals[j]);
-                        }
-                    } else {
-                        is_long = true;
-                    }
-                }
-                if (!EXACT) {
-                    unsigned m = __ballot_sync(0xffffffffu, is_long);
-                    while (m) {
-                        const int src = __ffs(m) - 1;
-                        m &= m - 1;
-                        const uint32_t a = __shfl_sync(0xffffffffu, o0, src);
-                        const uint32_t b = __shfl_sync(0xffffffffu, o1, src);
-                        float tsum = 0.0f;
-                        for (uint32_t j = a + lane; j < b; j += 32)
-                            tsum = __fadd_rn(tsum, vals[j]);
-                        tsum = ag_warp_sum_f(tsum);
-                        if ((int)lane == src)
-                            s = tsum;
-                    }
-                }
-                bool changed = false;
-                if (act)
-                    changed = ps.finish_dd(r, s, rp, od);
-                else if (live)
-                    ps.keep_dd(r);
-                __syncwarp();
-                unsigned m = __ballot_sync(0xffffffffu, changed);
+                is_long = true;
+            }
+            if (!EXACT) {
+                unsigned m = __ballot_sync(0xffffffffu, is_long);
                 while (m) {
                     const int src = __ffs(m) - 1;
                     m &= m - 1;
-                    ps.activate(__shfl_sync(0xffffffffu, r, src), lane);
+                    const uint32_t a = __shfl_sync(0xffffffffu, o0, src);
+                    const uint32_t b = __shfl_sync(0xffffffffu, o1, src);
+                    float tsum = 0.0f;
+                    uint32_t tneg = 0;
+                    for (uint32_t j = a + lane; j < b; j += 32) {
+                        const float v = vals[j];
+                        tneg |= ps.dd_neg(v);
+                        tsum = __fadd_rn(tsum, fabsf(v));
+                    }
+                    tsum = ag_warp_sum_f(tsum);
+                    tneg = __any_sync(0xffffffffu, tneg) ? 1u : 0u;
+                    if ((int)lane == src) {
+                        s = tsum;
+                        neg = tneg;
+                    }
                 }
             }
+            if (live)
+                ps.finish_dd(r, s, rp, od, ps.dd_all || neg);
+            __syncwarp();
             pf = pn;
         } else if (kind == AG_T_ROWS) {
             /* one row per lane; its bounds, previous rank and out-degree are
@@ -764,35 +763,25 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         } else if (kind == AG_T_LONG) {
             float rp = 0.0f;
             uint32_t od = 0;
-            const bool act = MODE != AG_MODE_DD || ps.wl_cur[r0] != 0;
             if (MODE != AG_MODE_SPMV && lane == 0) {
                 rp = p.rank[r0];
                 od = p.outdeg[r0];
             }
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
-            if (!act) {
-                if (lane == 0)
-                    ps.keep_dd(r0);
+            float s;
+            uint32_t neg = 0;
+            if (EXACT) {
+                s = ps.ordered_sum(vals, eb, ee, lane, neg);
             } else {
-                float s;
-                if (EXACT) {
-                    s = ps.ordered_sum(vals, eb, ee, lane);
-                } else {
-                    s = ps.strided_partial(eb, ee, lane, pf);
-                    s = ag_warp_sum_f(s);
-                }
-                if (MODE == AG_MODE_DD) {
-                    /* every lane has read the flag before the sum's shuffles */
-                    bool changed = false;
-                    if (lane == 0) {
-                        changed = ps.finish_dd(r0, s, rp, od);
-                        ps.wl_cur[r0] = 0;
-                    }
-                    if (__shfl_sync(0xffffffffu, changed, 0))
-                        ps.activate(r0, lane);
-                } else if (lane == 0) {
-                    ps.finish(r0, s, rp, od);
-                }
+                s = ps.strided_partial(eb, ee, lane, pf, neg);
+                s = ag_warp_sum_f(s);
+            }
+            if (MODE == AG_MODE_DD) {
+                const bool act = ps.dd_all || __any_sync(0xffffffffu, neg);
+                if (lane == 0)
+                    ps.finish_dd(r0, s, rp, od, act);
+            } else if (lane == 0) {
+                ps.finish(r0, s, rp, od);
             }
             __syncwarp();
             pf = pn;
@@ -803,23 +792,13 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             if (lane == 0)
                 deg = p.row_off[r0 + 1] - p.row_off[r0];
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
-            /* data-driven: a row off the worklist is skipped by all its
-             * chunks (chunk 0 keeps its contribution); the flag of an active
-             * row is cleared by the last chunk to arrive, after every chunk
-             * has read it */
-            const bool act = MODE != AG_MODE_DD || ps.wl_cur[r0] != 0;
-            if (!act) {
-                if (chunk == 0 && lane == 0)
-                    ps.keep_dd(r0);
-                __syncwarp();
-                pf = pn;
-                task = task_n;
-                t = tn;
-                continue;
-            }
-            float s = ps.strided_partial(eb, ee, lane, pf);
+            /* data-driven: each chunk's partial carries the sign of a change
+             * among its in-neighbours; the last chunk ORs them */
+            uint32_t neg = 0;
+            float s = ps.strided_partial(eb, ee, lane, pf, neg);
             s = ag_warp_sum_f(s);
-            bool changed = false;
+            if (MODE == AG_MODE_DD && __any_sync(0xffffffffu, neg))
+                s = __uint_as_float(__float_as_uint(s) | 0x80000000u);
             if (lane == 0) {
                 const uint32_t nch = (deg + p.whub - 1) / p.whub;
                 p.hub_part[pbase + chunk] = s;
@@ -828,8 +807,17 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 if (prev == nch - 1) {
                     __threadfence();
                     float tot = __ldcg(p.hub_part + pbase);
-                    for (uint32_t c = 1; c < nch; ++c)
-                        tot = __fadd_rn(tot, __ldcg(p.hub_part + pbase + c));
+                    uint32_t any = 0;
+                    if (MODE == AG_MODE_DD) {
+                        any = ps.dd_neg(tot);
+                        tot = fabsf(tot);
+                    }
+                    for (uint32_t c = 1; c < nch; ++c) {
+                        const float part = __ldcg(p.hub_part + pbase + c);
+                        if (MODE == AG_MODE_DD)
+                            any |= ps.dd_neg(part);
+                        tot = __fadd_rn(tot, MODE == AG_MODE_DD ? fabsf(part) : part);
+                    }
                     p.hub_cnt[pbase] = 0;
                     float rp = 0.0f;
                     uint32_t od = 0;
@@ -837,16 +825,12 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                         rp = p.rank[r0];
                         od = p.outdeg[r0];
                     }
-                    if (MODE == AG_MODE_DD) {
-                        changed = ps.finish_dd(r0, tot, rp, od);
-                        ps.wl_cur[r0] = 0;
-                    } else {
+                    if (MODE == AG_MODE_DD)
+                        ps.finish_dd(r0, tot, rp, od, ps.dd_all || any);
+                    else
                         ps.finish(r0, tot, rp, od);
-                    }
                 }
             }
-            if (MODE == AG_MODE_DD && __shfl_sync(0xffffffffu, changed, 0))
-                ps.activate(r0, lane);
             __syncwarp();
             pf = pn;
         }
@@ -1000,11 +984,6 @@ __global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams
             ag_st_keep_u16(p.c16_0 + v, ag_f32_to_low<PREC>(c), pol_last);
         else
             ag_st_keep_f32(p.c32_0 + p.c_base + v, c, pol_last);
-        if (p.wl0) {
-            /* data-driven mode: every vertex starts on the worklist */
-            p.wl0[v] = 1;
-            p.wl1[v] = 0;
-        }
     }
     for (uint32_t g = blockIdx.x * AG_SBLK + threadIdx.x; g < p.ngraphs; g += gridDim.x * AG_SBLK) {
         p.g_active[g] = 0;

@@ -326,10 +326,7 @@ struct ag_graph_s
     uint32_t *flag;
     AgExec exe[3][2];
     int have_exe[3][2];
-    /* data-driven mode: forward CSR in device numbering, two byte worklists,
-     * and its launch graphs (FAST, EXACT) */
-    uint32_t *fwd_off, *fwd_dst;
-    uint8_t *wl;
+    /* data-driven mode: its launch graphs (FAST, EXACT) */
     AgExec exe_dd[2];
     int have_exe_dd[2];
     cudaEvent_t ev0, ev1;
@@ -394,9 +391,6 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     if (g_ctx.ready)
         stream_wait(g_ctx.stream, 0);
     drop_execs(g);
-    dev_free(g->fwd_off);
-    dev_free(g->fwd_dst);
-    dev_free(g->wl);
     dev_free(g->row_off);
     dev_free(g->ids);
     dev_free(g->perm);
@@ -918,12 +912,6 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
     x->params.use_cond = 1;
-    if (dd) {
-        x->params.wl0 = g->wl;
-        x->params.wl1 = g->wl + g->N;
-        x->params.fwd_off = g->fwd_off;
-        x->params.fwd_dst = g->fwd_dst;
-    }
     const void *kpull = ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
     x->grid = pull_grid(kpull, x->params.ntasks, pull_smem(g));
 
@@ -974,37 +962,6 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
     return AG_OK;
 }
 
-/* data-driven mode: the forward CSR in device numbering (the transpose of
- * the inverse rows) and the two worklists, made on first use */
-static ag_status_t ensure_dd(ag_graph_s *g)
-{
-    if (g->fwd_off)
-        return AG_OK;
-    if (g->E >= (1u << 31))
-        return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven pull handles fewer than 2^31 edges");
-    ag_status_t st = AG_OK;
-    uint32_t *off = (uint32_t *)dev_alloc(g, ((size_t)g->N + 1) * 4, &st);
-    uint32_t *dst = (uint32_t *)dev_alloc(g, (size_t)g->E * 4 + 16, &st);
-    uint8_t *wl = (uint8_t *)dev_alloc(g, 2 * (size_t)g->N + 16, &st);
-    if (st == AG_OK) {
-        cudaError_t e = ag_csr_transpose_device(g->row_off, g->ids, g->N, g->E, off, dst, g_ctx.stream);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            st = ag_set_error(AG_ERR_CUDA, "forward CSR for the data-driven pull: %s", cudaGetErrorString(e));
-        }
-    }
-    if (st != AG_OK) {
-        dev_free(off);
-        dev_free(dst);
-        dev_free(wl);
-        return st;
-    }
-    g->fwd_off = off;
-    g->fwd_dst = dst;
-    g->wl = wl;
-    return AG_OK;
-}
-
 extern "C" void ag_pr_opts_init(ag_pr_opts *o)
 {
     if (!o)
@@ -1036,8 +993,6 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
     const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
     ag_status_t st = ensure_buffers(g, prec);
     if (st != AG_OK)
-        return st;
-    if (dd && (st = ensure_dd(g)) != AG_OK)
         return st;
     if (o.init_ranks && !g->init_buf) {
         g->init_buf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
