@@ -49,21 +49,64 @@ __global__ void ag_permuted_degrees_kernel(const uint32_t *perm, const uint32_t 
     }
 }
 
-/* one warp per new row: copy the old row in order, mapping ids through inv */
+/* Rows copied in the new order, mapping ids through inv, rows keeping their
+ * edge order.  The new edge array is cut into segments of AG_COPY_SEG
+ * positions, one warp per segment, so that a row of any length is spread
+ * over many warps.  A warp finds the row holding its first position by a
+ * binary search of the new row starts, then walks its positions 32 at a time
+ * (coalesced stores) over a window of 32 consecutive rows: each lane holds
+ * one row's old start and new start, and a position's row is found by a
+ * five-step binary search over the lanes (shuffles).  When the window's rows
+ * end before the segment does, the window moves on. */
+#define AG_COPY_SEG 2048u
+
 __global__ void ag_copy_rows_kernel(const uint32_t *perm, const uint32_t *inv, const uint32_t *off_old,
                                     const uint32_t *off_new, const uint32_t *ids_old, uint32_t *ids_new,
-                                    const float *w_old, float *w_new, uint32_t n)
+                                    const float *w_old, float *w_new, uint32_t n, uint32_t e)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-        const uint32_t o = perm[i];
-        const uint32_t src = off_old[o], dst = off_new[i];
-        const uint32_t d = off_old[o + 1] - src;
-        for (uint32_t j = lane; j < d; j += 32) {
-            ids_new[dst + j] = inv[ids_old[src + j]];
-            if (w_new)
-                w_new[dst + j] = w_old[src + j];
+    const uint32_t nseg = (e + AG_COPY_SEG - 1) / AG_COPY_SEG;
+    for (uint32_t seg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; seg < nseg; seg += nw) {
+        const uint32_t p0 = seg * AG_COPY_SEG;
+        const uint32_t p1 = min(e, p0 + AG_COPY_SEG);
+        /* the last row starting at or before p0 (rows 0 .. n-1; off_new[n] = e > p0) */
+        uint32_t lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+            if (off_new[mid] <= p0)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        uint32_t rbase = lo, jb = p0;
+        while (jb < p1) {
+            const uint32_t i = rbase + lane;
+            /* lanes past the last row start at e, so no position maps to them */
+            const uint32_t dst = off_new[i < n ? i : n];
+            const uint32_t src = i < n ? off_old[perm[i]] : 0u;
+            const uint32_t wend = off_new[rbase + 32 < n ? rbase + 32 : n];
+            const uint32_t stop = min(p1, wend);
+            for (; jb < stop; jb += 32) {
+                const uint32_t j = jb + lane;
+                /* the last lane whose row starts at or before j owns it (an
+                 * empty row shares its start with the next row, which wins) */
+                uint32_t l = 0;
+#pragma unroll
+                for (uint32_t step = 16; step >= 1; step >>= 1) {
+                    const uint32_t cand = l + step;
+                    if (__shfl_sync(0xffffffffu, dst, cand) <= j)
+                        l = cand;
+                }
+                const uint32_t k = __shfl_sync(0xffffffffu, src, l) + (j - __shfl_sync(0xffffffffu, dst, l));
+                if (j < stop) {
+                    ids_new[j] = inv[ids_old[k]];
+                    if (w_new)
+                        w_new[j] = w_old[k];
+                }
+            }
+            jb = stop;
+            rbase += 32;
         }
     }
 }
@@ -138,8 +181,8 @@ extern "C" cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const u
             goto done;
     }
     if (e > 0)
-        ag_copy_rows_kernel<<<grid_for((uint64_t)n * 32, 256), 256, 0, s>>>(perm, inv, off_old, off_new, ids_old,
-                                                                          ids_new, w_old, w_new, n);
+        ag_copy_rows_kernel<<<grid_for(((uint64_t)e + AG_COPY_SEG - 1) / AG_COPY_SEG * 32, 256), 256, 0, s>>>(
+            perm, inv, off_old, off_new, ids_old, ids_new, w_old, w_new, n, e);
     err = cudaGetLastError();
 done:
     if (iota)
