@@ -37,6 +37,11 @@ def _load() -> C.CDLL:
     lib.oracle_pagerank_pull.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p, f32p,
                                          u32p, f64p, f64p, u32p, f64p, f64p, C.c_int]
     lib.oracle_pagerank_pull.restype = C.c_uint32
+    u64p = C.POINTER(C.c_uint64)
+    lib.oracle_gather_u64.argtypes = [C.c_uint32, u32p, u32p, u32p, u64p, u64p, C.c_int]
+    lib.oracle_pagerank_fixed64.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p,
+                                            u32p, f64p, u32p, C.c_int]
+    lib.oracle_pagerank_fixed64.restype = C.c_uint32
     lib.oracle_pagerank_dd.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double,
                                        f32p, u32p, f64p, u32p, C.c_int]
     lib.oracle_pagerank_dd.restype = C.c_uint32
@@ -111,6 +116,34 @@ def pagerank_pull(in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4, i
                                       C.byref(et), C.byref(rs), _p(ha, u32p), _p(he, f64p), _p(hs, f64p), threads)
     return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
             "rank_sum": rs.value, "active": ha[:passes], "error": he[:passes], "seconds": hs[:passes]}
+
+
+def gather_u64(in_idx, in_deg, in_nb, x, threads=0):
+    """Fixed-point gather: integer sums modulo 2^64 (rows without in-edges 0)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    x = np.ascontiguousarray(x, np.uint64)
+    y = np.zeros(len(in_deg), np.uint64)
+    u64p = C.POINTER(C.c_uint64)
+    lib.oracle_gather_u64(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(x, u64p),
+                          _p(y, u64p), threads)
+    return y
+
+
+def pagerank_fixed64(in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4, threads=0):
+    """64-bit fixed-point pull (pageRank.c:1276-1453). Returns dict(ranks,
+    iterations, passes, error_total, active)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    n = len(in_deg)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    ha = np.zeros(max(iterations, 1), np.uint32)
+    passes = lib.oracle_pagerank_fixed64(n, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_deg, u32p),
+                                         iterations, epsilon, _p(ranks, f32p), C.byref(it), C.byref(et),
+                                         _p(ha, u32p), threads)
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "active": ha[:passes]}
 
 
 def pagerank_dd(in_idx, in_deg, in_nb, out_idx, out_deg, out_nb, iterations=20, epsilon=1e-4, threads=0):

@@ -177,6 +177,92 @@ uint32_t oracle_pagerank_pull(uint32_t n, const uint32_t *in_idx, const uint32_t
     return passes;
 }
 
+/* Fixed-point conversions of the 64-bit pull (OpenGraph's fixedPoint.h is
+ * absent from the reference checkout; restated as 32 fractional bits, the
+ * conversion to fixed point truncating toward zero). */
+#define ORACLE_FIXED64_ONE 4294967296.0
+static inline uint64_t oracle_d2fixed64(double x) { return (uint64_t)(int64_t)(x * ORACLE_FIXED64_ONE); }
+static inline double oracle_fixed64_2d(uint64_t x) { return (double)(int64_t)x / ORACLE_FIXED64_ONE; }
+
+/* fixed-point gather: y[v] = sum of x[u] over v's in-edges, modulo 2^64,
+ * for every vertex with in-edges (pagerank_kernel_tb.sv:13-16, 303-314) */
+void oracle_gather_u64(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                       const uint64_t *x, uint64_t *y, int threads)
+{
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    uint32_t v;
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nt)
+    for (v = 0; v < n; v++) {
+        uint64_t s = 0;
+        uint32_t j;
+        if (!in_deg[v])
+            continue;
+        for (j = in_idx[v]; j < in_idx[v] + in_deg[v]; j++)
+            s += x[in_nb[j]];
+        y[v] = s;
+    }
+}
+
+/* 64-bit fixed-point pull, pageRank.c:1276-1453 (pushpull 2): contributions
+ * DoubleToFixed64(r / out_degree) (binary32 division), the accelerator's
+ * integer sums, and the update base + damp * Fixed64ToDouble(sum) evaluated in
+ * binary64 and stored in binary32; residual, stop test and normalisation as
+ * in the plain pull. */
+uint32_t oracle_pagerank_fixed64(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                                 const uint32_t *out_deg, uint32_t iterations, double epsilon, float *ranks_out,
+                                 uint32_t *iterations_out, double *error_total_out, uint32_t *hist_active,
+                                 int threads)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    float *pageRanks = ranks_out;
+    uint64_t *next = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
+    uint64_t *contrib = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v;
+    for (v = 0; v < n; v++)
+        pageRanks[v] = base_pr;
+    for (it = 0; it < iterations; it++) {
+        error_total = 0;
+        activeVertices = 0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++) {
+            if (out_deg[v])
+                contrib[v] = oracle_d2fixed64(pageRanks[v] / out_deg[v]);
+            else
+                contrib[v] = 0;
+        }
+        oracle_gather_u64(n, in_idx, in_deg, in_nb, contrib, next, nt);
+#pragma omp parallel for reduction(+ : error_total, activeVertices) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            float prevPageRank = pageRanks[v];
+            float nextPageRank = base_pr + (damp * oracle_fixed64_2d(next[v]));
+            pageRanks[v] = nextPageRank;
+            next[v] = 0;
+            double error = fabs(nextPageRank - prevPageRank);
+            error_total += (error / n);
+            if (error >= epsilon)
+                activeVertices++;
+        }
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (activeVertices == 0)
+            break;
+    }
+#pragma omp parallel for num_threads(nt)
+    for (v = 0; v < n; v++)
+        pageRanks[v] = pageRanks[v] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(next);
+    free(contrib);
+    return passes;
+}
+
 /* Data-driven (worklist) pull, pageRank.c:2810-2969: every vertex starts
  * active; in each iteration the contributions of all vertices are formed
  * from the current ranks, every active vertex v gathers its in-edges in

@@ -64,6 +64,8 @@ def _load():
         lib.pageRankPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
         lib.pageRankDataDrivenPullGraphCSR.restype = C.POINTER(_PageRankStats)
         lib.pageRankDataDrivenPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
+        lib.pageRankPullFixedPoint64BitGraphCSR.restype = C.POINTER(_PageRankStats)
+        lib.pageRankPullFixedPoint64BitGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
         lib.freePageRankStats.argtypes = [C.POINTER(_PageRankStats)]
         lib.SPMVPullGraphCSR.restype = C.POINTER(_SPMVStats)
         lib.SPMVPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
@@ -106,6 +108,26 @@ def pagerank_dd(arguments_ptr, graph_ptr, num_vertices: int):
         ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
             np.zeros(0, np.float32)
         out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total)}
+    finally:
+        lib.freePageRankStats(st)
+    return out
+
+
+def pagerank_fixed64(arguments_ptr, graph_ptr, num_vertices: int):
+    """Run the reference's pageRankPullFixedPoint64BitGraphCSR (pushpull 2,
+    pageRank.c:1276-1453) with the emulated fixed-point gather and the
+    stand-in conversions of oracle/refstubs/fixedPoint.h."""
+    import numpy as np
+    lib = _load()
+    lib.refemu_set_kernel(2)
+    g0 = lib.refemu_gathers()
+    st = lib.pageRankPullFixedPoint64BitGraphCSR(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
+    try:
+        s = st.contents
+        ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
+            np.zeros(0, np.float32)
+        out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total),
+               "gathers": int(lib.refemu_gathers() - g0)}
     finally:
         lib.freePageRankStats(st)
     return out

@@ -13,7 +13,9 @@
  *     vertex v with in-edges, auxiliary2[v] = sum over its in-edges j, in
  *     stream order, of auxiliary1[src_j] (PageRank CU) or w_j * auxiliary1[src_j]
  *     (SpMV CU, binary32 multiply then add), the accumulator starting from the
- *     first value; vertices without in-edges are not written.  These are the
+ *     first value, or the exact modulo-2^64 integer sum of 64-bit
+ *     contributions (fixed-point PageRank CU, pagerank_kernel_tb.sv:13-16);
+ *     vertices without in-edges are not written.  These are the
  *     compute units' semantics (cu_sum_kernel_control.sv, golden models
  *     pagerank_kernel_tb.sv:303-314, spmv_kernel_tb.sv:304,359).  With no
  *     weight array (WEIGHTED = 0) the SpMV weight is the reference's
@@ -38,11 +40,11 @@
 #include "timer.h"
 #include "worklist.h"
 
-static int g_emu_kernel = 0; /* 0: PageRank CU, 1: SpMV CU */
+static int g_emu_kernel = 0; /* 0: PageRank CU, 1: SpMV CU, 2: fixed-point PageRank CU */
 static struct WEDGraphCSR *g_emu_wed = NULL;
 static uint64_t g_emu_runs = 0;
 
-void refemu_set_kernel(int spmv) { g_emu_kernel = spmv ? 1 : 0; }
+void refemu_set_kernel(int kind) { g_emu_kernel = (kind == 1 || kind == 2) ? kind : 0; }
 uint64_t refemu_gathers(void) { return g_emu_runs; }
 
 void Start(struct Timer *timer) { clock_gettime(CLOCK_MONOTONIC, &timer->start_time); }
@@ -134,8 +136,28 @@ void waitAFU(struct cxl_afu_h **afu, struct AFUStatus *afu_status)
     const float *wt = (const float *)w->inverse_edges_array_weight;
     const float *x = (const float *)w->auxiliary1;
     float *y = (float *)w->auxiliary2;
-    const int spmv = g_emu_kernel;
+    const int spmv = g_emu_kernel == 1;
     int64_t v;
+    if (g_emu_kernel == 2) {
+        /* fixed-point CU: 64-bit contributions, exact integer sum modulo 2^64
+         * (pagerank_kernel_tb.sv:13-16) */
+        const uint64_t *x64 = (const uint64_t *)w->auxiliary1;
+        uint64_t *y64 = (uint64_t *)w->auxiliary2;
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (v = 0; v < (int64_t)n; ++v) {
+            const uint32_t d = deg[v], b = idx[v];
+            uint64_t s = 0;
+            if (!d)
+                continue;
+            for (uint32_t j = 0; j < d; ++j)
+                s += x64[src[b + j]];
+            y64[v] = s;
+        }
+        afu_status->cu_return_done = n;
+        afu_status->cu_status = 0;
+        ++g_emu_runs;
+        return;
+    }
 #pragma omp parallel for schedule(dynamic, 1024)
     for (v = 0; v < (int64_t)n; ++v) {
         const uint32_t d = deg[v], b = idx[v];

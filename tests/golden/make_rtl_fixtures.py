@@ -8,7 +8,9 @@ testbenches (AccelGraph,
   pagerank_kernel_tb.sv  contribution classes (:242-265), the run list
                          (:660-720) and the stream-order binary32 golden
                          (:303-314): the accumulator restarts with the first
-                         value of a row and adds each following value
+                         value of a row and adds each following value; for
+                         the FixedPoint context the 64-bit contributions
+                         (:256-263) and their exact sum modulo 2^64 (:13-16)
   spmv_kernel_tb.sv      coefficients w/2 (:277-293), product x*w in binary32
                          (:296-301) and the same stream-order sum (:349-359)
 and the 19-edge binary edge list 04_test_graphs/TEST/graphbrew/graph.bin.
@@ -92,6 +94,33 @@ def main() -> None:
             return -(f32(k + 1) / f32(7))
         return f32(nb + 1) / f32(3)
 
+    def contribution_fixed(cls: int, nb: int, k: int) -> int:
+        """the FixedPoint context's 64-bit contributions (pagerank_kernel_tb.sv:256-263)"""
+        if cls == 1:
+            return 0
+        if cls == 2:
+            return (1 << 64) - 1
+        if cls == 3:
+            return 0xFFFF_FFFF_0000_0001 if k % 2 == 0 else (nb + 1) * 7
+        return (nb + 1) * 7 + k
+
+    def fixed_runs():
+        text = (TB / "pagerank_kernel_tb.sv").read_text()
+        out = []
+        for m in re.finditer(r"run_fixture\((FX_[A-Z0-9_]+)\s*,\s*(CV_[A-Z]+)\s*,\s*0\s*\)", text):
+            fx, cls = names[m.group(1)], cv[m.group(2)]
+            fxd = fixtures[fx]
+            rows = []
+            for v in range(fxd["num_vertices"]):
+                nbs = fxd["inverse_neighbours"][v]
+                if not nbs:
+                    continue
+                vals = [contribution_fixed(cls, nb, k) for k, nb in enumerate(nbs)]
+                acc = sum(vals) % (1 << 64)  # exact sum, wraps modulo 2^64 (:13-16, :312)
+                rows.append({"v": v, "elements": ["%016x" % x for x in vals], "golden": "%016x" % acc})
+            out.append({"fixture": fxd["name"], "fixture_id": fx, "class": m.group(2), "rows": rows})
+        return out
+
     def coefficient(cls: int, weight: int):
         if cls == 1:
             return f32(0.0)
@@ -147,11 +176,13 @@ def main() -> None:
         "fixtures": fixtures,
         "pagerank_runs": runs("pagerank_kernel_tb.sv", weighted=False),
         "spmv_runs": runs("spmv_kernel_tb.sv", weighted=True),
+        "pagerank_fixed_runs": fixed_runs(),
         "fp_exception_rows": exc,
         "graphbrew": {"src": raw[:, 0].tolist(), "dst": raw[:, 1].tolist()},
     }
     OUT.write_text(json.dumps(doc, indent=1) + "\n")
     print(f"wrote {OUT}: {len(fixtures)} fixtures, {len(doc['pagerank_runs'])} pagerank runs, "
+          f"{len(doc['pagerank_fixed_runs'])} fixed-point runs, "
           f"{len(doc['spmv_runs'])} spmv runs, graphbrew {len(raw)} edges")
 
 

@@ -130,3 +130,19 @@ def test_oracle_f64_fixpoint_is_a_fixpoint(oracle):
     np.add.at(s, dst, c[src])
     nxt = float(np.float32(1.0) - np.float32(0.85)) + float(np.float32(0.85)) * s
     assert np.max(np.abs(nxt - rr)) < 1e-12
+
+
+@pytest.mark.parametrize("i", range(13))
+def test_oracle_fixed_gather_matches_rtl_golden(rtl, oracle, i):
+    """FixedPoint context: exact integer sums of 64-bit contributions, wrapping
+    modulo 2^64 (pagerank_kernel_tb.sv:13-16, 256-263, 312)."""
+    from conftest import fixed_inputs
+    run = rtl["pagerank_fixed_runs"][i]
+    fx = rtl["fixtures"][run["fixture_id"]]
+    n, deg, idx, nb, x = fixed_inputs(run, fx)
+    y = oracle.gather_u64(idx, deg, nb, x)
+    for row in run["rows"]:
+        assert "%016x" % int(y[row["v"]]) == row["golden"], (run["fixture"], run["class"], row["v"])
+    for v in range(n):
+        if deg[v] == 0:
+            assert y[v] == 0

@@ -73,3 +73,19 @@ def test_oracle_data_driven_equals_reference_code(ag, oracle, refcode, iteration
         # the worklist shrinks: the data-driven solve differs from the topology-driven one
         if epsilon >= 1e-6 and name.startswith("rmat"):
             assert (mine["active"][1:] <= g.num_vertices).all()
+
+
+@pytest.mark.parametrize("iterations,epsilon", [(20, 1e-4), (300, 1e-6)])
+def test_oracle_fixed64_equals_reference_code(ag, oracle, refcode, iterations, epsilon):
+    """The 64-bit fixed-point pull (pushpull 2): the oracle restatement equals
+    the reference's own host code bit for bit (same stand-in conversions)."""
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(iterations, epsilon)
+        args.pushpull = 2
+        ref = refcode.pagerank_fixed64(C.byref(args), g.ptr, g.num_vertices)
+        mine = oracle.pagerank_fixed64(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(),
+                                       iterations, epsilon)
+        assert ref["iterations"] == mine["iterations"], name
+        assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
+        assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
+        assert ref["gathers"] == mine["passes"], name
