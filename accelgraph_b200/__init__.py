@@ -131,7 +131,7 @@ AG_BUILD_DEDUPE, AG_BUILD_SORT, AG_BUILD_PINNED, AG_BUILD_WEIGHTS, AG_BUILD_SYMM
 AG_FILE_TEXT, AG_FILE_BINARY, AG_FILE_CSR = 0, 1, 2
 AG_UPLOAD_WEIGHTS, AG_UPLOAD_VALIDATE, AG_UPLOAD_TRUSTED = 1, 2, 4
 AG_UPLOAD_KEEP_ORDER, AG_UPLOAD_NO_SMEM_CACHE = 8, 16
-AG_PREC_FP32, AG_PREC_BF16, AG_PREC_FP16 = 0, 1, 2
+AG_PREC_FP32, AG_PREC_BF16, AG_PREC_FP16, AG_PREC_FIXED64 = 0, 1, 2, 3
 AG_ORDER_FAST, AG_ORDER_EXACT = 0, 1
 AG_SPMV_GRAPH_WEIGHTS, AG_SPMV_UNIT, AG_SPMV_EXACT = 0, 1, 2
 DAMP = np.float32(0.85)
@@ -175,6 +175,7 @@ SIGNATURES = [
     ("ag_graph_release", C.c_int32, [C.c_void_p]),
     ("ag_graph_get_info", C.c_int32, [C.c_void_p, C.POINTER(GraphInfo)]),
     ("ag_graph_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
+    ("ag_gather_u64", C.c_int32, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("ag_graph_get_tasks", C.c_int32, [C.c_void_p, C.c_int, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("ag_graph_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
     ("ag_autotune", C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(TileConfig), f64p]),
@@ -544,6 +545,14 @@ class DeviceGraph:
         check(lib.ag_ppr_spmm(self.h, src.ctypes.data_as(u32p), k, iterations, epsilon,
                               out.ctypes.data_as(f32p) if want_ranks else None, C.byref(res)), "ag_ppr_spmm")
         return out, res
+
+    def gather_u64(self, x) -> np.ndarray:
+        """ag_gather_u64: integer row sums of x modulo 2^64 (caller order)."""
+        x = np.ascontiguousarray(x, np.uint64)
+        y = np.zeros(self.num_vertices, np.uint64)
+        u64p = C.POINTER(C.c_uint64)
+        check(lib.ag_gather_u64(self.h, x.ctypes.data_as(u64p), y.ctypes.data_as(u64p)), "ag_gather_u64")
+        return y
 
     def spmv(self, x, mode=AG_SPMV_GRAPH_WEIGHTS) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float32)

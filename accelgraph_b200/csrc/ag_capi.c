@@ -103,8 +103,9 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
         printf(" -----------------------------------------------------\n");
         printf("| %-51s | \n", "               ---->>> B200 <<<----");
         printf(" -----------------------------------------------------\n");
-        printf("| %-51s | \n", o.data_driven ? "Starting Page Rank Pull DD (tolerance/epsilon)"
-                                               : "Starting Page Rank Pull (tolerance/epsilon)");
+        printf("| %-51s | \n", o.data_driven                     ? "Starting Page Rank Pull DD (tolerance/epsilon)"
+                                : o.precision == AG_PREC_FIXED64 ? "Starting Page Rank Pull FP_64 (tolerance/epsilon)"
+                                                                 : "Starting Page Rank Pull (tolerance/epsilon)");
         printf(" -----------------------------------------------------\n");
         printf("| %-51.13lf | \n", arguments->epsilon);
         printf(" -----------------------------------------------------\n");
@@ -176,19 +177,23 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
 }
 
 /* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 is the pull,
- * 6 the data-driven pull; the other codes (push, fixed-point and quantised
- * variants) run the FP32 pull, with a note on stderr */
+ * 2 the 64-bit fixed-point pull, 6 the data-driven pull; the other codes
+ * (push, narrower fixed-point and quantised variants) run the FP32 pull, with
+ * a note on stderr */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
 {
-    if (arguments && arguments->pushpull == 6) {
+    if (arguments && (arguments->pushpull == 6 || arguments->pushpull == 2)) {
         struct PageRankStats *stats = NULL;
         ag_pr_opts o;
         ag_status_t st;
         ag_pr_opts_init(&o);
-        o.data_driven = 1;
+        if (arguments->pushpull == 6)
+            o.data_driven = 1;
+        else
+            o.precision = AG_PREC_FIXED64;
         st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
         if (st != AG_OK)
-            fail_exit("pagerank-pull-dd", st);
+            fail_exit(arguments->pushpull == 6 ? "pagerank-pull-dd" : "pagerank-pull-fp64", st);
         return stats;
     }
     if (arguments && arguments->pushpull != 0)

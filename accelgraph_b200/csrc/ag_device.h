@@ -170,6 +170,12 @@ typedef struct AgPullParams
     uint32_t *g_passes;    /* per graph: passes run                            */
     uint32_t *g_conv;      /* per graph: 1 if a pass had no active vertex      */
     double *g_err_last;    /* per graph: error total of its last pass          */
+    /* 64-bit fixed-point pull (ag_fixed.cu): contribution ping-pong, hub
+     * partials, and the vectors of its plain gather */
+    uint64_t *c64_0, *c64_1;
+    uint64_t *hub_part64;
+    const uint64_t *x64;
+    uint64_t *y64;
     cudaGraphConditionalHandle cond;
 } AgPullParams;
 
@@ -239,6 +245,15 @@ int32_t ag_rt_graph_view(struct ag_graph_s *g, AgGraphView *v);
 const void *ag_pull_kernel_ptr(int mode, int prec, int exact);
 const void *ag_init_kernel_ptr(int prec);
 const void *ag_normalize_kernel_ptr(void);
+/* fixed-point pull (gather = 1: only the integer sums) and its init kernel */
+const void *ag_fixed_kernel_ptr(int gather);
+const void *ag_fixed_init_kernel_ptr(void);
+size_t ag_fixed_smem_bytes(void);
+/* 64-bit vectors into device order (out = 0: y[i] = x[map[i]], map = perm) or
+ * back to caller order (out = 1: y[v] = x[map[v]], map = inv); map NULL is the
+ * identity */
+cudaError_t ag_permute_u64(const uint32_t *map, const uint64_t *x, uint64_t *y, uint32_t n, int out,
+                           cudaStream_t s);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
 cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
                                      const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,

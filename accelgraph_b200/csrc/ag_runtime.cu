@@ -328,6 +328,13 @@ struct ag_graph_s
     int have_exe[3][2];
     /* data-driven mode: its launch graphs (FAST, EXACT) */
     AgExec exe_dd[2];
+    /* 64-bit fixed-point pull: contribution ping-pong, hub partials (capacity
+     * in chunks), and its launch graph (both orders give the same bits) */
+    uint64_t *c64[2];
+    uint64_t *hub_part64;
+    uint32_t hub64_cap;
+    AgExec exe_fx;
+    int have_exe_fx;
     int have_exe_dd[2];
     cudaEvent_t ev0, ev1;
     int launched;
@@ -382,6 +389,10 @@ static void drop_execs(ag_graph_s *g)
             free_exec(&g->exe_dd[b]);
             g->have_exe_dd[b] = 0;
         }
+    if (g->have_exe_fx) {
+        free_exec(&g->exe_fx);
+        g->have_exe_fx = 0;
+    }
 }
 
 extern "C" ag_status_t ag_graph_release(ag_graph_t g)
@@ -391,6 +402,9 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     if (g_ctx.ready)
         stream_wait(g_ctx.stream, 0);
     drop_execs(g);
+    dev_free(g->c64[0]);
+    dev_free(g->c64[1]);
+    dev_free(g->hub_part64);
     dev_free(g->row_off);
     dev_free(g->ids);
     dev_free(g->perm);
@@ -893,6 +907,9 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
         p.g_err = g->g_f64;
         p.g_err_last = g->g_f64 + g->ngraphs;
     }
+    p.c64_0 = g->c64[0];
+    p.c64_1 = g->c64[1];
+    p.hub_part64 = g->hub_part64;
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
@@ -903,23 +920,24 @@ static int pull_mode(const ag_graph_s *g, int dd)
     return dd ? AG_MODE_DD : (g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR);
 }
 
-static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
+static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, int fx = 0)
 {
-    AgExec *x = dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
+    AgExec *x = fx ? &g->exe_fx : dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
     memset(x, 0, sizeof(*x));
     AG_CUDA(cudaGraphCreate(&x->graph, 0));
     AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
     x->params.use_cond = 1;
-    const void *kpull = ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
-    x->grid = pull_grid(kpull, x->params.ntasks, pull_smem(g));
+    const void *kpull = fx ? ag_fixed_kernel_ptr(0) : ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
+    const size_t smem = fx ? ag_fixed_smem_bytes() : pull_smem(g);
+    x->grid = pull_grid(kpull, x->params.ntasks, smem);
 
     AgRunConfig run;
     memset(&run, 0, sizeof(run));
     void *init_args[2] = {&x->params, &run};
     cudaKernelNodeParams kp = {};
-    kp.func = (void *)ag_init_kernel_ptr(prec);
+    kp.func = (void *)(fx ? ag_fixed_init_kernel_ptr() : ag_init_kernel_ptr(prec));
     kp.gridDim = dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK,
                                                                           (uint64_t)g_ctx.num_sms * 8)));
     kp.blockDim = dim3(AG_SBLK);
@@ -940,7 +958,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
     kb.func = (void *)kpull;
     kb.gridDim = dim3(x->grid);
     kb.blockDim = dim3(AG_BLK);
-    kb.sharedMemBytes = (unsigned)pull_smem(g);
+    kb.sharedMemBytes = (unsigned)smem;
     kb.kernelParams = pull_args;
     cudaGraphNode_t pnode;
     AG_CUDA(cudaGraphAddKernelNode(&pnode, body, nullptr, 0, &kb));
@@ -955,10 +973,38 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
     AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
 
     AG_CUDA(cudaGraphInstantiate(&x->exec, x->graph, 0));
-    if (dd)
+    if (fx)
+        g->have_exe_fx = 1;
+    else if (dd)
         g->have_exe_dd[exact] = 1;
     else
         g->have_exe[prec][exact] = 1;
+    return AG_OK;
+}
+
+/* fixed-point pull buffers, made on first use; the hub partials follow the
+ * work list's chunk count (a new tile shape may need more) */
+static ag_status_t ensure_fixed(ag_graph_s *g)
+{
+    ag_status_t st = AG_OK;
+    if (!g->c64[0]) {
+        g->c64[0] = (uint64_t *)dev_alloc(g, (size_t)g->N * 8 + 16, &st);
+        g->c64[1] = (uint64_t *)dev_alloc(g, (size_t)g->N * 8 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        drop_execs(g);
+    }
+    if (!g->hub_part64 || g->hub64_cap < g->nparts) {
+        dev_free(g->hub_part64);
+        g->hub_part64 = (uint64_t *)dev_alloc(g, (size_t)g->nparts * 8 + 16, &st);
+        if (st != AG_OK) {
+            g->hub_part64 = nullptr;
+            g->hub64_cap = 0;
+            return st;
+        }
+        g->hub64_cap = g->nparts;
+        drop_execs(g);
+    }
     return AG_OK;
 }
 
@@ -983,15 +1029,18 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
     ag_pr_opts_init(&o);
     if (opts)
         memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
-    if (o.precision < 0 || o.precision > 2)
+    if (o.precision < 0 || o.precision > AG_PREC_FIXED64)
         return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
     if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks || o.data_driven))
         return ag_set_error(AG_ERR_UNSUPPORTED, "a graph union runs the FP32 form without a warm start");
     const int dd = o.data_driven ? 1 : 0;
     if (dd && (o.precision != AG_PREC_FP32 || g->norm_n || g->c_base))
         return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven pull runs in FP32 on a whole graph");
-    const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
-    ag_status_t st = ensure_buffers(g, prec);
+    const int fx = o.precision == AG_PREC_FIXED64 ? 1 : 0;
+    if (fx && (g->norm_n || g->c_base))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the fixed-point pull runs on a whole graph");
+    const int prec = fx ? 0 : o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
+    ag_status_t st = fx ? ensure_fixed(g) : ensure_buffers(g, prec);
     if (st != AG_OK)
         return st;
     if (o.init_ranks && !g->init_buf) {
@@ -1001,12 +1050,12 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         /* rebuild cached graphs: their parameters carry the warm-start pointer */
         drop_execs(g);
     }
-    if (dd ? !g->have_exe_dd[exact] : !g->have_exe[prec][exact]) {
-        st = build_exec(g, prec, exact, dd);
+    if (fx ? !g->have_exe_fx : dd ? !g->have_exe_dd[exact] : !g->have_exe[prec][exact]) {
+        st = build_exec(g, prec, exact, dd, fx);
         if (st != AG_OK)
             return st;
     }
-    AgExec *x = dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
+    AgExec *x = fx ? &g->exe_fx : dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
     cudaStream_t s = g_ctx.stream;
     if (o.init_ranks && g->N)
         AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4,
@@ -1034,9 +1083,10 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         void *ia[2] = {&sp, &run};
         AG_CUDA(cudaLaunchKernel(ki.func, ki.gridDim, ki.blockDim, ia, 0, s));
         void *pa[1] = {&sp};
-        const void *kpull = ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
+        const void *kpull = fx ? ag_fixed_kernel_ptr(0) : ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
+        const size_t smem = fx ? ag_fixed_smem_bytes() : pull_smem(g);
         for (uint32_t i = 0; i < run.max_iter; ++i)
-            AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, pull_smem(g), s));
+            AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, smem, s));
         AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
     } else {
         AG_CUDA(cudaGraphLaunch(x->exec, s));
@@ -1832,5 +1882,51 @@ extern "C" ag_status_t ag_graph_build(uint32_t num_vertices, uint64_t num_edges,
     st = upload_impl(nullptr, upload_flags, nullptr, 0, 0, out, &c);
     ag_csr_free_device(&c, g_ctx.stream);
     ag_status_t w = stream_wait(g_ctx.stream, 0);
+    return st != AG_OK ? st : w;
+}
+
+/* ------------------------------------------------ fixed-point gather */
+extern "C" ag_status_t ag_gather_u64(ag_graph_t g, const uint64_t *x, uint64_t *y)
+{
+    ag_clear_error();
+    if (!g || (g->N && (!x || !y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_gather_u64: NULL argument");
+    if (g->norm_n || g->c_base)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_gather_u64: a row partition indexes a vector it does not hold");
+    if (g->N == 0)
+        return AG_OK;
+    ag_status_t st = ensure_fixed(g);
+    if (st != AG_OK)
+        return st;
+    cudaStream_t s = g_ctx.stream;
+    const size_t bytes = (size_t)g->N * 8;
+    uint64_t *buf = nullptr;
+    AG_CUDA(cudaMallocAsync((void **)&buf, 2 * bytes + 16, s));
+    uint64_t *xa = buf, *xb = buf + g->N;
+    cudaError_t e = cudaMemcpyAsync(xa, x, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = ag_permute_u64(g->perm, xa, xb, g->N, 0, s);
+    if (e == cudaSuccess) {
+        AgPullParams p = base_params(g, 0);
+        p.x64 = xb;
+        p.y64 = xa; /* the caller-order copy of x is no longer needed */
+        const void *k = ag_fixed_kernel_ptr(1);
+        const unsigned grid = pull_grid(k, p.ntasks, ag_fixed_smem_bytes());
+        void *args[1] = {&p};
+        if (p.ntasks)
+            e = cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, ag_fixed_smem_bytes(), s);
+        else
+            e = cudaMemsetAsync(xa, 0, bytes, s);
+    }
+    if (e == cudaSuccess)
+        e = ag_permute_u64(g->inv, xa, xb, g->N, 1, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        st = ag_set_error(AG_ERR_CUDA, "ag_gather_u64: %s", cudaGetErrorString(e));
+    }
+    if (st == AG_OK)
+        st = copy_to_host(y, xb, bytes);
+    cudaFreeAsync(buf, s);
+    ag_status_t w = stream_wait(s, 0);
     return st != AG_OK ? st : w;
 }

@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--workload", default="pagerank",
                    choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe",
-                            "data-driven"],
+                            "data-driven", "fixed-point"],
                    help="pagerank: the headline line (driver contract); the others measure the other forms")
     p.add_argument("--graphs", type=int, default=256, help="multigraph: number of graphs")
     p.add_argument("--train-graphs", type=int, default=200, help="warmstart: training graphs")
@@ -548,6 +548,43 @@ def run_data_driven(a):
     print(json.dumps(out), flush=True)
 
 
+def run_fixed_point(a):
+    """64-bit fixed-point pull (the reference's pushpull 2) against the FP32
+    pull on the same graph: time to epsilon on the device, passes, accuracy
+    against the FP64 fixpoint, and the CPU oracle of the fixed-point pull."""
+    import time
+    import oracle
+    ag = _gpu_setup()
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g)
+    r64, _ = dg.pagerank_f64(5000, 1e-13)
+    peak, kind = peak_hbm()
+    out = {"workload": f"fixed-point PageRank pull to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}",
+           "N": N, "E": E}
+    for name, prec, cbytes in (("fp32", ag.AG_PREC_FP32, 4), ("fixed64", ag.AG_PREC_FIXED64, 8)):
+        dg.pagerank(a.iterations, a.epsilon, precision=prec)
+        best = None
+        for _ in range(max(1, a.steps)):
+            r, res, _ = dg.pagerank(a.iterations, a.epsilon, precision=prec)
+            if best is None or res.device_ms < best[1].device_ms:
+                best = (r, res)
+        r, res = best
+        rl, mx = _rel(r, r64)
+        alg = 4 * E + (16 + 2 * cbytes) * N + 4 * N
+        pass_s = res.device_ms * 1e-3 / max(res.passes, 1)
+        out[name] = {"device_ms_to_eps": res.device_ms, "passes": res.passes, "iterations": res.iterations,
+                     "pass_us": pass_s * 1e6, "roofline_frac": alg / pass_s / 1e9 / peak,
+                     "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx}
+    out["fixed64_vs_fp32_time"] = out["fp32"]["device_ms_to_eps"] / out["fixed64"]["device_ms_to_eps"]
+    t0 = time.perf_counter()
+    ref = oracle.pagerank_fixed64(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(),
+                                  a.iterations, a.epsilon)
+    out["cpu_oracle"] = {"seconds_to_eps": time.perf_counter() - t0, "iterations": ref["iterations"],
+                         "threads": oracle.lib.oracle_max_threads()}
+    print(json.dumps(out), flush=True)
+
+
 def run_rows(a):
     """One graph split by rows over all ranks (NCCL all-gather per pass);
     strong scaling: the whole job solves one graph."""
@@ -612,7 +649,7 @@ def main():
     else:
         {"spmv": run_spmv, "precision": run_precision, "ppr": run_ppr, "multigraph": run_multigraph,
          "warmstart": run_warmstart, "gather-probe": run_gather_probe,
-         "data-driven": run_data_driven}[a.workload](a)
+         "data-driven": run_data_driven, "fixed-point": run_fixed_point}[a.workload](a)
 
 
 if __name__ == "__main__":

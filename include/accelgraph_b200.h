@@ -205,6 +205,12 @@ ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, dou
 #define AG_PREC_FP32 0   /* contributions stored in binary32 (reference)     */
 #define AG_PREC_BF16 1   /* contributions stored in bfloat16, FP32 accumulate */
 #define AG_PREC_FP16 2   /* contributions stored in binary16, FP32 accumulate */
+#define AG_PREC_FIXED64 3 /* the reference's 64-bit fixed-point pull (pushpull
+                             2, pageRank.c:1276-1453): contributions converted
+                             to fixed point with 32 fractional bits
+                             (truncating), rows summed as integers modulo
+                             2^64, the update formed in binary64; both orders
+                             give the same bits */
 
 #define AG_ORDER_FAST  0 /* rows of <= 32 in-edges summed in stream order,
                             longer rows by a fixed lane-strided tree         */
@@ -247,6 +253,13 @@ typedef struct ag_pr_result
 } ag_pr_result;
 
 void ag_pr_opts_init(ag_pr_opts *opts);
+
+/* Fixed-point gather on a device graph: y[v] = sum of x[u] over v's in-edges,
+ * as 64-bit integers modulo 2^64 (0 for a vertex without in-edges), x and y in
+ * caller vertex order, host memory.  The arithmetic of the reference's
+ * FixedPoint compute unit (cu_PageRank/CSR/PULL/FixedPoint; testbench contract
+ * pagerank_kernel_tb.sv:13-16). */
+ag_status_t ag_gather_u64(struct ag_graph_s *g, const uint64_t *x, uint64_t *y);
 
 /* Status-returning form of pageRankPullGraphCSR with the precision, order and
  * warm-start options.  *out receives a stats object owned by the caller. */
