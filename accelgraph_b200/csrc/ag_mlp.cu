@@ -64,49 +64,87 @@ struct ag_mlp_s
 };
 
 /* ---------------------------------------------------------- features */
-__global__ void ag_features_kernel(AgGraphView gv, float *X)
+/* (in-degree, out-degree) of every vertex, device order: one 8-byte gather
+ * per in-edge instead of three */
+__global__ void ag_deg2_kernel(AgGraphView gv, uint2 *deg2)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < gv.N; v += gridDim.x * blockDim.x)
+        deg2[v] = make_uint2(gv.row_off[v + 1] - gv.row_off[v], gv.outdeg[v]);
+}
+
+/* the eight features of a vertex, written in caller order */
+__device__ __forceinline__ void ag_features_store(const AgGraphView &gv, float *X, uint32_t v, uint32_t deg,
+                                                  float s_in, float s_out, float s_c, float mn_out, float mx_out,
+                                                  float mx_in)
+{
+    const uint32_t dst = gv.perm ? gv.perm[v] : v;
+    float *x = X + (size_t)dst * AG_MLP_IN;
+    x[0] = log1pf((float)deg);
+    x[1] = log1pf((float)gv.outdeg[v]);
+    x[2] = log1pf(s_in);
+    x[3] = log1pf(s_out);
+    x[4] = log1pf(deg ? mn_out : 0.0f);
+    x[5] = log1pf(mx_out);
+    x[6] = log1pf(s_c);
+    x[7] = log1pf(mx_in);
+}
+
+/* Vertices of at most 32 in-edges, one per lane.  Degree sums are sums of
+ * integers below 2^24, exact in any order. */
+__global__ void ag_features_kernel(AgGraphView gv, const uint2 *deg2, float *X)
+{
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < gv.N; v += gridDim.x * blockDim.x) {
+        const uint32_t b = gv.row_off[v], e = gv.row_off[v + 1];
+        if (e - b > 32)
+            continue;
+        float s_in = 0.f, s_out = 0.f, s_c = 0.f, mx_in = 0.f, mx_out = 0.f, mn_out = 3.0e38f;
+        for (uint32_t j = b; j < e; ++j) {
+            const uint2 d = __ldg(deg2 + __ldg(gv.ids + j));
+            const float din = (float)d.x, dout = (float)d.y;
+            s_in += din;
+            s_out += dout;
+            s_c += d.y ? 1.0f / dout : 0.0f;
+            mx_in = fmaxf(mx_in, din);
+            mx_out = fmaxf(mx_out, dout);
+            mn_out = fminf(mn_out, dout);
+        }
+        ag_features_store(gv, X, v, e - b, s_in, s_out, s_c, mn_out, mx_out, mx_in);
+    }
+}
+
+/* Vertices of more than 32 in-edges, one warp each (lane-strided partials,
+ * xor tree), so that the long rows, which the relabelling puts side by side,
+ * spread over all warps. */
+__global__ void ag_features_long_kernel(AgGraphView gv, const uint2 *deg2, float *X)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < gv.N; v += nw) {
         const uint32_t b = gv.row_off[v], e = gv.row_off[v + 1];
-        float s_in = 0.f, s_out = 0.f, s_c = 0.f, mx_in = 0.f, mx_out = 0.f, mn_out = 3.0e38f;
+        if (e - b <= 32)
+            continue;
+        float a_in = 0.f, a_out = 0.f, a_c = 0.f, x_in = 0.f, x_out = 0.f, n_out = 3.0e38f;
         for (uint32_t j = b + lane; j < e; j += 32) {
-            const uint32_t u = gv.ids[j];
-            const float din = (float)(gv.row_off[u + 1] - gv.row_off[u]);
-            const uint32_t od = gv.outdeg[u];
-            const float dout = (float)od;
-            s_in += din;
-            s_out += dout;
-            s_c += od ? 1.0f / dout : 0.0f;
-            mx_in = fmaxf(mx_in, din);
-            mx_out = fmaxf(mx_out, dout);
-            mn_out = fminf(mn_out, dout);
+            const uint2 d = __ldg(deg2 + __ldg(gv.ids + j));
+            const float din = (float)d.x, dout = (float)d.y;
+            a_in += din;
+            a_out += dout;
+            a_c += d.y ? 1.0f / dout : 0.0f;
+            x_in = fmaxf(x_in, din);
+            x_out = fmaxf(x_out, dout);
+            n_out = fminf(n_out, dout);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            s_in += __shfl_xor_sync(0xffffffffu, s_in, o);
-            s_out += __shfl_xor_sync(0xffffffffu, s_out, o);
-            s_c += __shfl_xor_sync(0xffffffffu, s_c, o);
-            mx_in = fmaxf(mx_in, __shfl_xor_sync(0xffffffffu, mx_in, o));
-            mx_out = fmaxf(mx_out, __shfl_xor_sync(0xffffffffu, mx_out, o));
-            mn_out = fminf(mn_out, __shfl_xor_sync(0xffffffffu, mn_out, o));
+            a_in += __shfl_xor_sync(0xffffffffu, a_in, o);
+            a_out += __shfl_xor_sync(0xffffffffu, a_out, o);
+            a_c += __shfl_xor_sync(0xffffffffu, a_c, o);
+            x_in = fmaxf(x_in, __shfl_xor_sync(0xffffffffu, x_in, o));
+            x_out = fmaxf(x_out, __shfl_xor_sync(0xffffffffu, x_out, o));
+            n_out = fminf(n_out, __shfl_xor_sync(0xffffffffu, n_out, o));
         }
-        if (lane < AG_MLP_IN) {
-            float f;
-            switch (lane) {
-            case 0: f = (float)(e - b); break;
-            case 1: f = (float)gv.outdeg[v]; break;
-            case 2: f = s_in; break;
-            case 3: f = s_out; break;
-            case 4: f = (e > b) ? mn_out : 0.0f; break;
-            case 5: f = mx_out; break;
-            case 6: f = s_c; break;
-            default: f = mx_in; break;
-            }
-            const uint32_t dst = gv.perm ? gv.perm[v] : v;
-            X[(size_t)dst * AG_MLP_IN + lane] = log1pf(f);
-        }
+        if (lane == 0)
+            ag_features_store(gv, X, v, e - b, a_in, a_out, a_c, n_out, x_out, x_in);
     }
 }
 
@@ -423,11 +461,17 @@ extern "C" ag_status_t ag_features(ag_graph_t g, float *features)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_features: NULL output");
     if (gv.N == 0)
         return AG_OK;
-    uint64_t blocks = ((uint64_t)gv.N * 32 + 255) / 256;
+    uint2 *deg2 = nullptr;
+    MCHK(cudaMallocAsync((void **)&deg2, (size_t)gv.N * sizeof(uint2), gv.stream));
+    uint64_t blocks = ((uint64_t)gv.N + 255) / 256;
     if (blocks > 148 * 16)
         blocks = 148 * 16;
-    ag_features_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, features);
-    MCHK(cudaGetLastError());
+    ag_deg2_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2);
+    ag_features_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2, features);
+    ag_features_long_kernel<<<148 * 16, 256, 0, gv.stream>>>(gv, deg2, features);
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(deg2, gv.stream);
+    MCHK(e);
     return AG_OK;
 }
 
