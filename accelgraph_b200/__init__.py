@@ -132,6 +132,14 @@ AG_FILE_TEXT, AG_FILE_BINARY, AG_FILE_CSR = 0, 1, 2
 AG_UPLOAD_WEIGHTS, AG_UPLOAD_VALIDATE, AG_UPLOAD_TRUSTED = 1, 2, 4
 AG_UPLOAD_KEEP_ORDER, AG_UPLOAD_NO_SMEM_CACHE = 8, 16
 AG_PREC_FP32, AG_PREC_BF16, AG_PREC_FP16, AG_PREC_FIXED64 = 0, 1, 2, 3
+AG_PREC_FIXED32, AG_PREC_FIXED16, AG_PREC_FIXED8 = 4, 5, 6
+AG_PREC_QUANT32, AG_PREC_QUANT16, AG_PREC_QUANT8 = 7, 8, 9
+# pageRankGraphCSR's pushpull code of each integer pull (pageRank.c:874-939)
+PUSHPULL_OF_PREC = {AG_PREC_FIXED64: 2, AG_PREC_FIXED32: 9, AG_PREC_FIXED16: 10, AG_PREC_FIXED8: 11,
+                    AG_PREC_QUANT32: 4, AG_PREC_QUANT16: 12, AG_PREC_QUANT8: 13}
+# (quantised, width in bits) of each narrow integer pull
+NARROW_FORM = {AG_PREC_FIXED32: (False, 32), AG_PREC_FIXED16: (False, 16), AG_PREC_FIXED8: (False, 8),
+               AG_PREC_QUANT32: (True, 32), AG_PREC_QUANT16: (True, 16), AG_PREC_QUANT8: (True, 8)}
 AG_ORDER_FAST, AG_ORDER_EXACT = 0, 1
 AG_SPMV_GRAPH_WEIGHTS, AG_SPMV_UNIT, AG_SPMV_EXACT = 0, 1, 2
 DAMP = np.float32(0.85)
@@ -176,6 +184,7 @@ SIGNATURES = [
     ("ag_graph_get_info", C.c_int32, [C.c_void_p, C.POINTER(GraphInfo)]),
     ("ag_graph_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
     ("ag_gather_u64", C.c_int32, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("ag_gather_uint", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)]),
     ("ag_graph_get_tasks", C.c_int32, [C.c_void_p, C.c_int, u32p, C.c_uint32, C.POINTER(C.c_uint32)]),
     ("ag_graph_set_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
     ("ag_autotune", C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(TileConfig), f64p]),
@@ -552,6 +561,17 @@ class DeviceGraph:
         y = np.zeros(self.num_vertices, np.uint64)
         u64p = C.POINTER(C.c_uint64)
         check(lib.ag_gather_u64(self.h, x.ctypes.data_as(u64p), y.ctypes.data_as(u64p)), "ag_gather_u64")
+        return y
+
+    def gather_uint(self, x) -> np.ndarray:
+        """ag_gather_uint: row sums of x (uint8, uint16, uint32 or uint64),
+        each element zero-extended, modulo 2^64 (caller order)."""
+        x = np.ascontiguousarray(x)
+        if x.dtype not in (np.uint8, np.uint16, np.uint32, np.uint64):
+            raise TypeError("gather_uint: x must be uint8, uint16, uint32 or uint64")
+        y = np.zeros(self.num_vertices, np.uint64)
+        check(lib.ag_gather_uint(self.h, x.ctypes.data_as(C.c_void_p), x.dtype.itemsize,
+                                 y.ctypes.data_as(C.POINTER(C.c_uint64))), "ag_gather_uint")
         return y
 
     def spmv(self, x, mode=AG_SPMV_GRAPH_WEIGHTS) -> np.ndarray:

@@ -103,9 +103,20 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
         printf(" -----------------------------------------------------\n");
         printf("| %-51s | \n", "               ---->>> B200 <<<----");
         printf(" -----------------------------------------------------\n");
-        printf("| %-51s | \n", o.data_driven                     ? "Starting Page Rank Pull DD (tolerance/epsilon)"
-                                : o.precision == AG_PREC_FIXED64 ? "Starting Page Rank Pull FP_64 (tolerance/epsilon)"
-                                                                 : "Starting Page Rank Pull (tolerance/epsilon)");
+        if (o.precision >= AG_PREC_QUANT32 && o.precision <= AG_PREC_QUANT8)
+            /* the quantised forms' title layout (pageRank.c:2155) */
+            printf("| %-30s %-19s| \n",
+                   o.precision == AG_PREC_QUANT32   ? "Starting Page Rank Pull Quant_32"
+                   : o.precision == AG_PREC_QUANT16 ? "Starting Page Rank Pull Quant_16"
+                                                    : "Starting Page Rank Pull Quant_8",
+                   "(tolerance/epsilon)");
+        else
+            printf("| %-51s | \n", o.data_driven                     ? "Starting Page Rank Pull DD (tolerance/epsilon)"
+                                    : o.precision == AG_PREC_FIXED64 ? "Starting Page Rank Pull FP_64 (tolerance/epsilon)"
+                                    : o.precision == AG_PREC_FIXED32 ? "Starting Page Rank Pull FP_32 (tolerance/epsilon)"
+                                    : o.precision == AG_PREC_FIXED16 ? "Starting Page Rank Pull FP_16 (tolerance/epsilon)"
+                                    : o.precision == AG_PREC_FIXED8  ? "Starting Page Rank Pull FP_8 (tolerance/epsilon)"
+                                                                     : "Starting Page Rank Pull (tolerance/epsilon)");
         printf(" -----------------------------------------------------\n");
         printf("| %-51.13lf | \n", arguments->epsilon);
         printf(" -----------------------------------------------------\n");
@@ -177,23 +188,36 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
 }
 
 /* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 is the pull,
- * 2 the 64-bit fixed-point pull, 6 the data-driven pull; the other codes
- * (push, narrower fixed-point and quantised variants) run the FP32 pull, with
- * a note on stderr */
+ * 2, 9, 10, 11 the 64/32/16/8-bit fixed-point pulls, 4, 12, 13 the 32/16/8-bit
+ * quantised pulls, 6 the data-driven pull; the other codes (the push
+ * variants) run the FP32 pull, with a note on stderr */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
 {
-    if (arguments && (arguments->pushpull == 6 || arguments->pushpull == 2)) {
+    /* pull variants on the GPU: pushpull code, precision form, phase name of
+     * the failure line */
+    static const struct
+    {
+        uint32_t pushpull;
+        int32_t precision;
+        const char *phase;
+    } forms[] = {
+        {2, AG_PREC_FIXED64, "pagerank-pull-fp64"},  {9, AG_PREC_FIXED32, "pagerank-pull-fp32"},
+        {10, AG_PREC_FIXED16, "pagerank-pull-fp16"}, {11, AG_PREC_FIXED8, "pagerank-pull-fp8"},
+        {4, AG_PREC_QUANT32, "pagerank-pull-quant32"}, {12, AG_PREC_QUANT16, "pagerank-pull-quant16"},
+        {13, AG_PREC_QUANT8, "pagerank-pull-quant8"},  {6, AG_PREC_FP32, "pagerank-pull-dd"},
+    };
+    for (size_t i = 0; arguments && i < sizeof(forms) / sizeof(forms[0]); ++i) {
+        if (arguments->pushpull != forms[i].pushpull)
+            continue;
         struct PageRankStats *stats = NULL;
         ag_pr_opts o;
         ag_status_t st;
         ag_pr_opts_init(&o);
-        if (arguments->pushpull == 6)
-            o.data_driven = 1;
-        else
-            o.precision = AG_PREC_FIXED64;
+        o.precision = forms[i].precision;
+        o.data_driven = arguments->pushpull == 6;
         st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
         if (st != AG_OK)
-            fail_exit(arguments->pushpull == 6 ? "pagerank-pull-dd" : "pagerank-pull-fp64", st);
+            fail_exit(forms[i].phase, st);
         return stats;
     }
     if (arguments && arguments->pushpull != 0)

@@ -170,10 +170,15 @@ typedef struct AgPullParams
     uint32_t *g_passes;    /* per graph: passes run                            */
     uint32_t *g_conv;      /* per graph: 1 if a pass had no active vertex      */
     double *g_err_last;    /* per graph: error total of its last pass          */
-    /* 64-bit fixed-point pull (ag_fixed.cu): contribution ping-pong, hub
-     * partials, and the vectors of its plain gather */
+    /* integer pulls (ag_fixed.cu): contribution buffers (64-bit, or W-bit
+     * in their first N * W/8 bytes), hub partials, the quantised forms'
+     * binary32 contributions and min/max key slots (mm[0..1] minimum keys,
+     * mm[2..3] maximum keys, one of each per pass parity), and the vectors of
+     * the plain gather (x of any width, y 64-bit) */
     uint64_t *c64_0, *c64_1;
     uint64_t *hub_part64;
+    float *cqf;
+    uint32_t *qmm;
     const uint64_t *x64;
     uint64_t *y64;
     cudaGraphConditionalHandle cond;
@@ -245,15 +250,19 @@ int32_t ag_rt_graph_view(struct ag_graph_s *g, AgGraphView *v);
 const void *ag_pull_kernel_ptr(int mode, int prec, int exact);
 const void *ag_init_kernel_ptr(int prec);
 const void *ag_normalize_kernel_ptr(void);
-/* fixed-point pull (gather = 1: only the integer sums) and its init kernel */
-const void *ag_fixed_kernel_ptr(int gather);
-const void *ag_fixed_init_kernel_ptr(void);
+/* integer pulls: contributions of `bytes` (8, 4, 2, 1) bytes, fixed point or
+ * quantised; gather = 1: only the integer sums.  Their init kernel, the
+ * quantised forms' element-wise quantiser, and the dynamic shared memory of
+ * the pull kernels */
+const void *ag_int_kernel_ptr(int bytes, int quant, int gather);
+const void *ag_int_init_kernel_ptr(int bytes, int quant);
+const void *ag_quant_kernel_ptr(int bytes);
 size_t ag_fixed_smem_bytes(void);
-/* 64-bit vectors into device order (out = 0: y[i] = x[map[i]], map = perm) or
- * back to caller order (out = 1: y[v] = x[map[v]], map = inv); map NULL is the
+/* vectors of `bytes`-byte elements into device order (y[i] = x[perm[i]]) and
+ * 64-bit sums back to caller order (y[v] = x[inv[v]]); a NULL map is the
  * identity */
-cudaError_t ag_permute_u64(const uint32_t *map, const uint64_t *x, uint64_t *y, uint32_t n, int out,
-                           cudaStream_t s);
+cudaError_t ag_permute_uint_in(const uint32_t *perm, const void *x, void *y, uint32_t n, int bytes, cudaStream_t s);
+cudaError_t ag_permute_u64_out(const uint32_t *inv, const uint64_t *x, uint64_t *y, uint32_t n, cudaStream_t s);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
 cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
                                      const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,

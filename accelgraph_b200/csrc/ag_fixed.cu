@@ -1,35 +1,53 @@
 /*
- * ag_fixed.cu -- 64-bit fixed-point pull (the reference's pushpull 2,
- * 02_capi_graph/src/algorithms/capi/pageRank.c:1276-1453).
+ * ag_fixed.cu -- integer pulls: the reference's fixed-point and quantised
+ * PageRank forms (02_capi_graph/src/algorithms/capi/pageRank.c):
+ *   pushpull 2        64-bit fixed point          :1276-1453
+ *   pushpull 9/10/11  32/16/8-bit fixed point     :1455-1991
+ *   pushpull 4/12/13  32/16/8-bit quantised       :2119-2677
  *
- * Per pass the reference converts every contribution r[v] / out_degree[v]
- * (binary32 division) to 64-bit fixed point, the accelerator sums each row's
- * contributions as integers modulo 2^64 (its FixedPoint contract,
- * pagerank_kernel_tb.sv:13-16), and the host forms
- * r' = base + damp * to_double(sum) in binary64, stored in binary32.  The
- * conversions are OpenGraph's (absent from the reference checkout); they are
- * restated as 32 fractional bits, the conversion to fixed point truncating
- * toward zero.
+ * Per pass the reference turns every contribution r[v] / out_degree[v]
+ * (binary32 division) into a W-bit integer, the accelerator sums each row's
+ * integers zero-extended into 64 bits modulo 2^64 (its FixedPoint and
+ * Quantized contracts, pagerank_kernel_tb.sv:13-19), and the host forms the
+ * new rank from the sum:
+ *   64-bit fixed   r' = base + damp * to_double(sum) in binary64, stored in
+ *                  binary32; 32 fractional bits, conversion truncating
+ *   W-bit fixed    r' = base + damp * to_float(sum) in binary32; W/2
+ *                  fractional bits (Q16.16, Q8.8, Q4.4), conversion
+ *                  truncating, the sum rounded once to binary32
+ *   W-bit quant    r' = base + damp * (scale * (float)sum) in binary32, with
+ *                  scale = (max - min) / (2^W - 1) over the pass's float
+ *                  contributions, q = round-half-even(c / scale) clamped to
+ *                  [0, 2^W - 1], zero point 0 (pageRank.c:2225-2226)
+ * The conversions and the quantiser are OpenGraph's (absent from the
+ * reference checkout) and are restated as above.
  *
- * The first AG_FX_HOT values of the gathered vector (the most-gathered
- * after the upload's relabelling by out-degree) are copied into shared
- * memory at the start of each pass.
+ * The quantised forms need the minimum and maximum of all contributions
+ * before any of them is quantised: the pull kernel writes binary32
+ * contributions and folds their order-preserving keys into a min/max slot
+ * (one per pass parity); a separate element-wise kernel, the first node of
+ * the next loop iteration, quantises them with the scale of that slot.
+ *
+ * The first 64 KB of the gathered vector (the most-gathered ids after the
+ * upload's relabelling by out-degree: 8K 64-bit, 16K 32-bit, 32K 16-bit or
+ * 64K 8-bit values) are copied into shared memory at the start of each pass.
  *
  * Integer sums do not depend on their order, so one kernel serves both
  * orders and its results are the same bits whatever the work split: a row
  * item's values are staged in shared memory by the whole warp and each lane
  * sums its row, long rows are summed warp-strided, hub rows in chunks whose
- * partials the last chunk adds.  The
- * update, residual, stop test, per-pass record and the loop's WHILE
- * condition follow the FP32 pull kernel.  GATHER mode only sums: y[r] = the
- * row's sum of x (rows without in-edges give 0).
+ * partials the last chunk adds.  The update, residual, stop test, per-pass
+ * record and the loop's WHILE condition follow the FP32 pull kernel.  GATHER
+ * mode only sums: y[r] = the row's sum of x (rows without in-edges give 0).
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "ag_device.h"
 
-#define AG_FX_ONE 4294967296.0 /* 2^32: fixed-point unit */
+#define AG_FX_ONE 4294967296.0 /* 2^32: 64-bit fixed-point unit */
+#define AG_INT_FIXED 0
+#define AG_INT_QUANT 1
 
 __device__ __forceinline__ uint64_t ag_d2fixed(double x)
 {
@@ -39,6 +57,57 @@ __device__ __forceinline__ uint64_t ag_d2fixed(double x)
 __device__ __forceinline__ double ag_fixed2d(uint64_t x)
 {
     return __ddiv_rn(__ll2double_rn((long long)x), AG_FX_ONE);
+}
+
+/* W-bit fixed point, W/2 fractional bits: the exact binary32 product
+ * truncated toward zero, kept modulo 2^W; back: the 64-bit sum rounded once
+ * to binary32, scaled by 2^-(W/2) (exact) */
+template <typename T> __device__ __forceinline__ T ag_to_fixed(float x)
+{
+    constexpr float one = (float)(1u << (4 * sizeof(T)));
+    return (T)(unsigned long long)__float2ll_rz(__fmul_rn(x, one));
+}
+
+template <typename T> __device__ __forceinline__ float ag_from_fixed(uint64_t s)
+{
+    constexpr float one = (float)(1u << (4 * sizeof(T)));
+    return __fdiv_rn(__ull2float_rn(s), one);
+}
+
+/* order-preserving 32-bit keys of binary32 values (for atomic min/max) */
+__device__ __forceinline__ uint32_t ag_fkey(float f)
+{
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float ag_fkey_value(uint32_t k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+/* scale of the contributions whose min/max keys are in slot `slot`
+ * (mm[0..1] minimum keys, mm[2..3] maximum keys); 0 for an empty slot */
+template <typename T> __device__ __forceinline__ float ag_quant_scale(const uint32_t *mm, uint32_t slot)
+{
+    constexpr float levels = (float)((1ull << (8 * sizeof(T))) - 1ull);
+    const uint32_t kmin = mm[slot], kmax = mm[2 + slot];
+    if (kmin > kmax)
+        return 0.0f;
+    return __fdiv_rn(__fsub_rn(ag_fkey_value(kmax), ag_fkey_value(kmin)), levels);
+}
+
+template <typename T> __device__ __forceinline__ T ag_quantize(float x, float scale)
+{
+    constexpr unsigned long long top = (1ull << (8 * sizeof(T))) - 1ull;
+    if (!(scale > 0.0f))
+        return (T)0;
+    const float q = rintf(__fdiv_rn(x, scale));
+    if (!(q > 0.0f))
+        return (T)0;
+    if (q >= (float)top)
+        return (T)top;
+    return (T)(unsigned long long)q;
 }
 
 __device__ __forceinline__ uint64_t ag_warp_sum_u64(uint64_t v)
@@ -52,48 +121,81 @@ __device__ __forceinline__ uint64_t ag_warp_sum_u64(uint64_t v)
 /* one warp's stage: a row item's AG_WCAP in-edges start anywhere in their
  * first 16-byte quad, so they span up to AG_WCAP + 3 slots */
 #define AG_FX_WSTRIDE (AG_WCAP + 4)
-#define AG_FX_HOT 8192u /* entries of the shared-memory table (64 KB) */
+#define AG_FX_HOT_BYTES 65536u /* shared-memory table of the gathered vector */
 extern __shared__ __align__(16) uint64_t ag_fx_stage[];
 
-template <bool GATHER>
-__global__ void __launch_bounds__(AG_BLK, 1) ag_fixed_kernel(const AgPullParams p)
+/* T: contribution type (uint64_t, uint32_t, uint16_t, uint8_t); KIND:
+ * AG_INT_FIXED or AG_INT_QUANT (narrow T only); GATHER: sums only */
+template <typename T, int KIND, bool GATHER>
+__global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
 {
+    constexpr bool WIDE = sizeof(T) == 8;
+    constexpr bool QUANT = KIND == AG_INT_QUANT;
+    constexpr uint32_t HOT = AG_FX_HOT_BYTES / sizeof(T);
     __shared__ double s_redd[AG_WARPS];
     __shared__ uint32_t s_redu[AG_WARPS];
+    __shared__ uint32_t s_mn[AG_WARPS], s_mx[AG_WARPS];
     __shared__ uint32_t s_last;
     if (!GATHER && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
         return;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t nwarps = gridDim.x * AG_WARPS;
     uint64_t *vals = ag_fx_stage + (size_t)warp * AG_FX_WSTRIDE;
-    uint64_t *hot = ag_fx_stage + (size_t)AG_WARPS * AG_FX_WSTRIDE;
+    T *hot = reinterpret_cast<T *>(ag_fx_stage + (size_t)AG_WARPS * AG_FX_WSTRIDE);
     const uint32_t pass = GATHER ? 0u : p.ctl->iter;
-    const uint64_t *cin = GATHER ? p.x64 : ((pass & 1u) ? p.c64_1 : p.c64_0);
+    /* quantised forms read one buffer (re-quantised between passes); fixed
+     * forms ping-pong */
+    const T *cin = reinterpret_cast<const T *>(GATHER ? p.x64 : (QUANT || !(pass & 1u)) ? p.c64_0 : p.c64_1);
+    T *cout = reinterpret_cast<T *>((pass & 1u) ? p.c64_0 : p.c64_1);
     /* the most-gathered values (the first ids after the relabelling by
-     * out-degree) are copied into shared memory once per pass */
-    const uint32_t hot_n = min(p.N, (uint32_t)AG_FX_HOT);
-    for (uint32_t i = tid; i < hot_n; i += AG_BLK)
-        hot[i] = __ldg(cin + i);
+     * out-degree) are copied into shared memory once per pass, 16 bytes at a
+     * time (the buffers hold at least 16 bytes past their last element) */
+    const uint32_t hot_n = min(p.N, HOT);
+    {
+        const uint32_t nvec = (hot_n * (uint32_t)sizeof(T) + 15u) >> 4;
+        const uint4 *src = reinterpret_cast<const uint4 *>(cin);
+        uint4 *dst = reinterpret_cast<uint4 *>(hot);
+        for (uint32_t i = tid; i < nvec; i += AG_BLK)
+            dst[i] = __ldg(src + i);
+    }
     __syncthreads();
-    auto gather = [&](uint32_t u) -> uint64_t { return u < hot_n ? hot[u] : __ldg(cin + u); };
-    uint64_t *cout = (pass & 1u) ? p.c64_0 : p.c64_1;
+    auto gather = [&](uint32_t u) -> uint64_t { return u < hot_n ? (uint64_t)hot[u] : (uint64_t)__ldg(cin + u); };
+    float qscale = 0.0f;
+    if constexpr (QUANT && !GATHER)
+        qscale = ag_quant_scale<T>(p.qmm, pass & 1u);
     const double eps = GATHER ? 0.0 : p.ctl->eps;
     double my_err = 0.0;
-    uint32_t my_active = 0;
+    uint32_t my_active = 0, my_mn = 0xFFFFFFFFu, my_mx = 0u;
 
-    /* the reference's update of row r from its fixed-point sum; rp and od
-     * are the row's previous rank and out-degree, loaded ahead of time */
+    /* the reference's update of row r from its integer sum; rp and od are the
+     * row's previous rank and out-degree, loaded ahead of time */
     auto finish = [&](uint32_t r, uint64_t s, float rp, uint32_t od) {
         if (GATHER) {
             p.y64[r] = s;
             return;
         }
-        const float rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_fixed2d(s))));
+        float rn;
+        if constexpr (WIDE)
+            rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_fixed2d(s))));
+        else if constexpr (QUANT)
+            rn = __fadd_rn(p.base, __fmul_rn(p.damp, __fmul_rn(qscale, __ull2float_rn(s))));
+        else
+            rn = __fadd_rn(p.base, __fmul_rn(p.damp, ag_from_fixed<T>(s)));
         const double err = (double)fabsf(__fsub_rn(rn, rp));
         my_err += err;
         my_active += (err >= eps) ? 1u : 0u;
         p.rank[r] = rn;
-        cout[r] = od ? ag_d2fixed((double)__fdiv_rn(rn, __uint2float_rn(od))) : 0ull;
+        if constexpr (QUANT) {
+            const float c = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
+            p.cqf[r] = c;
+            const uint32_t k = ag_fkey(c);
+            my_mn = min(my_mn, k);
+            my_mx = max(my_mx, k);
+        } else if constexpr (WIDE) {
+            cout[r] = od ? ag_d2fixed((double)__fdiv_rn(rn, __uint2float_rn(od))) : 0ull;
+        } else {
+            cout[r] = od ? ag_to_fixed<T>(__fdiv_rn(rn, __uint2float_rn(od))) : (T)0;
+        }
     };
 
     /* the next item's descriptor is requested before the current item runs */
@@ -192,7 +294,8 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_fixed_kernel(const AgPullParams 
     if (GATHER)
         return;
 
-    /* close the pass: CTA totals, then the last CTA records the pass and sets
+    /* close the pass: CTA totals (and the quantised forms' min/max keys of
+     * the next contributions), then the last CTA records the pass and sets
      * the loop condition */
     {
         double e = my_err;
@@ -202,22 +305,37 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_fixed_kernel(const AgPullParams 
             e += __shfl_xor_sync(0xffffffffu, e, o);
             a += __shfl_xor_sync(0xffffffffu, a, o);
         }
+        if (QUANT) {
+            my_mn = __reduce_min_sync(0xffffffffu, my_mn);
+            my_mx = __reduce_max_sync(0xffffffffu, my_mx);
+        }
         if (lane == 0) {
             s_redd[warp] = e;
             s_redu[warp] = a;
+            s_mn[warp] = my_mn;
+            s_mx[warp] = my_mx;
         }
         __syncthreads();
         if (tid == 0) {
             double be = 0.0;
-            uint32_t ba = 0;
+            uint32_t ba = 0, bmn = 0xFFFFFFFFu, bmx = 0u;
             for (int w = 0; w < AG_WARPS; ++w) {
                 be += s_redd[w];
                 ba += s_redu[w];
+                bmn = min(bmn, s_mn[w]);
+                bmx = max(bmx, s_mx[w]);
             }
             if (be != 0.0)
                 atomicAdd(&p.ctl->err_acc, be);
             if (ba)
                 atomicAdd(&p.ctl->active_acc, ba);
+            if (QUANT) {
+                const uint32_t nslot = (pass + 1u) & 1u;
+                if (bmn != 0xFFFFFFFFu)
+                    atomicMin(&p.qmm[nslot], bmn);
+                if (bmx)
+                    atomicMax(&p.qmm[2 + nslot], bmx);
+            }
             __threadfence();
             const uint32_t ticket = atomicAdd(&p.ctl->done_ctas, 1u);
             s_last = (ticket == gridDim.x - 1) ? 1u : 0u;
@@ -238,6 +356,12 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_fixed_kernel(const AgPullParams 
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             c->hist_t[P] = t;
         }
+        if (QUANT) {
+            /* every CTA read this pass's slot at its start: free it for the
+             * pass after next */
+            p.qmm[P & 1u] = 0xFFFFFFFFu;
+            p.qmm[2 + (P & 1u)] = 0u;
+        }
         const bool conv = active == 0;
         c->prev_err = err;
         c->last_err_sum = vc->err_acc;
@@ -254,15 +378,50 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_fixed_kernel(const AgPullParams 
     }
 }
 
-/* init: r = base (or the warm start), first fixed-point contributions,
- * control reset */
-__global__ void __launch_bounds__(AG_SBLK) ag_fixed_init_kernel(const AgPullParams p, const AgRunConfig run)
+/* init: r = base (or the warm start), first contributions (quantised forms:
+ * binary32 contributions and their min/max keys in slot 0, which the graph
+ * clears before this kernel), control reset */
+template <typename T, int KIND>
+__global__ void __launch_bounds__(AG_SBLK) ag_int_init_kernel(const AgPullParams p, const AgRunConfig run)
 {
+    constexpr bool WIDE = sizeof(T) == 8;
+    constexpr bool QUANT = KIND == AG_INT_QUANT;
+    __shared__ uint32_t s_mn[AG_SBLK / 32], s_mx[AG_SBLK / 32];
+    uint32_t mn = 0xFFFFFFFFu, mx = 0u;
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
         const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
         p.rank[v] = r0;
         const uint32_t od = p.outdeg[v];
-        p.c64_0[v] = od ? ag_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
+        if constexpr (QUANT) {
+            const float c = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
+            p.cqf[v] = c;
+            const uint32_t k = ag_fkey(c);
+            mn = min(mn, k);
+            mx = max(mx, k);
+        } else if constexpr (WIDE) {
+            p.c64_0[v] = od ? ag_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
+        } else {
+            reinterpret_cast<T *>(p.c64_0)[v] = od ? ag_to_fixed<T>(__fdiv_rn(r0, __uint2float_rn(od))) : (T)0;
+        }
+    }
+    if (QUANT) {
+        mn = __reduce_min_sync(0xffffffffu, mn);
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if ((threadIdx.x & 31) == 0) {
+            s_mn[threadIdx.x >> 5] = mn;
+            s_mx[threadIdx.x >> 5] = mx;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < AG_SBLK / 32; ++w) {
+                mn = min(mn, s_mn[w]);
+                mx = max(mx, s_mx[w]);
+            }
+            if (mn != 0xFFFFFFFFu)
+                atomicMin(&p.qmm[0], mn);
+            if (mx)
+                atomicMax(&p.qmm[2], mx);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         AgControl *c = p.ctl;
@@ -290,8 +449,36 @@ __global__ void __launch_bounds__(AG_SBLK) ag_fixed_init_kernel(const AgPullPara
     }
 }
 
-/* 64-bit vectors between caller order and device order */
-__global__ void ag_permute_in_u64_kernel(const uint32_t *perm, const uint64_t *x, uint64_t *x_new, uint32_t n)
+/* quantise the binary32 contributions with the scale of this pass's min/max
+ * slot: four per thread, one 4-, 8- or 16-byte store */
+template <typename T> __global__ void __launch_bounds__(AG_SBLK) ag_quant_kernel(const AgPullParams p)
+{
+    if (!p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
+        return;
+    const float scale = ag_quant_scale<T>(p.qmm, p.ctl->iter & 1u);
+    T *q = reinterpret_cast<T *>(p.c64_0);
+    const uint32_t n4 = p.N >> 2;
+    const uint32_t stride = gridDim.x * AG_SBLK;
+    for (uint32_t i = blockIdx.x * AG_SBLK + threadIdx.x; i < n4; i += stride) {
+        const float4 f = __ldg(reinterpret_cast<const float4 *>(p.cqf) + i);
+        const T a = ag_quantize<T>(f.x, scale), b = ag_quantize<T>(f.y, scale);
+        const T c = ag_quantize<T>(f.z, scale), d = ag_quantize<T>(f.w, scale);
+        if constexpr (sizeof(T) == 4)
+            reinterpret_cast<uint4 *>(q)[i] = make_uint4(a, b, c, d);
+        else if constexpr (sizeof(T) == 2)
+            reinterpret_cast<uint2 *>(q)[i] = make_uint2((uint32_t)a | ((uint32_t)b << 16), (uint32_t)c | ((uint32_t)d << 16));
+        else
+            reinterpret_cast<uint32_t *>(q)[i] =
+                (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)c << 16) | ((uint32_t)d << 24);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < (p.N & 3u)) {
+        const uint32_t v = (n4 << 2) + threadIdx.x;
+        q[v] = ag_quantize<T>(p.cqf[v], scale);
+    }
+}
+
+/* vectors between caller order and device order: W-bit in, 64-bit out */
+template <typename T> __global__ void ag_permute_in_kernel(const uint32_t *perm, const T *x, T *x_new, uint32_t n)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         x_new[i] = x[perm ? perm[i] : i];
@@ -303,30 +490,82 @@ __global__ void ag_permute_out_u64_kernel(const uint32_t *inv, const uint64_t *y
         y[v] = y_new[inv ? inv[v] : v];
 }
 
-extern "C" const void *ag_fixed_kernel_ptr(int gather)
+extern "C" const void *ag_int_kernel_ptr(int bytes, int quant, int gather)
 {
-    return gather ? (const void *)ag_fixed_kernel<true> : (const void *)ag_fixed_kernel<false>;
+    if (gather) {
+        switch (bytes) {
+        case 1: return (const void *)ag_int_kernel<uint8_t, AG_INT_FIXED, true>;
+        case 2: return (const void *)ag_int_kernel<uint16_t, AG_INT_FIXED, true>;
+        case 4: return (const void *)ag_int_kernel<uint32_t, AG_INT_FIXED, true>;
+        default: return (const void *)ag_int_kernel<uint64_t, AG_INT_FIXED, true>;
+        }
+    }
+    switch (bytes) {
+    case 1: return quant ? (const void *)ag_int_kernel<uint8_t, AG_INT_QUANT, false>
+                         : (const void *)ag_int_kernel<uint8_t, AG_INT_FIXED, false>;
+    case 2: return quant ? (const void *)ag_int_kernel<uint16_t, AG_INT_QUANT, false>
+                         : (const void *)ag_int_kernel<uint16_t, AG_INT_FIXED, false>;
+    case 4: return quant ? (const void *)ag_int_kernel<uint32_t, AG_INT_QUANT, false>
+                         : (const void *)ag_int_kernel<uint32_t, AG_INT_FIXED, false>;
+    default: return (const void *)ag_int_kernel<uint64_t, AG_INT_FIXED, false>;
+    }
 }
 
-extern "C" const void *ag_fixed_init_kernel_ptr(void) { return (const void *)ag_fixed_init_kernel; }
+extern "C" const void *ag_int_init_kernel_ptr(int bytes, int quant)
+{
+    switch (bytes) {
+    case 1: return quant ? (const void *)ag_int_init_kernel<uint8_t, AG_INT_QUANT>
+                         : (const void *)ag_int_init_kernel<uint8_t, AG_INT_FIXED>;
+    case 2: return quant ? (const void *)ag_int_init_kernel<uint16_t, AG_INT_QUANT>
+                         : (const void *)ag_int_init_kernel<uint16_t, AG_INT_FIXED>;
+    case 4: return quant ? (const void *)ag_int_init_kernel<uint32_t, AG_INT_QUANT>
+                         : (const void *)ag_int_init_kernel<uint32_t, AG_INT_FIXED>;
+    default: return (const void *)ag_int_init_kernel<uint64_t, AG_INT_FIXED>;
+    }
+}
 
-extern "C" cudaError_t ag_permute_u64(const uint32_t *map, const uint64_t *x, uint64_t *y, uint32_t n, int out,
-                                      cudaStream_t s)
+extern "C" const void *ag_quant_kernel_ptr(int bytes)
+{
+    switch (bytes) {
+    case 1: return (const void *)ag_quant_kernel<uint8_t>;
+    case 2: return (const void *)ag_quant_kernel<uint16_t>;
+    default: return (const void *)ag_quant_kernel<uint32_t>;
+    }
+}
+
+static unsigned ag_elem_blocks(uint32_t n)
+{
+    unsigned blocks = (n + 255) / 256;
+    return blocks > 148 * 16 ? 148 * 16 : blocks;
+}
+
+extern "C" cudaError_t ag_permute_uint_in(const uint32_t *perm, const void *x, void *y, uint32_t n, int bytes,
+                                          cudaStream_t s)
 {
     if (n == 0)
         return cudaSuccess;
-    unsigned blocks = (n + 255) / 256;
-    if (blocks > 148 * 16)
-        blocks = 148 * 16;
-    if (out)
-        ag_permute_out_u64_kernel<<<blocks, 256, 0, s>>>(map, x, y, n);
-    else
-        ag_permute_in_u64_kernel<<<blocks, 256, 0, s>>>(map, x, y, n);
+    const unsigned blocks = ag_elem_blocks(n);
+    switch (bytes) {
+    case 1: ag_permute_in_kernel<uint8_t><<<blocks, 256, 0, s>>>(perm, (const uint8_t *)x, (uint8_t *)y, n); break;
+    case 2: ag_permute_in_kernel<uint16_t><<<blocks, 256, 0, s>>>(perm, (const uint16_t *)x, (uint16_t *)y, n); break;
+    case 4: ag_permute_in_kernel<uint32_t><<<blocks, 256, 0, s>>>(perm, (const uint32_t *)x, (uint32_t *)y, n); break;
+    default: ag_permute_in_kernel<uint64_t><<<blocks, 256, 0, s>>>(perm, (const uint64_t *)x, (uint64_t *)y, n); break;
+    }
     return cudaGetLastError();
 }
 
-/* dynamic shared memory of the fixed-point kernel (the warps' stages) */
+extern "C" cudaError_t ag_permute_u64_out(const uint32_t *inv, const uint64_t *x, uint64_t *y, uint32_t n,
+                                          cudaStream_t s)
+{
+    if (n == 0)
+        return cudaSuccess;
+    ag_permute_out_u64_kernel<<<ag_elem_blocks(n), 256, 0, s>>>(inv, x, y, n);
+    return cudaGetLastError();
+}
+
+/* dynamic shared memory of the integer kernels (the warps' stages and the
+ * 64 KB table) */
 extern "C" size_t ag_fixed_smem_bytes(void)
 {
-    return ((size_t)AG_WARPS * AG_FX_WSTRIDE + AG_FX_HOT) * sizeof(uint64_t);
+    return (size_t)AG_WARPS * AG_FX_WSTRIDE * sizeof(uint64_t) + AG_FX_HOT_BYTES;
 }

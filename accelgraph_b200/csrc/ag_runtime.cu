@@ -282,6 +282,24 @@ static ag_status_t copy_to_host(void *dst, const void *src, size_t bytes)
 }
 
 /* ------------------------------------------------------- graph handle */
+/* the integer pulls, AG_PREC_FIXED64 .. AG_PREC_QUANT8: contribution width in
+ * bytes and whether the form is quantised */
+#define AG_NUM_INT_FORMS (AG_PREC_QUANT8 - AG_PREC_FIXED64 + 1)
+
+static int is_int_prec(int prec) { return prec >= AG_PREC_FIXED64 && prec <= AG_PREC_QUANT8; }
+
+static int int_bytes(int prec)
+{
+    switch (prec) {
+    case AG_PREC_FIXED32: case AG_PREC_QUANT32: return 4;
+    case AG_PREC_FIXED16: case AG_PREC_QUANT16: return 2;
+    case AG_PREC_FIXED8: case AG_PREC_QUANT8: return 1;
+    default: return 8;
+    }
+}
+
+static int int_quant(int prec) { return prec >= AG_PREC_QUANT32 && prec <= AG_PREC_QUANT8; }
+
 struct AgExec
 {
     cudaGraph_t graph;
@@ -328,13 +346,17 @@ struct ag_graph_s
     int have_exe[3][2];
     /* data-driven mode: its launch graphs (FAST, EXACT) */
     AgExec exe_dd[2];
-    /* 64-bit fixed-point pull: contribution ping-pong, hub partials (capacity
-     * in chunks), and its launch graph (both orders give the same bits) */
+    /* integer pulls (fixed point and quantised): contribution buffers (the
+     * narrow forms use the first N * W/8 bytes), hub partials (capacity in
+     * chunks), the quantised forms' binary32 contributions and min/max key
+     * slots, and one launch graph per form (both orders give the same bits) */
     uint64_t *c64[2];
     uint64_t *hub_part64;
     uint32_t hub64_cap;
-    AgExec exe_fx;
-    int have_exe_fx;
+    float *cqf;
+    uint32_t *qmm;
+    AgExec exe_int[AG_NUM_INT_FORMS];
+    int have_exe_int[AG_NUM_INT_FORMS];
     int have_exe_dd[2];
     cudaEvent_t ev0, ev1;
     int launched;
@@ -389,10 +411,11 @@ static void drop_execs(ag_graph_s *g)
             free_exec(&g->exe_dd[b]);
             g->have_exe_dd[b] = 0;
         }
-    if (g->have_exe_fx) {
-        free_exec(&g->exe_fx);
-        g->have_exe_fx = 0;
-    }
+    for (int b = 0; b < AG_NUM_INT_FORMS; ++b)
+        if (g->have_exe_int[b]) {
+            free_exec(&g->exe_int[b]);
+            g->have_exe_int[b] = 0;
+        }
 }
 
 extern "C" ag_status_t ag_graph_release(ag_graph_t g)
@@ -405,6 +428,8 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->c64[0]);
     dev_free(g->c64[1]);
     dev_free(g->hub_part64);
+    dev_free(g->cqf);
+    dev_free(g->qmm);
     dev_free(g->row_off);
     dev_free(g->ids);
     dev_free(g->perm);
@@ -910,6 +935,8 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.c64_0 = g->c64[0];
     p.c64_1 = g->c64[1];
     p.hub_part64 = g->hub_part64;
+    p.cqf = g->cqf;
+    p.qmm = g->qmm;
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
@@ -920,29 +947,71 @@ static int pull_mode(const ag_graph_s *g, int dd)
     return dd ? AG_MODE_DD : (g->ngraphs ? AG_MODE_MULTI : AG_MODE_PR);
 }
 
-static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, int fx = 0)
+/* the solve's kernels: pull, init and (quantised forms) quantise */
+static const void *solve_pull_kernel(const ag_graph_s *g, int prec, int exact, int dd)
 {
-    AgExec *x = fx ? &g->exe_fx : dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
+    return is_int_prec(prec) ? ag_int_kernel_ptr(int_bytes(prec), int_quant(prec), 0)
+                             : ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
+}
+
+static size_t solve_smem(const ag_graph_s *g, int prec)
+{
+    return is_int_prec(prec) ? ag_fixed_smem_bytes() : pull_smem(g);
+}
+
+static dim3 elem_grid(const ag_graph_s *g)
+{
+    return dim3((unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8)));
+}
+
+/* prec: AG_PREC_* (the integer forms take both orders through one graph) */
+static AgExec *exec_slot(ag_graph_s *g, int prec, int exact, int dd)
+{
+    return is_int_prec(prec) ? &g->exe_int[prec - AG_PREC_FIXED64] : dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
+}
+
+static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
+{
+    const int ip = is_int_prec(prec), quant = ip && int_quant(prec);
+    AgExec *x = exec_slot(g, prec, exact, dd);
     memset(x, 0, sizeof(*x));
     AG_CUDA(cudaGraphCreate(&x->graph, 0));
     AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
     x->params = base_params(g, exact);
     x->params.cond = x->cond;
     x->params.use_cond = 1;
-    const void *kpull = fx ? ag_fixed_kernel_ptr(0) : ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
-    const size_t smem = fx ? ag_fixed_smem_bytes() : pull_smem(g);
+    const void *kpull = solve_pull_kernel(g, prec, exact, dd);
+    const size_t smem = solve_smem(g, prec);
     x->grid = pull_grid(kpull, x->params.ntasks, smem);
+
+    /* quantised forms: both min/max slots cleared before the init kernel
+     * folds the first contributions into slot 0 */
+    cudaGraphNode_t pre[2];
+    int npre = 0;
+    if (quant) {
+        cudaMemsetParams ms = {};
+        ms.dst = g->qmm;
+        ms.elementSize = 4;
+        ms.width = 2;
+        ms.height = 1;
+        ms.pitch = 0;
+        ms.value = 0xFFFFFFFFu;
+        AG_CUDA(cudaGraphAddMemsetNode(&pre[npre++], x->graph, nullptr, 0, &ms));
+        ms.dst = g->qmm + 2;
+        ms.value = 0u;
+        AG_CUDA(cudaGraphAddMemsetNode(&pre[npre++], x->graph, nullptr, 0, &ms));
+    }
 
     AgRunConfig run;
     memset(&run, 0, sizeof(run));
     void *init_args[2] = {&x->params, &run};
     cudaKernelNodeParams kp = {};
-    kp.func = (void *)(fx ? ag_fixed_init_kernel_ptr() : ag_init_kernel_ptr(prec));
-    kp.gridDim = dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK,
-                                                                          (uint64_t)g_ctx.num_sms * 8)));
+    kp.func = (void *)(ip ? ag_int_init_kernel_ptr(int_bytes(prec), quant) : ag_init_kernel_ptr(prec));
+    kp.gridDim = elem_grid(g);
     kp.blockDim = dim3(AG_SBLK);
     kp.kernelParams = init_args;
-    AG_CUDA(cudaGraphAddKernelNode(&x->init_node, x->graph, nullptr, 0, &kp));
+    AG_CUDA(cudaGraphAddKernelNode(&x->init_node, x->graph, npre ? pre : nullptr, (size_t)npre, &kp));
 
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -954,6 +1023,16 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, in
     cudaGraph_t body = cp.conditional.phGraph_out[0];
 
     void *pull_args[1] = {&x->params};
+    /* quantised forms: each iteration first quantises the contributions */
+    cudaGraphNode_t qnode;
+    if (quant) {
+        cudaKernelNodeParams kq = {};
+        kq.func = (void *)ag_quant_kernel_ptr(int_bytes(prec));
+        kq.gridDim = elem_grid(g);
+        kq.blockDim = dim3(AG_SBLK);
+        kq.kernelParams = pull_args;
+        AG_CUDA(cudaGraphAddKernelNode(&qnode, body, nullptr, 0, &kq));
+    }
     cudaKernelNodeParams kb = {};
     kb.func = (void *)kpull;
     kb.gridDim = dim3(x->grid);
@@ -961,7 +1040,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, in
     kb.sharedMemBytes = (unsigned)smem;
     kb.kernelParams = pull_args;
     cudaGraphNode_t pnode;
-    AG_CUDA(cudaGraphAddKernelNode(&pnode, body, nullptr, 0, &kb));
+    AG_CUDA(cudaGraphAddKernelNode(&pnode, body, quant ? &qnode : nullptr, quant ? 1 : 0, &kb));
 
     void *norm_args[1] = {&x->params};
     cudaKernelNodeParams kn = {};
@@ -973,8 +1052,8 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, in
     AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
 
     AG_CUDA(cudaGraphInstantiate(&x->exec, x->graph, 0));
-    if (fx)
-        g->have_exe_fx = 1;
+    if (ip)
+        g->have_exe_int[prec - AG_PREC_FIXED64] = 1;
     else if (dd)
         g->have_exe_dd[exact] = 1;
     else
@@ -982,11 +1061,25 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0, in
     return AG_OK;
 }
 
-/* fixed-point pull buffers, made on first use; the hub partials follow the
+static int have_exec(const ag_graph_s *g, int prec, int exact, int dd)
+{
+    return is_int_prec(prec) ? g->have_exe_int[prec - AG_PREC_FIXED64]
+           : dd              ? g->have_exe_dd[exact]
+                             : g->have_exe[prec][exact];
+}
+
+/* integer pull buffers, made on first use; the hub partials follow the
  * work list's chunk count (a new tile shape may need more) */
-static ag_status_t ensure_fixed(ag_graph_s *g)
+static ag_status_t ensure_fixed(ag_graph_s *g, int quant = 0)
 {
     ag_status_t st = AG_OK;
+    if (quant && !g->cqf) {
+        g->cqf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        g->qmm = (uint32_t *)dev_alloc(g, 16, &st);
+        if (st != AG_OK)
+            return st;
+        drop_execs(g);
+    }
     if (!g->c64[0]) {
         g->c64[0] = (uint64_t *)dev_alloc(g, (size_t)g->N * 8 + 16, &st);
         g->c64[1] = (uint64_t *)dev_alloc(g, (size_t)g->N * 8 + 16, &st);
@@ -1029,18 +1122,19 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
     ag_pr_opts_init(&o);
     if (opts)
         memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
-    if (o.precision < 0 || o.precision > AG_PREC_FIXED64)
+    if (o.precision < 0 || o.precision > AG_PREC_QUANT8)
         return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
     if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks || o.data_driven))
         return ag_set_error(AG_ERR_UNSUPPORTED, "a graph union runs the FP32 form without a warm start");
     const int dd = o.data_driven ? 1 : 0;
     if (dd && (o.precision != AG_PREC_FP32 || g->norm_n || g->c_base))
         return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven pull runs in FP32 on a whole graph");
-    const int fx = o.precision == AG_PREC_FIXED64 ? 1 : 0;
-    if (fx && (g->norm_n || g->c_base))
-        return ag_set_error(AG_ERR_UNSUPPORTED, "the fixed-point pull runs on a whole graph");
-    const int prec = fx ? 0 : o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
-    ag_status_t st = fx ? ensure_fixed(g) : ensure_buffers(g, prec);
+    const int ip = is_int_prec(o.precision);
+    if (ip && (g->norm_n || g->c_base))
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the fixed-point and quantised pulls run on a whole graph");
+    const int prec = o.precision, exact = o.order == AG_ORDER_EXACT ? 1 : 0;
+    const int quant = ip && int_quant(prec);
+    ag_status_t st = ip ? ensure_fixed(g, quant) : ensure_buffers(g, prec);
     if (st != AG_OK)
         return st;
     if (o.init_ranks && !g->init_buf) {
@@ -1050,12 +1144,12 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         /* rebuild cached graphs: their parameters carry the warm-start pointer */
         drop_execs(g);
     }
-    if (fx ? !g->have_exe_fx : dd ? !g->have_exe_dd[exact] : !g->have_exe[prec][exact]) {
-        st = build_exec(g, prec, exact, dd, fx);
+    if (!have_exec(g, prec, exact, dd)) {
+        st = build_exec(g, prec, exact, dd);
         if (st != AG_OK)
             return st;
     }
-    AgExec *x = fx ? &g->exe_fx : dd ? &g->exe_dd[exact] : &g->exe[prec][exact];
+    AgExec *x = exec_slot(g, prec, exact, dd);
     cudaStream_t s = g_ctx.stream;
     if (o.init_ranks && g->N)
         AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4,
@@ -1081,12 +1175,19 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         cudaKernelNodeParams ki;
         AG_CUDA(cudaGraphKernelNodeGetParams(x->init_node, &ki));
         void *ia[2] = {&sp, &run};
+        if (quant) {
+            AG_CUDA(cudaMemsetAsync(g->qmm, 0xFF, 8, s));
+            AG_CUDA(cudaMemsetAsync(g->qmm + 2, 0, 8, s));
+        }
         AG_CUDA(cudaLaunchKernel(ki.func, ki.gridDim, ki.blockDim, ia, 0, s));
         void *pa[1] = {&sp};
-        const void *kpull = fx ? ag_fixed_kernel_ptr(0) : ag_pull_kernel_ptr(pull_mode(g, dd), prec, exact);
-        const size_t smem = fx ? ag_fixed_smem_bytes() : pull_smem(g);
-        for (uint32_t i = 0; i < run.max_iter; ++i)
+        const void *kpull = solve_pull_kernel(g, prec, exact, dd);
+        const size_t smem = solve_smem(g, prec);
+        for (uint32_t i = 0; i < run.max_iter; ++i) {
+            if (quant)
+                AG_CUDA(cudaLaunchKernel(ag_quant_kernel_ptr(int_bytes(prec)), ki.gridDim, ki.blockDim, pa, 0, s));
             AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, smem, s));
+        }
         AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
     } else {
         AG_CUDA(cudaGraphLaunch(x->exec, s));
@@ -1885,48 +1986,60 @@ extern "C" ag_status_t ag_graph_build(uint32_t num_vertices, uint64_t num_edges,
     return st != AG_OK ? st : w;
 }
 
-/* ------------------------------------------------ fixed-point gather */
-extern "C" ag_status_t ag_gather_u64(ag_graph_t g, const uint64_t *x, uint64_t *y)
+/* ------------------------------------------------ integer gathers */
+extern "C" ag_status_t ag_gather_uint(ag_graph_t g, const void *x, uint32_t elem_bytes, uint64_t *y)
 {
     ag_clear_error();
     if (!g || (g->N && (!x || !y)))
-        return ag_set_error(AG_ERR_INVALID_ARG, "ag_gather_u64: NULL argument");
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_gather_uint: NULL argument");
+    if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_gather_uint: element size %u is not 1, 2, 4 or 8", elem_bytes);
     if (g->norm_n || g->c_base)
-        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_gather_u64: a row partition indexes a vector it does not hold");
+        return ag_set_error(AG_ERR_UNSUPPORTED, "ag_gather_uint: a row partition indexes a vector it does not hold");
     if (g->N == 0)
         return AG_OK;
     ag_status_t st = ensure_fixed(g);
     if (st != AG_OK)
         return st;
     cudaStream_t s = g_ctx.stream;
-    const size_t bytes = (size_t)g->N * 8;
-    uint64_t *buf = nullptr;
-    AG_CUDA(cudaMallocAsync((void **)&buf, 2 * bytes + 16, s));
-    uint64_t *xa = buf, *xb = buf + g->N;
-    cudaError_t e = cudaMemcpyAsync(xa, x, bytes, cudaMemcpyHostToDevice, s);
+    const size_t xbytes = (size_t)g->N * elem_bytes, ybytes = (size_t)g->N * 8;
+    /* two 64-bit vectors, the second 256-byte aligned; the kernel's 16-byte
+     * table copy may read up to 15 bytes past x */
+    const size_t off = (ybytes + 255) & ~(size_t)255;
+    uint8_t *buf = nullptr;
+    AG_CUDA(cudaMallocAsync((void **)&buf, off + ybytes + 16, s));
+    uint64_t *ya = (uint64_t *)buf, *yb = (uint64_t *)(buf + off);
+    /* x lands in ya (caller order), is permuted into yb (device order); the
+     * sums go to ya, then back to caller order in yb */
+    cudaError_t e = cudaMemcpyAsync(ya, x, xbytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-        e = ag_permute_u64(g->perm, xa, xb, g->N, 0, s);
+        e = ag_permute_uint_in(g->perm, ya, yb, g->N, (int)elem_bytes, s);
     if (e == cudaSuccess) {
         AgPullParams p = base_params(g, 0);
-        p.x64 = xb;
-        p.y64 = xa; /* the caller-order copy of x is no longer needed */
-        const void *k = ag_fixed_kernel_ptr(1);
+        p.x64 = yb;
+        p.y64 = ya;
+        const void *k = ag_int_kernel_ptr((int)elem_bytes, 0, 1);
         const unsigned grid = pull_grid(k, p.ntasks, ag_fixed_smem_bytes());
         void *args[1] = {&p};
         if (p.ntasks)
             e = cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, ag_fixed_smem_bytes(), s);
         else
-            e = cudaMemsetAsync(xa, 0, bytes, s);
+            e = cudaMemsetAsync(ya, 0, ybytes, s);
     }
     if (e == cudaSuccess)
-        e = ag_permute_u64(g->inv, xa, xb, g->N, 1, s);
+        e = ag_permute_u64_out(g->inv, ya, yb, g->N, s);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        st = ag_set_error(AG_ERR_CUDA, "ag_gather_u64: %s", cudaGetErrorString(e));
+        st = ag_set_error(AG_ERR_CUDA, "ag_gather_uint: %s", cudaGetErrorString(e));
     }
     if (st == AG_OK)
-        st = copy_to_host(y, xb, bytes);
+        st = copy_to_host(y, yb, ybytes);
     cudaFreeAsync(buf, s);
     ag_status_t w = stream_wait(s, 0);
     return st != AG_OK ? st : w;
+}
+
+extern "C" ag_status_t ag_gather_u64(ag_graph_t g, const uint64_t *x, uint64_t *y)
+{
+    return ag_gather_uint(g, x, 8, y);
 }

@@ -549,9 +549,11 @@ def run_data_driven(a):
 
 
 def run_fixed_point(a):
-    """64-bit fixed-point pull (the reference's pushpull 2) against the FP32
-    pull on the same graph: time to epsilon on the device, passes, accuracy
-    against the FP64 fixpoint, and the CPU oracle of the fixed-point pull."""
+    """The reference's integer pulls against the FP32 pull on the same graph:
+    64/32/16/8-bit fixed point (pushpull 2, 9, 10, 11) and 32/16/8-bit
+    quantised (pushpull 4, 12, 13).  Per form: time to epsilon on the device,
+    passes, pass time against the HBM roofline, accuracy against the FP64
+    fixpoint, and the CPU oracle of the same form."""
     import time
     import oracle
     ag = _gpu_setup()
@@ -560,9 +562,16 @@ def run_fixed_point(a):
     dg = ag.DeviceGraph(g)
     r64, _ = dg.pagerank_f64(5000, 1e-13)
     peak, kind = peak_hbm()
-    out = {"workload": f"fixed-point PageRank pull to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}",
-           "N": N, "E": E}
-    for name, prec, cbytes in (("fp32", ag.AG_PREC_FP32, 4), ("fixed64", ag.AG_PREC_FIXED64, 8)):
+    out = {"workload": f"integer PageRank pulls to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}",
+           "N": N, "E": E, "peak_gbs": peak, "peak_kind": kind,
+           "bytes_per_pass": "fixed W: 4E + (16 + 2 W/8) N; quantised W: 4E + (24 + 2 W/8) N "
+                             "(pull 4E + (20 + W/8) N, quantiser 4N + W/8 N); FP32: 4E + 24N"}
+    forms = (("fp32", ag.AG_PREC_FP32), ("fixed64", ag.AG_PREC_FIXED64), ("fixed32", ag.AG_PREC_FIXED32),
+             ("fixed16", ag.AG_PREC_FIXED16), ("fixed8", ag.AG_PREC_FIXED8), ("quant32", ag.AG_PREC_QUANT32),
+             ("quant16", ag.AG_PREC_QUANT16), ("quant8", ag.AG_PREC_QUANT8))
+    for name, prec in forms:
+        quant, width = ag.NARROW_FORM.get(prec, (False, 64 if prec == ag.AG_PREC_FIXED64 else 32))
+        cb = width // 8
         dg.pagerank(a.iterations, a.epsilon, precision=prec)
         best = None
         for _ in range(max(1, a.steps)):
@@ -571,17 +580,24 @@ def run_fixed_point(a):
                 best = (r, res)
         r, res = best
         rl, mx = _rel(r, r64)
-        alg = 4 * E + (16 + 2 * cbytes) * N + 4 * N
+        alg = 4 * E + ((24 + 2 * cb) if quant else (16 + 2 * cb)) * N
         pass_s = res.device_ms * 1e-3 / max(res.passes, 1)
         out[name] = {"device_ms_to_eps": res.device_ms, "passes": res.passes, "iterations": res.iterations,
-                     "pass_us": pass_s * 1e6, "roofline_frac": alg / pass_s / 1e9 / peak,
-                     "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx}
-    out["fixed64_vs_fp32_time"] = out["fp32"]["device_ms_to_eps"] / out["fixed64"]["device_ms_to_eps"]
-    t0 = time.perf_counter()
-    ref = oracle.pagerank_fixed64(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(),
-                                  a.iterations, a.epsilon)
-    out["cpu_oracle"] = {"seconds_to_eps": time.perf_counter() - t0, "iterations": ref["iterations"],
-                         "threads": oracle.lib.oracle_max_threads()}
+                     "converged": res.converged, "pass_us": pass_s * 1e6,
+                     "roofline_frac": alg / pass_s / 1e9 / peak, "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx}
+        if name != "fp32":
+            out[name]["time_vs_fp32"] = out["fp32"]["device_ms_to_eps"] / res.device_ms
+            t0 = time.perf_counter()
+            if prec == ag.AG_PREC_FIXED64:
+                ref = oracle.pagerank_fixed64(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(),
+                                              a.iterations, a.epsilon)
+            else:
+                ref = oracle.pagerank_narrow(quant, width, g.in_edges_idx(), g.in_degree(), g.in_neighbours(),
+                                             g.out_degree(), a.iterations, a.epsilon)
+            out[name]["cpu_oracle"] = {"seconds_to_eps": time.perf_counter() - t0, "iterations": ref["iterations"],
+                                       "threads": oracle.lib.oracle_max_threads(),
+                                       "bit_identical": bool(ref["iterations"] == res.iterations and
+                                                             (ref["ranks"].view("u4") == r.view("u4")).all())}
     print(json.dumps(out), flush=True)
 
 

@@ -211,6 +211,20 @@ ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, dou
                              (truncating), rows summed as integers modulo
                              2^64, the update formed in binary64; both orders
                              give the same bits */
+/* The reference's narrow integer pulls (pageRank.c:1455-1991 fixed point,
+ * :2119-2677 quantised; dispatched by pageRankGraphCSR on pushpull 9, 10, 11,
+ * 4, 12, 13).  Contributions are stored in W bits, rows summed as integers
+ * zero-extended into 64 bits, the update formed in binary32; both orders give
+ * the same bits.  Fixed point: W/2 fractional bits (Q16.16, Q8.8, Q4.4),
+ * conversion truncating.  Quantised: per pass, scale = (max - min) / (2^W - 1)
+ * over all contributions, q = round-half-even(c / scale) clamped to
+ * [0, 2^W - 1], r' = base + damp * (scale * sum). */
+#define AG_PREC_FIXED32 4
+#define AG_PREC_FIXED16 5
+#define AG_PREC_FIXED8  6
+#define AG_PREC_QUANT32 7
+#define AG_PREC_QUANT16 8
+#define AG_PREC_QUANT8  9
 
 #define AG_ORDER_FAST  0 /* rows of <= 32 in-edges summed in stream order,
                             longer rows by a fixed lane-strided tree         */
@@ -260,6 +274,13 @@ void ag_pr_opts_init(ag_pr_opts *opts);
  * FixedPoint compute unit (cu_PageRank/CSR/PULL/FixedPoint; testbench contract
  * pagerank_kernel_tb.sv:13-16). */
 ag_status_t ag_gather_u64(struct ag_graph_s *g, const uint64_t *x, uint64_t *y);
+/* Integer gather of 8-, 16-, 32- or 64-bit elements (elem_bytes 1, 2, 4, 8):
+ * y[v] = sum of x[u] over v's in-edges, each element zero-extended, as 64-bit
+ * integers modulo 2^64 (0 without in-edges); x and y in caller vertex order,
+ * host memory.  The Quantized compute unit's arithmetic for 4-byte elements
+ * (cu_PageRank/CSR/PULL/Quantized; testbench contract
+ * pagerank_kernel_tb.sv:17-19). */
+ag_status_t ag_gather_uint(struct ag_graph_s *g, const void *x, uint32_t elem_bytes, uint64_t *y);
 
 /* Status-returning form of pageRankPullGraphCSR with the precision, order and
  * warm-start options.  *out receives a stats object owned by the caller. */

@@ -42,6 +42,10 @@ def _load() -> C.CDLL:
     lib.oracle_pagerank_fixed64.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p,
                                             u32p, f64p, u32p, C.c_int]
     lib.oracle_pagerank_fixed64.restype = C.c_uint32
+    lib.oracle_gather_uint.argtypes = [C.c_uint32, u32p, u32p, u32p, C.c_void_p, C.c_uint32, u64p, C.c_int]
+    lib.oracle_pagerank_narrow.argtypes = [C.c_int, C.c_int, C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32,
+                                           C.c_double, f32p, u32p, f64p, u32p, C.c_int]
+    lib.oracle_pagerank_narrow.restype = C.c_uint32
     lib.oracle_pagerank_dd.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double,
                                        f32p, u32p, f64p, u32p, C.c_int]
     lib.oracle_pagerank_dd.restype = C.c_uint32
@@ -142,6 +146,43 @@ def pagerank_fixed64(in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4
     passes = lib.oracle_pagerank_fixed64(n, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_deg, u32p),
                                          iterations, epsilon, _p(ranks, f32p), C.byref(it), C.byref(et),
                                          _p(ha, u32p), threads)
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "active": ha[:passes]}
+
+
+_UINT = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+
+
+def gather_uint(in_idx, in_deg, in_nb, x, threads=0):
+    """Integer gather of 8/16/32/64-bit elements (the dtype of x) zero-extended
+    into 64-bit sums modulo 2^64 (rows without in-edges 0)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    x = np.ascontiguousarray(x)
+    if x.dtype not in [np.dtype(t) for t in _UINT.values()]:
+        raise TypeError("gather_uint: x must be uint8, uint16, uint32 or uint64")
+    y = np.zeros(len(in_deg), np.uint64)
+    lib.oracle_gather_uint(len(in_deg), _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p),
+                           x.ctypes.data_as(C.c_void_p), x.dtype.itemsize, _p(y, C.POINTER(C.c_uint64)), threads)
+    return y
+
+
+def pagerank_narrow(quant, width, in_idx, in_deg, in_nb, out_deg, iterations=20, epsilon=1e-4, threads=0):
+    """Narrow integer pulls: quant=False the W-bit fixed-point forms
+    (pageRank.c:1455-1991), quant=True the W-bit quantised forms
+    (pageRank.c:2119-2677), width 32, 16 or 8.  Returns dict(ranks,
+    iterations, passes, error_total, active)."""
+    if width not in (8, 16, 32):
+        raise ValueError("width must be 8, 16 or 32")
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    n = len(in_deg)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    ha = np.zeros(max(iterations, 1), np.uint32)
+    passes = lib.oracle_pagerank_narrow(1 if quant else 0, width, n, _p(in_idx, u32p), _p(in_deg, u32p),
+                                        _p(in_nb, u32p), _p(out_deg, u32p), iterations, epsilon, _p(ranks, f32p),
+                                        C.byref(it), C.byref(et), _p(ha, u32p), threads)
     return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
             "active": ha[:passes]}
 

@@ -263,6 +263,172 @@ uint32_t oracle_pagerank_fixed64(uint32_t n, const uint32_t *in_idx, const uint3
     return passes;
 }
 
+/* Integer gather of W-bit elements (elem_bytes 1, 2, 4 or 8), each
+ * zero-extended into a 64-bit sum modulo 2^64: the FixedPoint and Quantized
+ * compute units' contract (pagerank_kernel_tb.sv:13-19; 4-byte reads zero
+ * extended into the 8-byte accumulator in the Quantized context).  Rows
+ * without in-edges are not written. */
+void oracle_gather_uint(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, const uint32_t *in_nb,
+                        const void *x, uint32_t elem_bytes, uint64_t *y, int threads)
+{
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    uint32_t v;
+#pragma omp parallel for schedule(dynamic, 1024) num_threads(nt)
+    for (v = 0; v < n; v++) {
+        uint64_t s = 0;
+        uint32_t j;
+        if (!in_deg[v])
+            continue;
+        for (j = in_idx[v]; j < in_idx[v] + in_deg[v]; j++) {
+            const uint32_t u = in_nb[j];
+            switch (elem_bytes) {
+            case 1: s += ((const uint8_t *)x)[u]; break;
+            case 2: s += ((const uint16_t *)x)[u]; break;
+            case 4: s += ((const uint32_t *)x)[u]; break;
+            default: s += ((const uint64_t *)x)[u]; break;
+            }
+        }
+        y[v] = s;
+    }
+}
+
+/* Narrow fixed point (OpenGraph's FloatToFixed32/16/8 and Fixed32/16/8ToFloat
+ * are absent from the reference checkout): W-bit values with W/2 fractional
+ * bits.  Q16.16 for 32 bits is the format the reference's fixed-point SpMV
+ * compute unit assumes of its 32-bit operands (products shifted right by
+ * SCALEF = 16, cu_SPMV/CSR/PULL/FixedPoint/pkg/globals_cu_pkg.sv:37,
+ * cu_sum_kernel_control.sv:164); Q8.8 and Q4.4 follow it.  To fixed point:
+ * the binary32 product x * 2^(W/2) (exact) truncated toward zero, kept modulo
+ * 2^W.  Back: the 64-bit sum rounded once to binary32, scaled by 2^-(W/2). */
+static inline uint64_t oracle_f2fixed(float x, int W)
+{
+    const uint64_t mask = W >= 64 ? ~0ull : ((1ull << W) - 1);
+    return (uint64_t)(int64_t)(x * (float)(1u << (W / 2))) & mask;
+}
+
+static inline float oracle_fixed2f(uint64_t s, int W) { return (float)s / (float)(1u << (W / 2)); }
+
+/* Affine quantisation (OpenGraph's quantization.h is absent; restated from
+ * the published uniform affine scheme, Jacob et al., CVPR 2018, with the
+ * zero point the reference forces to 0, pageRank.c:2225-2226):
+ * scale = (max - min) / (2^W - 1) in binary32, q = round-half-even(x / scale)
+ * clamped to [0, 2^W - 1]; a zero scale quantises everything to 0. */
+static void oracle_minmax(const float *x, uint32_t n, float *mn, float *mx)
+{
+    uint32_t v;
+    float a = n ? x[0] : 0.0f, b = n ? x[0] : 0.0f;
+    for (v = 1; v < n; v++) {
+        if (x[v] < a)
+            a = x[v];
+        if (x[v] > b)
+            b = x[v];
+    }
+    *mn = a;
+    *mx = b;
+}
+
+static inline float oracle_quant_scale(float mn, float mx, int W)
+{
+    return (mx - mn) / (float)((1ull << W) - 1);
+}
+
+static inline uint64_t oracle_quantize(float x, float scale, int W)
+{
+    const uint64_t top = (1ull << W) - 1;
+    float q;
+    if (!(scale > 0.0f))
+        return 0;
+    q = rintf(x / scale);
+    if (!(q > 0.0f))
+        return 0;
+    if (q >= (float)top)
+        return top;
+    return (uint64_t)q;
+}
+
+static void oracle_store_uint(void *a, uint32_t v, uint64_t x, int W)
+{
+    switch (W) {
+    case 8: ((uint8_t *)a)[v] = (uint8_t)x; break;
+    case 16: ((uint16_t *)a)[v] = (uint16_t)x; break;
+    default: ((uint32_t *)a)[v] = (uint32_t)x; break;
+    }
+}
+
+/* Narrow integer pulls (W = 32, 16, 8):
+ *   quant = 0: fixed point, pageRank.c:1455-1991 (pushpull 9, 10, 11):
+ *     c[v] = FloatToFixedW(r[v] / out_degree[v]) (0 without out-edges),
+ *     r' = base + damp * FixedWToFloat(sum) in binary32;
+ *   quant = 1: quantised, pageRank.c:2119-2677 (pushpull 4, 12, 13):
+ *     f[v] = r[v] / out_degree[v] (0.0f without out-edges), min and max of f
+ *     over all vertices, scale from them, c[v] = quantize(f[v]),
+ *     r' = base + damp * (scale * (float)sum) in binary32.
+ * The W-bit contributions are gathered into 64-bit sums; residual, stop test
+ * and normalisation as in the plain pull. */
+uint32_t oracle_pagerank_narrow(int quant, int W, uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg,
+                                const uint32_t *in_nb, const uint32_t *out_deg, uint32_t iterations, double epsilon,
+                                float *ranks_out, uint32_t *iterations_out, double *error_total_out,
+                                uint32_t *hist_active, int threads)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    const int nt = threads > 0 ? threads : omp_get_max_threads();
+    float *pageRanks = ranks_out;
+    uint64_t *next = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
+    float *f = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    void *c = malloc((size_t)(n ? n : 1) * (size_t)(W / 8));
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v;
+    for (v = 0; v < n; v++)
+        pageRanks[v] = base_pr;
+    for (it = 0; it < iterations; it++) {
+        float scale = 0.0f;
+        error_total = 0;
+        activeVertices = 0;
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++)
+            f[v] = out_deg[v] ? pageRanks[v] / out_deg[v] : 0.0f;
+        if (quant) {
+            float mn, mx;
+            oracle_minmax(f, n, &mn, &mx);
+            scale = oracle_quant_scale(mn, mx, W);
+        }
+#pragma omp parallel for num_threads(nt)
+        for (v = 0; v < n; v++)
+            oracle_store_uint(c, v, quant ? oracle_quantize(f[v], scale, W) : (out_deg[v] ? oracle_f2fixed(f[v], W) : 0),
+                              W);
+        oracle_gather_uint(n, in_idx, in_deg, in_nb, c, (uint32_t)(W / 8), next, nt);
+#pragma omp parallel for reduction(+ : error_total, activeVertices) num_threads(nt)
+        for (v = 0; v < n; v++) {
+            float prevPageRank = pageRanks[v];
+            float nextPageRank = quant ? base_pr + damp * (scale * (float)next[v])
+                                       : base_pr + (damp * oracle_fixed2f(next[v], W));
+            pageRanks[v] = nextPageRank;
+            next[v] = 0;
+            double error = fabs(nextPageRank - prevPageRank);
+            error_total += (error / n);
+            if (error >= epsilon)
+                activeVertices++;
+        }
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (activeVertices == 0)
+            break;
+    }
+#pragma omp parallel for num_threads(nt)
+    for (v = 0; v < n; v++)
+        pageRanks[v] = pageRanks[v] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(next);
+    free(f);
+    free(c);
+    return passes;
+}
+
 /* Data-driven (worklist) pull, pageRank.c:2810-2969: every vertex starts
  * active; in each iteration the contributions of all vertices are formed
  * from the current ranks, every active vertex v gathers its in-edges in

@@ -66,6 +66,9 @@ def _load():
         lib.pageRankDataDrivenPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
         lib.pageRankPullFixedPoint64BitGraphCSR.restype = C.POINTER(_PageRankStats)
         lib.pageRankPullFixedPoint64BitGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
+        for name in _NARROW.values():
+            getattr(lib, name).restype = C.POINTER(_PageRankStats)
+            getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p]
         lib.freePageRankStats.argtypes = [C.POINTER(_PageRankStats)]
         lib.SPMVPullGraphCSR.restype = C.POINTER(_SPMVStats)
         lib.SPMVPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
@@ -122,6 +125,33 @@ def pagerank_fixed64(arguments_ptr, graph_ptr, num_vertices: int):
     lib.refemu_set_kernel(2)
     g0 = lib.refemu_gathers()
     st = lib.pageRankPullFixedPoint64BitGraphCSR(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
+    try:
+        s = st.contents
+        ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
+            np.zeros(0, np.float32)
+        out = {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total),
+               "gathers": int(lib.refemu_gathers() - g0)}
+    finally:
+        lib.freePageRankStats(st)
+    return out
+
+
+_NARROW = {(False, 32): "pageRankPullFixedPoint32BitGraphCSR", (False, 16): "pageRankPullFixedPoint16BitGraphCSR",
+           (False, 8): "pageRankPullFixedPoint8BitGraphCSR", (True, 32): "pageRankPullQuant32BitGraphCSR",
+           (True, 16): "pageRankPullQuant16BitGraphCSR", (True, 8): "pageRankPullQuant8BitGraphCSR"}
+
+
+def pagerank_narrow(quant: bool, width: int, arguments_ptr, graph_ptr, num_vertices: int):
+    """Run one of the reference's narrow integer pulls: the W-bit fixed-point
+    forms (pushpull 9, 10, 11; pageRank.c:1455-1991) or the W-bit quantised
+    forms (pushpull 4, 12, 13; pageRank.c:2119-2677), with the emulated
+    zero-extending integer gather and the stand-in conversions of
+    oracle/refstubs/fixedPoint.h and quantization.h."""
+    import numpy as np
+    lib = _load()
+    lib.refemu_set_kernel({32: 3, 16: 4, 8: 5}[width])
+    g0 = lib.refemu_gathers()
+    st = getattr(lib, _NARROW[(bool(quant), width)])(C.cast(arguments_ptr, C.c_void_p), C.cast(graph_ptr, C.c_void_p))
     try:
         s = st.contents
         ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \

@@ -14,7 +14,11 @@
  *     stream order, of auxiliary1[src_j] (PageRank CU) or w_j * auxiliary1[src_j]
  *     (SpMV CU, binary32 multiply then add), the accumulator starting from the
  *     first value, or the exact modulo-2^64 integer sum of 64-bit
- *     contributions (fixed-point PageRank CU, pagerank_kernel_tb.sv:13-16);
+ *     contributions (fixed-point PageRank CU, pagerank_kernel_tb.sv:13-16), or
+ *     the same sum of 32-, 16- or 8-bit contributions zero-extended into
+ *     64 bits (the narrow fixed-point and quantised pulls; the testbench's
+ *     Quantized context reads 4 bytes into the 8-byte accumulator,
+ *     pagerank_kernel_tb.sv:17-19);
  *     vertices without in-edges are not written.  These are the
  *     compute units' semantics (cu_sum_kernel_control.sv, golden models
  *     pagerank_kernel_tb.sv:303-314, spmv_kernel_tb.sv:304,359).  With no
@@ -40,11 +44,13 @@
 #include "timer.h"
 #include "worklist.h"
 
-static int g_emu_kernel = 0; /* 0: PageRank CU, 1: SpMV CU, 2: fixed-point PageRank CU */
+/* 0: PageRank CU, 1: SpMV CU, 2: 64-bit fixed-point PageRank CU,
+ * 3, 4, 5: 32-, 16-, 8-bit contributions into 64-bit sums */
+static int g_emu_kernel = 0;
 static struct WEDGraphCSR *g_emu_wed = NULL;
 static uint64_t g_emu_runs = 0;
 
-void refemu_set_kernel(int kind) { g_emu_kernel = (kind == 1 || kind == 2) ? kind : 0; }
+void refemu_set_kernel(int kind) { g_emu_kernel = (kind >= 1 && kind <= 5) ? kind : 0; }
 uint64_t refemu_gathers(void) { return g_emu_runs; }
 
 void Start(struct Timer *timer) { clock_gettime(CLOCK_MONOTONIC, &timer->start_time); }
@@ -138,10 +144,11 @@ void waitAFU(struct cxl_afu_h **afu, struct AFUStatus *afu_status)
     float *y = (float *)w->auxiliary2;
     const int spmv = g_emu_kernel == 1;
     int64_t v;
-    if (g_emu_kernel == 2) {
-        /* fixed-point CU: 64-bit contributions, exact integer sum modulo 2^64
-         * (pagerank_kernel_tb.sv:13-16) */
-        const uint64_t *x64 = (const uint64_t *)w->auxiliary1;
+    if (g_emu_kernel >= 2) {
+        /* integer CU: 64-, 32-, 16- or 8-bit contributions, exact integer sum
+         * modulo 2^64 (pagerank_kernel_tb.sv:13-19) */
+        const int kind = g_emu_kernel;
+        const void *xi = w->auxiliary1;
         uint64_t *y64 = (uint64_t *)w->auxiliary2;
 #pragma omp parallel for schedule(dynamic, 1024)
         for (v = 0; v < (int64_t)n; ++v) {
@@ -149,8 +156,13 @@ void waitAFU(struct cxl_afu_h **afu, struct AFUStatus *afu_status)
             uint64_t s = 0;
             if (!d)
                 continue;
-            for (uint32_t j = 0; j < d; ++j)
-                s += x64[src[b + j]];
+            for (uint32_t j = 0; j < d; ++j) {
+                const uint32_t u = src[b + j];
+                s += kind == 2   ? ((const uint64_t *)xi)[u]
+                     : kind == 3 ? ((const uint32_t *)xi)[u]
+                     : kind == 4 ? ((const uint16_t *)xi)[u]
+                                 : ((const uint8_t *)xi)[u];
+            }
             y64[v] = s;
         }
         afu_status->cu_return_done = n;

@@ -100,20 +100,21 @@ def run_inputs(run: dict, fx: dict, weighted: bool):
     return n, deg, idx, nb, w, od, x, position_dependent
 
 
-def fixed_inputs(run: dict, fx: dict):
-    """Inputs reproducing one FixedPoint-context testbench run as a gather.
+def fixed_inputs(run: dict, fx: dict, dtype=np.uint64):
+    """Inputs reproducing one FixedPoint-context (uint64 elements) or
+    Quantized-context (uint32 elements) testbench run as a gather.
 
-    The 64-bit contributions depend on the stream position, so every in-edge
-    is given a source vertex of its own (n + j for edge j) carrying its
-    element; the rows and their in-degrees are the fixture's."""
+    The contributions depend on the stream position, so every in-edge is
+    given a source vertex of its own (n + j for edge j) carrying its element;
+    the rows and their in-degrees are the fixture's."""
     n, deg, idx, nb, wt, od = fixture_csr(fx)
     e = len(nb)
-    x = np.zeros(n + e, np.uint64)
+    x = np.zeros(n + e, dtype)
     nb2 = (n + np.arange(e)).astype(np.uint32)
     for row in run["rows"]:
         v = row["v"]
         for k, el in enumerate(row["elements"]):
-            x[n + idx[v] + k] = np.uint64(int(el, 16))
+            x[n + idx[v] + k] = dtype(int(el, 16))
     deg2 = np.concatenate([deg, np.zeros(e, np.uint32)]).astype(np.uint32)
     idx2 = np.concatenate([idx, np.full(e, e, np.uint32)]).astype(np.uint32)
     return n, deg2, idx2, nb2, x

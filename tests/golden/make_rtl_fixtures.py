@@ -10,7 +10,10 @@ testbenches (AccelGraph,
                          (:303-314): the accumulator restarts with the first
                          value of a row and adds each following value; for
                          the FixedPoint context the 64-bit contributions
-                         (:256-263) and their exact sum modulo 2^64 (:13-16)
+                         (:256-263) and their exact sum modulo 2^64 (:13-16);
+                         for the Quantized context the same classes cut to
+                         32 bits (DATA_SIZE_READ = 4) and zero-extended into
+                         the 64-bit sum (:17-19, :312)
   spmv_kernel_tb.sv      coefficients w/2 (:277-293), product x*w in binary32
                          (:296-301) and the same stream-order sum (:349-359)
 and the 19-edge binary edge list 04_test_graphs/TEST/graphbrew/graph.bin.
@@ -104,9 +107,16 @@ def main() -> None:
             return 0xFFFF_FFFF_0000_0001 if k % 2 == 0 else (nb + 1) * 7
         return (nb + 1) * 7 + k
 
-    def fixed_runs():
+    def contribution_quant(cls: int, nb: int, k: int) -> int:
+        """the Quantized context's 32-bit contributions: the same classes at
+        DATA_SIZE_READ_BITS = 32 (pagerank_kernel_tb.sv:256-263)"""
+        return contribution_fixed(cls, nb, k) & 0xFFFF_FFFF
+
+    def fixed_runs(quant: bool = False):
         text = (TB / "pagerank_kernel_tb.sv").read_text()
         out = []
+        value = contribution_quant if quant else contribution_fixed
+        digits = 8 if quant else 16
         for m in re.finditer(r"run_fixture\((FX_[A-Z0-9_]+)\s*,\s*(CV_[A-Z]+)\s*,\s*0\s*\)", text):
             fx, cls = names[m.group(1)], cv[m.group(2)]
             fxd = fixtures[fx]
@@ -115,9 +125,9 @@ def main() -> None:
                 nbs = fxd["inverse_neighbours"][v]
                 if not nbs:
                     continue
-                vals = [contribution_fixed(cls, nb, k) for k, nb in enumerate(nbs)]
+                vals = [value(cls, nb, k) for k, nb in enumerate(nbs)]
                 acc = sum(vals) % (1 << 64)  # exact sum, wraps modulo 2^64 (:13-16, :312)
-                rows.append({"v": v, "elements": ["%016x" % x for x in vals], "golden": "%016x" % acc})
+                rows.append({"v": v, "elements": ["%0*x" % (digits, x) for x in vals], "golden": "%016x" % acc})
             out.append({"fixture": fxd["name"], "fixture_id": fx, "class": m.group(2), "rows": rows})
         return out
 
@@ -177,12 +187,13 @@ def main() -> None:
         "pagerank_runs": runs("pagerank_kernel_tb.sv", weighted=False),
         "spmv_runs": runs("spmv_kernel_tb.sv", weighted=True),
         "pagerank_fixed_runs": fixed_runs(),
+        "pagerank_quant_runs": fixed_runs(quant=True),
         "fp_exception_rows": exc,
         "graphbrew": {"src": raw[:, 0].tolist(), "dst": raw[:, 1].tolist()},
     }
     OUT.write_text(json.dumps(doc, indent=1) + "\n")
     print(f"wrote {OUT}: {len(fixtures)} fixtures, {len(doc['pagerank_runs'])} pagerank runs, "
-          f"{len(doc['pagerank_fixed_runs'])} fixed-point runs, "
+          f"{len(doc['pagerank_fixed_runs'])} fixed-point runs, {len(doc['pagerank_quant_runs'])} quantized runs, "
           f"{len(doc['spmv_runs'])} spmv runs, graphbrew {len(raw)} edges")
 
 

@@ -89,3 +89,21 @@ def test_oracle_fixed64_equals_reference_code(ag, oracle, refcode, iterations, e
         assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
         assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
         assert ref["gathers"] == mine["passes"], name
+
+
+@pytest.mark.parametrize("quant", [False, True])
+@pytest.mark.parametrize("width", [32, 16, 8])
+def test_oracle_narrow_equals_reference_code(ag, oracle, refcode, quant, width):
+    """The narrow integer pulls (fixed point pushpull 9/10/11, quantised
+    pushpull 4/12/13): the oracle restatement equals the reference's own host
+    code bit for bit, iteration count and per-pass gathers included."""
+    iterations, epsilon = 60, 1e-6
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(iterations, epsilon)
+        ref = refcode.pagerank_narrow(quant, width, C.byref(args), g.ptr, g.num_vertices)
+        mine = oracle.pagerank_narrow(quant, width, g.in_edges_idx(), g.in_degree(), g.in_neighbours(),
+                                      g.out_degree(), iterations, epsilon)
+        assert ref["iterations"] == mine["iterations"], name
+        assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
+        assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
+        assert ref["gathers"] == mine["passes"], name
