@@ -257,7 +257,7 @@ const void *ag_normalize_kernel_ptr(void);
 const void *ag_int_kernel_ptr(int bytes, int quant, int gather);
 const void *ag_int_init_kernel_ptr(int bytes, int quant);
 const void *ag_quant_kernel_ptr(int bytes);
-size_t ag_fixed_smem_bytes(void);
+size_t ag_fixed_smem_bytes(int bytes);
 /* vectors of `bytes`-byte elements into device order (y[i] = x[perm[i]]) and
  * 64-bit sums back to caller order (y[v] = x[inv[v]]); a NULL map is the
  * identity */

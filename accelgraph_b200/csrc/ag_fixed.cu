@@ -43,7 +43,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "ag_device.h"
+#include "ag_mem.h"
 
 #define AG_FX_ONE 4294967296.0 /* 2^32: 64-bit fixed-point unit */
 #define AG_INT_FIXED 0
@@ -122,6 +125,20 @@ __device__ __forceinline__ uint64_t ag_warp_sum_u64(uint64_t v)
  * first 16-byte quad, so they span up to AG_WCAP + 3 slots */
 #define AG_FX_WSTRIDE (AG_WCAP + 4)
 #define AG_FX_HOT_BYTES 65536u /* shared-memory table of the gathered vector */
+/* cache policy of the integer kernels (tuning builds may override):
+ *   AG_FX_IDS_NA    1: ids streamed without L1 lines, first out of L2
+ *   AG_FX_ROW_NA    1: row offsets, degrees and ranks read without L1 lines
+ *   AG_FX_GATHER    0: plain read-only gathers; 1: every gather may take an
+ *                   L1 line, kept in L2; 2: only the warm tier takes L1 lines */
+#ifndef AG_FX_IDS_NA
+#define AG_FX_IDS_NA 1
+#endif
+#ifndef AG_FX_ROW_NA
+#define AG_FX_ROW_NA 1
+#endif
+#ifndef AG_FX_GATHER
+#define AG_FX_GATHER 2
+#endif
 extern __shared__ __align__(16) uint64_t ag_fx_stage[];
 
 /* T: contribution type (uint64_t, uint32_t, uint16_t, uint8_t); KIND:
@@ -132,6 +149,8 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
     constexpr bool WIDE = sizeof(T) == 8;
     constexpr bool QUANT = KIND == AG_INT_QUANT;
     constexpr uint32_t HOT = AG_FX_HOT_BYTES / sizeof(T);
+    /* staged values: one element each, so 32 bits hold the narrow ones */
+    using S = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
     __shared__ double s_redd[AG_WARPS];
     __shared__ uint32_t s_redu[AG_WARPS];
     __shared__ uint32_t s_mn[AG_WARPS], s_mx[AG_WARPS];
@@ -140,8 +159,8 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
         return;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t nwarps = gridDim.x * AG_WARPS;
-    uint64_t *vals = ag_fx_stage + (size_t)warp * AG_FX_WSTRIDE;
-    T *hot = reinterpret_cast<T *>(ag_fx_stage + (size_t)AG_WARPS * AG_FX_WSTRIDE);
+    S *vals = reinterpret_cast<S *>(ag_fx_stage) + (size_t)warp * AG_FX_WSTRIDE;
+    T *hot = reinterpret_cast<T *>(reinterpret_cast<S *>(ag_fx_stage) + (size_t)AG_WARPS * AG_FX_WSTRIDE);
     const uint32_t pass = GATHER ? 0u : p.ctl->iter;
     /* quantised forms read one buffer (re-quantised between passes); fixed
      * forms ping-pong */
@@ -159,7 +178,20 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
             dst[i] = __ldg(src + i);
     }
     __syncthreads();
-    auto gather = [&](uint32_t u) -> uint64_t { return u < hot_n ? (uint64_t)hot[u] : (uint64_t)__ldg(cin + u); };
+    /* ids streamed once (no L1 line, first out of L2); gathers kept in L2,
+     * and below the warm tier (the same bytes of the vector as the FP32
+     * pull's tier, so 4 / sizeof(T) times its entries) allowed into L1 */
+    const uint64_t pol_first = ag_policy_evict_first(), pol_last = ag_policy_evict_last();
+    const uint32_t warm_n = (uint32_t)min((uint64_t)p.warm_n * 4u / sizeof(T), (uint64_t)p.N);
+    auto gather = [&](uint32_t u) -> uint64_t {
+        if (u < hot_n)
+            return (uint64_t)hot[u];
+        if (AG_FX_GATHER == 0)
+            return (uint64_t)__ldg(cin + u);
+        return ag_ld_gather_uint<T>(cin + u, pol_last, AG_FX_GATHER == 1 || u < warm_n);
+    };
+    auto ld_row = [&](const uint32_t *q) -> uint32_t { return AG_FX_ROW_NA ? ag_ld_row_u32(q) : __ldg(q); };
+    auto ld_rank = [&](const float *q) -> float { return AG_FX_ROW_NA ? ag_ld_rank(q) : *q; };
     float qscale = 0.0f;
     if constexpr (QUANT && !GATHER)
         qscale = ag_quant_scale<T>(p.qmm, pass & 1u);
@@ -198,75 +230,157 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
         }
     };
 
-    /* the next item's descriptor is requested before the current item runs */
+    /* a pair of 16-byte id quads per lane: quads qa and qa + 32 */
+    struct IdPair
+    {
+        uint4 a, b;
+    };
+    const uint4 *ids4 = reinterpret_cast<const uint4 *>(p.ids);
+    auto ld_quad = [&](uint32_t q) -> uint4 { return AG_FX_IDS_NA ? ag_ld_stream_u4(ids4 + q, pol_first) : __ldg(ids4 + q); };
+    auto load_pair = [&](uint32_t qa, uint32_t q1) -> IdPair {
+        IdPair r;
+        r.a = qa < q1 ? ld_quad(qa) : make_uint4(0, 0, 0, 0);
+        r.b = qa + 32 < q1 ? ld_quad(qa + 32) : make_uint4(0, 0, 0, 0);
+        return r;
+    };
+    /* the lane's first pair of an item's in-edges [eb, ee) */
+    auto prefetch = [&](uint32_t eb, uint32_t ee) -> IdPair { return load_pair((eb >> 2) + lane, (ee + 3u) >> 2); };
+    /* the eight values of a pair; in-edges outside [eb, ee) give 0 */
+    auto gather8 = [&](const IdPair &q, uint32_t qa, uint32_t eb, uint32_t ee, S *v) {
+        const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+        v[0] = (ja >= eb && ja < ee) ? (S)gather(q.a.x) : (S)0;
+        v[1] = (ja + 1 >= eb && ja + 1 < ee) ? (S)gather(q.a.y) : (S)0;
+        v[2] = (ja + 2 >= eb && ja + 2 < ee) ? (S)gather(q.a.z) : (S)0;
+        v[3] = (ja + 3 >= eb && ja + 3 < ee) ? (S)gather(q.a.w) : (S)0;
+        v[4] = (jb >= eb && jb < ee) ? (S)gather(q.b.x) : (S)0;
+        v[5] = (jb + 1 >= eb && jb + 1 < ee) ? (S)gather(q.b.y) : (S)0;
+        v[6] = (jb + 2 >= eb && jb + 2 < ee) ? (S)gather(q.b.z) : (S)0;
+        v[7] = (jb + 3 >= eb && jb + 3 < ee) ? (S)gather(q.b.w) : (S)0;
+    };
+
+    /* each warp walks its items with a stride of all warps; the first id
+     * pair of the next item is requested before the current one is gathered,
+     * summed and written, so it is in flight meanwhile */
     uint32_t t = blockIdx.x * AG_WARPS + warp;
-    uint4 task_n = t < p.ntasks ? __ldg(p.tasks + t) : make_uint4(0, 0, 0, 0);
-    for (; t < p.ntasks; t += nwarps) {
-        const uint4 task = task_n;
-        if (t + nwarps < p.ntasks)
-            task_n = __ldg(p.tasks + t + nwarps);
+    uint4 task = t < p.ntasks ? __ldg(p.tasks + t) : make_uint4(0, 0, 0, 0);
+    IdPair pf = prefetch(task.z, task.w);
+    while (t < p.ntasks) {
+        const uint32_t tn = t + nwarps;
+        const uint4 task_n = tn < p.ntasks ? __ldg(p.tasks + tn) : make_uint4(0, 0, 0, 0);
         const uint32_t kind = task.x >> 30;
         const uint32_t r0 = task.x & AG_ROW_MASK;
+        const uint32_t eb = task.z, ee = task.w;
+        IdPair pn;
         if (kind == AG_T_ROWS) {
-            /* the warp stages the item's values: 16-byte id loads, four
-             * gathers in flight per quad, slot j - (eb & ~3) for in-edge j;
-             * then each lane sums its row from shared memory */
-            const uint32_t eb = task.z, ee = task.w, q0 = eb >> 2, q1 = (ee + 3u) >> 2;
+            /* one row per lane: its bounds, previous rank and out-degree load
+             * first; the warp stages the item's values (slot j - eb for
+             * in-edge j), then each lane sums its row if it is short, the
+             * whole warp each long one */
             const uint32_t r = r0 + lane;
+            const bool live = r < task.y;
             uint32_t o0 = ee, o1 = ee, od = 0;
             float rp = 0.0f;
-            if (r < task.y) {
-                o0 = __ldg(p.row_off + r);
-                o1 = __ldg(p.row_off + r + 1);
+            if (live) {
+                o0 = ld_row(p.row_off + r);
+                o1 = ld_row(p.row_off + r + 1);
                 if (!GATHER) {
-                    rp = p.rank[r];
-                    od = __ldg(p.outdeg + r);
+                    rp = ld_rank(p.rank + r);
+                    od = ld_row(p.outdeg + r);
                 }
             }
-            for (uint32_t qa = q0 + lane; qa < q1; qa += 64) {
-                /* two quads per lane and round: eight gathers in flight */
-                const uint32_t qb = qa + 32;
-                const uint4 ia = __ldg(reinterpret_cast<const uint4 *>(p.ids) + qa);
-                const uint4 ib = qb < q1 ? __ldg(reinterpret_cast<const uint4 *>(p.ids) + qb) : make_uint4(0, 0, 0, 0);
-                const uint32_t ja = qa << 2, jb = qb << 2;
-                uint64_t v[8];
-                v[0] = (ja >= eb && ja < ee) ? gather(ia.x) : 0ull;
-                v[1] = (ja + 1 >= eb && ja + 1 < ee) ? gather(ia.y) : 0ull;
-                v[2] = (ja + 2 >= eb && ja + 2 < ee) ? gather(ia.z) : 0ull;
-                v[3] = (ja + 3 < ee) ? gather(ia.w) : 0ull;
-                v[4] = (jb < ee) ? gather(ib.x) : 0ull;
-                v[5] = (jb + 1 < ee) ? gather(ib.y) : 0ull;
-                v[6] = (jb + 2 < ee) ? gather(ib.z) : 0ull;
-                v[7] = (jb + 3 < ee) ? gather(ib.w) : 0ull;
-                uint64_t *q = vals + ((qa - q0) << 2);
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    q[k] = v[k];
-                if (qb < q1) {
-                    q = vals + ((qb - q0) << 2);
+            pn = prefetch(task_n.z, task_n.w);
+            {
+                const uint32_t q1 = (ee + 3u) >> 2;
+                uint32_t qa = (eb >> 2) + lane;
+                IdPair cur = pf;
+                while (qa < q1) {
+                    S v[8];
+                    gather8(cur, qa, eb, ee, v);
+                    if (qa + 64 < q1)
+                        cur = load_pair(qa + 64, q1);
+                    const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        q[k] = v[4 + k];
+                        if (ja + k >= eb && ja + k < ee)
+                            vals[ja + k - eb] = v[k];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (jb + k >= eb && jb + k < ee)
+                            vals[jb + k - eb] = v[4 + k];
+                    qa += 64;
                 }
             }
             __syncwarp();
-            if (r < task.y) {
-                uint64_t s = 0;
+            o0 -= eb;
+            o1 -= eb;
+            uint64_t s = 0;
+            const bool is_long = o1 - o0 > AG_TSEQ;
+            if (!is_long)
                 for (uint32_t j = o0; j < o1; ++j)
-                    s += vals[j - (q0 << 2)];
-                finish(r, s, rp, od);
+                    s += (uint64_t)vals[j];
+            unsigned m = __ballot_sync(0xffffffffu, is_long);
+            while (m) {
+                const int src = __ffs(m) - 1;
+                m &= m - 1;
+                const uint32_t a = __shfl_sync(0xffffffffu, o0, src);
+                const uint32_t b = __shfl_sync(0xffffffffu, o1, src);
+                uint64_t ts = 0;
+                for (uint32_t j = a + lane; j < b; j += 32)
+                    ts += (uint64_t)vals[j];
+                ts = ag_warp_sum_u64(ts);
+                if ((int)lane == src)
+                    s = ts;
             }
+            if (live)
+                finish(r, s, rp, od);
         } else {
             float rp = 0.0f;
             uint32_t od = 0;
             if (!GATHER && lane == 0 && kind == AG_T_LONG) {
-                rp = p.rank[r0];
-                od = __ldg(p.outdeg + r0);
+                rp = ld_rank(p.rank + r0);
+                od = ld_row(p.outdeg + r0);
             }
+            pn = prefetch(task_n.z, task_n.w);
+            /* warp-strided partial sums straight from memory: the values of
+             * one round are added while the next round's gathers travel and
+             * the ids of the round after load */
             uint64_t s = 0;
-#pragma unroll 4
-            for (uint32_t j = task.z + lane; j < task.w; j += 32)
-                s += gather(__ldg(p.ids + j));
+            {
+                const uint32_t q1 = (ee + 3u) >> 2;
+                uint32_t qa = (eb >> 2) + lane;
+                if constexpr (sizeof(S) == 8) {
+                    /* 64-bit values take twice the registers: one round in
+                     * flight */
+                    IdPair cur = pf;
+                    while (qa < q1) {
+                        const IdPair nx = load_pair(qa + 64, q1);
+                        S v[8];
+                        gather8(cur, qa, eb, ee, v);
+#pragma unroll
+                        for (int k = 0; k < 8; ++k)
+                            s += (uint64_t)v[k];
+                        cur = nx;
+                        qa += 64;
+                    }
+                } else if (qa < q1) {
+                    S v[8];
+                    gather8(pf, qa, eb, ee, v);
+                    IdPair nxt = load_pair(qa + 64, q1);
+                    while (qa < q1) {
+                        const uint32_t qn = qa + 64;
+                        const IdPair nn = load_pair(qn + 64, q1);
+                        S vn[8];
+                        gather8(nxt, qn, eb, ee, vn);
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            s += (uint64_t)v[k];
+                            v[k] = vn[k];
+                        }
+                        nxt = nn;
+                        qa = qn;
+                    }
+                }
+            }
             s = ag_warp_sum_u64(s);
             if (kind == AG_T_LONG) {
                 if (lane == 0)
@@ -290,6 +404,9 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
             }
         }
         __syncwarp();
+        pf = pn;
+        task = task_n;
+        t = tn;
     }
     if (GATHER)
         return;
@@ -563,9 +680,10 @@ extern "C" cudaError_t ag_permute_u64_out(const uint32_t *inv, const uint64_t *x
     return cudaGetLastError();
 }
 
-/* dynamic shared memory of the integer kernels (the warps' stages and the
+/* dynamic shared memory of the integer kernels of `bytes`-byte elements (the
+ * warps' stages, 64-bit for 64-bit elements and 32-bit otherwise, and the
  * 64 KB table) */
-extern "C" size_t ag_fixed_smem_bytes(void)
+extern "C" size_t ag_fixed_smem_bytes(int bytes)
 {
-    return (size_t)AG_WARPS * AG_FX_WSTRIDE * sizeof(uint64_t) + AG_FX_HOT_BYTES;
+    return (size_t)AG_WARPS * AG_FX_WSTRIDE * (bytes == 8 ? 8u : 4u) + AG_FX_HOT_BYTES;
 }

@@ -956,7 +956,7 @@ static const void *solve_pull_kernel(const ag_graph_s *g, int prec, int exact, i
 
 static size_t solve_smem(const ag_graph_s *g, int prec)
 {
-    return is_int_prec(prec) ? ag_fixed_smem_bytes() : pull_smem(g);
+    return is_int_prec(prec) ? ag_fixed_smem_bytes(int_bytes(prec)) : pull_smem(g);
 }
 
 static dim3 elem_grid(const ag_graph_s *g)
@@ -2019,10 +2019,11 @@ extern "C" ag_status_t ag_gather_uint(ag_graph_t g, const void *x, uint32_t elem
         p.x64 = yb;
         p.y64 = ya;
         const void *k = ag_int_kernel_ptr((int)elem_bytes, 0, 1);
-        const unsigned grid = pull_grid(k, p.ntasks, ag_fixed_smem_bytes());
+        const size_t smem = ag_fixed_smem_bytes((int)elem_bytes);
+        const unsigned grid = pull_grid(k, p.ntasks, smem);
         void *args[1] = {&p};
         if (p.ntasks)
-            e = cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, ag_fixed_smem_bytes(), s);
+            e = cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, smem, s);
         else
             e = cudaMemsetAsync(ya, 0, ybytes, s);
     }
