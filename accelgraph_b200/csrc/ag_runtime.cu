@@ -965,6 +965,15 @@ static dim3 elem_grid(const ag_graph_s *g)
         1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8)));
 }
 
+/* the quantiser: one group of four contributions per thread, so that every
+ * load is in flight at once (its divisions are long dependent chains) */
+static dim3 quant_grid(const ag_graph_s *g)
+{
+    const uint64_t groups = ((uint64_t)g->N + 3) / 4;
+    return dim3((unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((groups + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 64)));
+}
+
 /* prec: AG_PREC_* (the integer forms take both orders through one graph) */
 static AgExec *exec_slot(ag_graph_s *g, int prec, int exact, int dd)
 {
@@ -1028,7 +1037,7 @@ static ag_status_t build_exec(ag_graph_s *g, int prec, int exact, int dd = 0)
     if (quant) {
         cudaKernelNodeParams kq = {};
         kq.func = (void *)ag_quant_kernel_ptr(int_bytes(prec));
-        kq.gridDim = elem_grid(g);
+        kq.gridDim = quant_grid(g);
         kq.blockDim = dim3(AG_SBLK);
         kq.kernelParams = pull_args;
         AG_CUDA(cudaGraphAddKernelNode(&qnode, body, nullptr, 0, &kq));
@@ -1185,7 +1194,7 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         const size_t smem = solve_smem(g, prec);
         for (uint32_t i = 0; i < run.max_iter; ++i) {
             if (quant)
-                AG_CUDA(cudaLaunchKernel(ag_quant_kernel_ptr(int_bytes(prec)), ki.gridDim, ki.blockDim, pa, 0, s));
+                AG_CUDA(cudaLaunchKernel(ag_quant_kernel_ptr(int_bytes(prec)), quant_grid(g), dim3(AG_SBLK), pa, 0, s));
             AG_CUDA(cudaLaunchKernel(kpull, dim3(x->grid), dim3(AG_BLK), pa, smem, s));
         }
         AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), ki.gridDim, ki.blockDim, pa, 0, s));
