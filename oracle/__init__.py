@@ -46,6 +46,12 @@ def _load() -> C.CDLL:
     lib.oracle_pagerank_narrow.argtypes = [C.c_int, C.c_int, C.c_uint32, u32p, u32p, u32p, u32p, C.c_uint32,
                                            C.c_double, f32p, u32p, f64p, u32p, C.c_int]
     lib.oracle_pagerank_narrow.restype = C.c_uint32
+    lib.oracle_pagerank_push.argtypes = [C.c_int, C.c_uint32, u32p, u32p, u32p, C.c_uint32, C.c_double, f32p, u32p,
+                                         f64p, u32p]
+    lib.oracle_pagerank_push.restype = C.c_uint32
+    lib.oracle_pagerank_residual.argtypes = [C.c_int, C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p, C.c_uint32,
+                                             C.c_double, f32p, u32p, f64p, u32p]
+    lib.oracle_pagerank_residual.restype = C.c_uint32
     lib.oracle_pagerank_dd.argtypes = [C.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p, C.c_uint32, C.c_double,
                                        f32p, u32p, f64p, u32p, C.c_int]
     lib.oracle_pagerank_dd.restype = C.c_uint32
@@ -183,6 +189,47 @@ def pagerank_narrow(quant, width, in_idx, in_deg, in_nb, out_deg, iterations=20,
     passes = lib.oracle_pagerank_narrow(1 if quant else 0, width, n, _p(in_idx, u32p), _p(in_deg, u32p),
                                         _p(in_nb, u32p), _p(out_deg, u32p), iterations, epsilon, _p(ranks, f32p),
                                         C.byref(it), C.byref(et), _p(ha, u32p), threads)
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "active": ha[:passes]}
+
+
+PUSH_FLOAT, PUSH_FIXED64, PUSH_QUANT32 = 0, 1, 2
+
+
+def pagerank_push(kind, out_idx, out_deg, out_nb, iterations=20, epsilon=1e-4):
+    """Push forms, single-thread instance (sources in vertex order): kind
+    PUSH_FLOAT (pushpull 1, pageRank.c:1111-1272), PUSH_FIXED64 (pushpull 3,
+    :1992-2118) or PUSH_QUANT32 (pushpull 5, :2678-2809).  Returns
+    dict(ranks, iterations, passes, error_total, active)."""
+    out_idx, out_deg, out_nb = _csr(out_idx, out_deg, out_nb)
+    n = len(out_deg)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    ha = np.zeros(max(iterations, 1), np.uint32)
+    passes = lib.oracle_pagerank_push(kind, n, _p(out_idx, u32p), _p(out_deg, u32p), _p(out_nb, u32p), iterations,
+                                      epsilon, _p(ranks, f32p), C.byref(it), C.byref(et), _p(ha, u32p))
+    return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
+            "active": ha[:passes]}
+
+
+def pagerank_residual(pull_push, in_idx, in_deg, in_nb, out_idx, out_deg, out_nb, iterations=20, epsilon=1e-4):
+    """Residual forms with a worklist, single-thread instance: pull_push=False
+    the data-driven push (pushpull 7, pageRank.c:2971-3127), True the
+    data-driven pull-push (pushpull 8, :3128-3325).  Returns dict(ranks,
+    iterations, passes, error_total, active) (active: activations per
+    iteration)."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_idx, out_deg, out_nb = _csr(out_idx, out_deg, out_nb)
+    n = len(in_deg)
+    ranks = np.zeros(n, np.float32)
+    it = C.c_uint32()
+    et = C.c_double()
+    ha = np.zeros(max(iterations, 1), np.uint32)
+    passes = lib.oracle_pagerank_residual(1 if pull_push else 0, n, _p(in_idx, u32p), _p(in_deg, u32p),
+                                          _p(in_nb, u32p), _p(out_idx, u32p), _p(out_deg, u32p), _p(out_nb, u32p),
+                                          iterations, epsilon, _p(ranks, f32p), C.byref(it), C.byref(et),
+                                          _p(ha, u32p))
     return {"ranks": ranks, "iterations": it.value, "passes": passes, "error_total": et.value,
             "active": ha[:passes]}
 

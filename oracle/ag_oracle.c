@@ -512,6 +512,194 @@ uint32_t oracle_pagerank_dd(uint32_t n, const uint32_t *in_idx, const uint32_t *
     return passes;
 }
 
+/* Push forms (pageRankGraphCSR pushpull 1, 3, 5): the host steps of the pull
+ * with the gather turned around: every vertex v adds its contribution into
+ * next[u] along each of its forward edges.  The reference runs these with
+ * OpenMP (pushpull 3, 5: unsynchronised or atomic adds from many threads) or
+ * on the FPGA's push unit (pushpull 1), so their add order is not fixed; this
+ * restatement is their single-thread instance: sources in vertex order, each
+ * source's out-edges in forward-row order, every next[u] starting from 0.
+ *   kind 0: pushpull 1, pageRank.c:1111-1272: binary32 c = r / out_degree,
+ *           binary32 adds, r' = base + damp * next;
+ *   kind 1: pushpull 3, pageRank.c:1992-2118: c = DoubleToFixed64(r / od),
+ *           64-bit integer adds, r' = base + damp * Fixed64ToDouble(next) in
+ *           binary64, stored binary32;
+ *   kind 2: pushpull 5, pageRank.c:2678-2809: binary32 c, min/max, 32-bit
+ *           quantisation with the pass's scale and zero point (OpenGraph's
+ *           GetZeroPoint is absent; its value is restated as 0, the zero
+ *           point the quantised pulls use), binary32 adds of
+ *           scale * (q - zero), r' = base + damp * next.
+ * Residual, stop test and normalisation as in the pull. */
+uint32_t oracle_pagerank_push(int kind, uint32_t n, const uint32_t *out_idx, const uint32_t *out_deg,
+                              const uint32_t *out_nb, uint32_t iterations, double epsilon, float *ranks_out,
+                              uint32_t *iterations_out, double *error_total_out, uint32_t *hist_active)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    float *pageRanks = ranks_out;
+    float *next = (float *)calloc(n ? n : 1, sizeof(float));
+    uint64_t *next64 = (uint64_t *)calloc(n ? n : 1, sizeof(uint64_t));
+    float *c = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    uint64_t *c64 = (uint64_t *)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+    uint32_t *q = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v, j;
+    for (v = 0; v < n; v++)
+        pageRanks[v] = base_pr;
+    for (it = 0; it < iterations; it++) {
+        float scale = 0.0f;
+        const uint32_t zero = 0;
+        error_total = 0;
+        activeVertices = 0;
+        for (v = 0; v < n; v++) {
+            c[v] = out_deg[v] ? pageRanks[v] / out_deg[v] : 0.0f;
+            if (kind == 1)
+                c64[v] = out_deg[v] ? oracle_d2fixed64(pageRanks[v] / out_deg[v]) : 0;
+        }
+        if (kind == 2) {
+            float mn, mx;
+            oracle_minmax(c, n, &mn, &mx);
+            scale = oracle_quant_scale(mn, mx, 32);
+            for (v = 0; v < n; v++)
+                q[v] = (uint32_t)oracle_quantize(c[v], scale, 32) + zero;
+        }
+        for (v = 0; v < n; v++)
+            for (j = out_idx[v]; j < out_idx[v] + out_deg[v]; j++) {
+                const uint32_t u = out_nb[j];
+                if (kind == 1)
+                    next64[u] += c64[v];
+                else if (kind == 2)
+                    next[u] += scale * (q[v] - zero);
+                else
+                    next[u] += c[v];
+            }
+        for (v = 0; v < n; v++) {
+            float prevPageRank = pageRanks[v];
+            float nextPageRank = kind == 1 ? base_pr + (damp * oracle_fixed64_2d(next64[v]))
+                                           : base_pr + (damp * next[v]);
+            pageRanks[v] = nextPageRank;
+            next[v] = 0;
+            next64[v] = 0;
+            double error = fabs(nextPageRank - prevPageRank);
+            error_total += (error / n);
+            if (error >= epsilon)
+                activeVertices++;
+        }
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (activeVertices == 0)
+            break;
+    }
+    for (v = 0; v < n; v++)
+        pageRanks[v] = pageRanks[v] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(next);
+    free(next64);
+    free(c);
+    free(c64);
+    free(q);
+    return passes;
+}
+
+/* Residual forms with a worklist (pushpull 7, 8), single-thread instance
+ * (vertices in order).  Both start from r = base and the residual
+ * res[v] = ((1 - damp) * damp) * (sum over v's in-edges u with out-edges of
+ * 1.0f / out_degree[u], in stream order), every vertex on the worklist.  Per
+ * iteration each vertex v on the worklist:
+ *   pull_push = 0 (data-driven push, pageRank.c:2971-3127):
+ *     r'[v] = res[v] + r[v];
+ *   pull_push = 1 (data-driven pull-push, pageRank.c:3128-3325):
+ *     r'[v] = base + damp * (sum over v's in-edges of r[u] / out_degree[u],
+ *     stream order, reading ranks already updated in this iteration);
+ *   then error_total += |r'[v] / n - r[v] / n| (binary32, summed in binary64),
+ *   delta = damp * (res[v] / out_degree[v]), and for each out-edge u:
+ *   prev = res[u]; res[u] += delta; if |prev + delta| >= epsilon and
+ *   prev <= epsilon, the iteration counts one activation and puts u on the
+ *   next worklist (the pull-push form adds delta to res[u] a second time
+ *   there, as the reference does); finally res[v] = 0.
+ * Stops after an iteration without activations (iterations = its index) or at
+ * the cap; ranks / n at the end.  hist_active: activations per iteration. */
+uint32_t oracle_pagerank_residual(int pull_push, uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg,
+                                  const uint32_t *in_nb, const uint32_t *out_idx, const uint32_t *out_deg,
+                                  const uint32_t *out_nb, uint32_t iterations, double epsilon, float *ranks_out,
+                                  uint32_t *iterations_out, double *error_total_out, uint32_t *hist_active)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    float *pageRanks = ranks_out;
+    float *res = (float *)calloc(n ? n : 1, sizeof(float));
+    uint8_t *wl_curr = (uint8_t *)calloc(n ? n : 1, 1);
+    uint8_t *wl_next = (uint8_t *)calloc(n ? n : 1, 1);
+    double error_total = 0.0;
+    uint32_t activeVertices = 0, it, passes = 0, v, j;
+    for (v = 0; v < n; v++) {
+        pageRanks[v] = base_pr;
+        res[v] = 0.0f;
+        wl_curr[v] = 1;
+        for (j = in_idx[v]; j < in_idx[v] + in_deg[v]; j++)
+            if (out_deg[in_nb[j]])
+                res[v] += 1.0f / out_deg[in_nb[j]];
+        res[v] = (1.0f - damp) * damp * res[v];
+    }
+    for (it = 0; it < iterations; it++) {
+        uint8_t *t;
+        error_total = 0;
+        activeVertices = 0;
+        for (v = 0; v < n; v++) {
+            if (!wl_curr[v])
+                continue;
+            float oldPageRank = pageRanks[v];
+            float newPageRank;
+            if (pull_push) {
+                float nodeIncomingPR = 0.0f;
+                for (j = in_idx[v]; j < in_idx[v] + in_deg[v]; j++)
+                    nodeIncomingPR += pageRanks[in_nb[j]] / out_deg[in_nb[j]];
+                newPageRank = base_pr + (damp * nodeIncomingPR);
+            } else {
+                newPageRank = res[v] + pageRanks[v];
+            }
+            error_total += fabs(newPageRank / n - oldPageRank / n);
+            pageRanks[v] = newPageRank;
+            float delta = damp * (res[v] / out_deg[v]);
+            for (j = out_idx[v]; j < out_idx[v] + out_deg[v]; j++) {
+                const uint32_t u = out_nb[j];
+                float prevResidual = res[u];
+                res[u] += delta;
+                if ((fabs(prevResidual + delta) >= epsilon) && (prevResidual <= epsilon)) {
+                    activeVertices++;
+                    if (pull_push)
+                        res[u] += delta;
+                    wl_next[u] = 1;
+                }
+            }
+            res[v] = 0.0f;
+        }
+        t = wl_curr;
+        wl_curr = wl_next;
+        wl_next = t;
+        memset(wl_next, 0, n);
+        passes++;
+        if (hist_active)
+            hist_active[it] = activeVertices;
+        if (activeVertices == 0)
+            break;
+    }
+    for (v = 0; v < n; v++)
+        pageRanks[v] = pageRanks[v] / n;
+    if (iterations_out)
+        *iterations_out = it < iterations ? it : iterations;
+    if (error_total_out)
+        *error_total_out = error_total;
+    free(res);
+    free(wl_curr);
+    free(wl_next);
+    return passes;
+}
+
 /* FP64 fixpoint with the reference's constants ((double)0.85f and
  * (double)(1.0f - 0.85f)): every operation in binary64, iterated until
  * max |r' - r| <= tol or max_iter passes.  ranks_out receives r / n. */

@@ -66,7 +66,7 @@ def _load():
         lib.pageRankDataDrivenPullGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
         lib.pageRankPullFixedPoint64BitGraphCSR.restype = C.POINTER(_PageRankStats)
         lib.pageRankPullFixedPoint64BitGraphCSR.argtypes = [C.c_void_p, C.c_void_p]
-        for name in _NARROW.values():
+        for name in list(_NARROW.values()) + list(_PUSH.values()) + list(_RESIDUAL.values()):
             getattr(lib, name).restype = C.POINTER(_PageRankStats)
             getattr(lib, name).argtypes = [C.c_void_p, C.c_void_p]
         lib.freePageRankStats.argtypes = [C.POINTER(_PageRankStats)]
@@ -161,6 +161,60 @@ def pagerank_narrow(quant: bool, width: int, arguments_ptr, graph_ptr, num_verti
     finally:
         lib.freePageRankStats(st)
     return out
+
+
+_PUSH = {0: "pageRankPushGraphCSR", 1: "pageRankPushFixedPointGraphCSR", 2: "pageRankPushQuantGraphCSR"}
+_RESIDUAL = {False: "pageRankDataDrivenPushGraphCSR", True: "pageRankDataDrivenPullPushGraphCSR"}
+
+
+def _single_thread(fn):
+    """Run fn with OpenMP limited to one thread: the push forms' adds (and
+    the residual forms' in-place updates) then happen in vertex order, the
+    instance the oracle restates.  The caller also sets
+    arguments->ker_numThreads = 1 for the loops that take it."""
+    gomp = C.CDLL("libgomp.so.1")
+    prev = gomp.omp_get_max_threads()
+    gomp.omp_set_num_threads(1)
+    try:
+        return fn()
+    finally:
+        gomp.omp_set_num_threads(prev)
+
+
+def _stats_out(lib, st, num_vertices, g0):
+    import numpy as np
+    try:
+        s = st.contents
+        ranks = np.ctypeslib.as_array(s.pageRanks, shape=(num_vertices,)).copy() if num_vertices else \
+            np.zeros(0, np.float32)
+        return {"ranks": ranks, "iterations": int(s.iterations), "error_total": float(s.error_total),
+                "gathers": int(lib.refemu_gathers() - g0)}
+    finally:
+        lib.freePageRankStats(st)
+
+
+def pagerank_push(kind: int, arguments_ptr, graph_ptr, num_vertices: int):
+    """Run one of the reference's push forms on one thread: kind 0
+    pageRankPushGraphCSR (pushpull 1, the emulated push unit), 1
+    pageRankPushFixedPointGraphCSR (pushpull 3), 2 pageRankPushQuantGraphCSR
+    (pushpull 5, stand-in quantiser with zero point 0).  arguments must carry
+    ker_numThreads = 1."""
+    lib = _load()
+    lib.refemu_set_kernel(6)
+    g0 = lib.refemu_gathers()
+    st = _single_thread(lambda: getattr(lib, _PUSH[kind])(C.cast(arguments_ptr, C.c_void_p),
+                                                         C.cast(graph_ptr, C.c_void_p)))
+    return _stats_out(lib, st, num_vertices, g0)
+
+
+def pagerank_residual(pull_push: bool, arguments_ptr, graph_ptr, num_vertices: int):
+    """Run the reference's data-driven push (pushpull 7) or pull-push
+    (pushpull 8) on one thread (arguments must carry ker_numThreads = 1)."""
+    lib = _load()
+    g0 = lib.refemu_gathers()
+    st = _single_thread(lambda: getattr(lib, _RESIDUAL[bool(pull_push)])(C.cast(arguments_ptr, C.c_void_p),
+                                                                        C.cast(graph_ptr, C.c_void_p)))
+    return _stats_out(lib, st, num_vertices, g0)
 
 
 def spmv_pull(arguments_ptr, graph_ptr, num_vertices: int):

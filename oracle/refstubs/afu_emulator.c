@@ -18,7 +18,9 @@
  *     the same sum of 32-, 16- or 8-bit contributions zero-extended into
  *     64 bits (the narrow fixed-point and quantised pulls; the testbench's
  *     Quantized context reads 4 bytes into the 8-byte accumulator,
- *     pagerank_kernel_tb.sv:17-19);
+ *     pagerank_kernel_tb.sv:17-19); for the push CU (pageRank.c:1111-1272)
+ *     the scatter next[u] += c[v] along each forward edge, one source after
+ *     the other in vertex order;
  *     vertices without in-edges are not written.  These are the
  *     compute units' semantics (cu_sum_kernel_control.sv, golden models
  *     pagerank_kernel_tb.sv:303-314, spmv_kernel_tb.sv:304,359).  With no
@@ -45,12 +47,13 @@
 #include "worklist.h"
 
 /* 0: PageRank CU, 1: SpMV CU, 2: 64-bit fixed-point PageRank CU,
- * 3, 4, 5: 32-, 16-, 8-bit contributions into 64-bit sums */
+ * 3, 4, 5: 32-, 16-, 8-bit contributions into 64-bit sums, 6: PageRank push
+ * CU (binary32 adds along the forward edges, one source after the other) */
 static int g_emu_kernel = 0;
 static struct WEDGraphCSR *g_emu_wed = NULL;
 static uint64_t g_emu_runs = 0;
 
-void refemu_set_kernel(int kind) { g_emu_kernel = (kind >= 1 && kind <= 5) ? kind : 0; }
+void refemu_set_kernel(int kind) { g_emu_kernel = (kind >= 1 && kind <= 6) ? kind : 0; }
 uint64_t refemu_gathers(void) { return g_emu_runs; }
 
 void Start(struct Timer *timer) { clock_gettime(CLOCK_MONOTONIC, &timer->start_time); }
@@ -144,6 +147,19 @@ void waitAFU(struct cxl_afu_h **afu, struct AFUStatus *afu_status)
     float *y = (float *)w->auxiliary2;
     const int spmv = g_emu_kernel == 1;
     int64_t v;
+    if (g_emu_kernel == 6) {
+        /* push CU: next[u] += c[v] along every forward edge, sources in order */
+        const uint32_t *fdeg = (const uint32_t *)w->vertex_out_degree;
+        const uint32_t *fidx = (const uint32_t *)w->vertex_edges_idx;
+        const uint32_t *fdst = (const uint32_t *)w->edges_array_dest;
+        for (v = 0; v < (int64_t)n; ++v)
+            for (uint32_t j = fidx[v]; j < fidx[v] + fdeg[v]; ++j)
+                y[fdst[j]] = y[fdst[j]] + x[v];
+        afu_status->cu_return_done = n;
+        afu_status->cu_status = 0;
+        ++g_emu_runs;
+        return;
+    }
     if (g_emu_kernel >= 2) {
         /* integer CU: 64-, 32-, 16- or 8-bit contributions, exact integer sum
          * modulo 2^64 (pagerank_kernel_tb.sv:13-19) */

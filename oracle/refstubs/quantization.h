@@ -1,12 +1,11 @@
 /* stand-in for OpenGraph's quantization.h (absent from the reference
- * checkout): the helpers of the quantised pulls (pageRank.c:2119-2677),
- * restated from the published uniform affine scheme (Jacob et al., CVPR
- * 2018); not pinned.  min and max of the vector in one sequential sweep,
- * scale = (max - min) / (2^W - 1) in binary32, q = round-half-even(x / scale)
- * clamped to [0, 2^W - 1] plus the zero point (which the reference sets to
- * 0); a zero scale quantises everything to the zero point.  The unsuffixed
- * forms are only declared: their users (the push variants) are never linked
- * here. */
+ * checkout): the helpers of the quantised pulls and push
+ * (pageRank.c:2119-2809), restated from the published uniform affine scheme
+ * (Jacob et al., CVPR 2018); not pinned.  min and max of the vector in one
+ * sequential sweep, scale = (max - min) / (2^W - 1) in binary32,
+ * q = round-half-even(x / scale) clamped to [0, 2^W - 1] plus the zero point
+ * (which the pulls set to 0); a zero scale quantises everything to the zero
+ * point. */
 #ifndef REFSTUB_QUANTIZATION_H
 #define REFSTUB_QUANTIZATION_H
 #include <math.h>
@@ -51,7 +50,22 @@ REFSTUB_QUANT_FORMS(32)
 REFSTUB_QUANT_FORMS(16)
 REFSTUB_QUANT_FORMS(8)
 
-void getMinMax(struct quant_params *p, const float *x, uint32_t n);
-float GetScale(float mn, float mx);
-uint32_t quantize(float x, float scale, uint32_t zero);
+/* the unsuffixed forms of the 32-bit push (pageRank.c:2725-2737): the same
+ * as the 32-bit ones; GetZeroPoint's value is restated as 0, the zero point
+ * the quantised pulls use */
+static inline void getMinMax(struct quant_params *p, const float *x, uint32_t n)
+{
+    struct quant_params_32 q;
+    getMinMax_32(&q, x, n);
+    p->min = q.min;
+    p->max = q.max;
+}
+static inline float GetScale(float mn, float mx) { return GetScale_32(mn, mx); }
+static inline uint32_t GetZeroPoint(float mx, float scale)
+{
+    (void)mx;
+    (void)scale;
+    return 0;
+}
+static inline uint32_t quantize(float x, float scale, uint32_t zero) { return quantize_32(x, scale, zero); }
 #endif

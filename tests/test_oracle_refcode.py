@@ -107,3 +107,51 @@ def test_oracle_narrow_equals_reference_code(ag, oracle, refcode, quant, width):
         assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
         assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
         assert ref["gathers"] == mine["passes"], name
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_oracle_push_equals_reference_code(ag, oracle, refcode, kind, capfd):
+    """The push forms (pushpull 1, 3, 5) on one thread: the oracle restatement
+    equals the reference's own host code bit for bit."""
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(80, 1e-6)
+        args.ker_numThreads = 1
+        ref = refcode.pagerank_push(kind, C.byref(args), g.ptr, g.num_vertices)
+        mine = oracle.pagerank_push(kind, g.out_edges_idx(), g.out_degree(), g.out_neighbours(), 80, 1e-6)
+        assert ref["iterations"] == mine["iterations"], name
+        assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
+        assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
+    capfd.readouterr()
+
+
+def test_oracle_push_float_equals_pull(ag, oracle):
+    """One source after the other, each next[u] receives its contributions in
+    increasing source order: the inverse row's stream order.  The sequential
+    push is therefore the pull, bit for bit (and the 64-bit fixed-point push
+    the 64-bit fixed-point pull)."""
+    for name, g in _graphs(ag):
+        push = oracle.pagerank_push(0, g.out_edges_idx(), g.out_degree(), g.out_neighbours(), 100, 1e-7)
+        pull = oracle.pagerank_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(), 100, 1e-7)
+        assert push["iterations"] == pull["iterations"], name
+        assert np.array_equal(push["ranks"].view(np.uint32), pull["ranks"].view(np.uint32)), name
+        pfx = oracle.pagerank_push(1, g.out_edges_idx(), g.out_degree(), g.out_neighbours(), 100, 1e-7)
+        fx = oracle.pagerank_fixed64(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(), 100, 1e-7)
+        assert pfx["iterations"] == fx["iterations"], name
+        assert np.array_equal(pfx["ranks"].view(np.uint32), fx["ranks"].view(np.uint32)), name
+
+
+@pytest.mark.parametrize("pull_push", [False, True])
+def test_oracle_residual_equals_reference_code(ag, oracle, refcode, pull_push, capfd):
+    """The data-driven push (pushpull 7) and pull-push (pushpull 8) on one
+    thread: the oracle restatement equals the reference's own code bit for
+    bit."""
+    for name, g in _graphs(ag):
+        args = ag.default_arguments(100, 1e-6)
+        args.ker_numThreads = 1
+        ref = refcode.pagerank_residual(pull_push, C.byref(args), g.ptr, g.num_vertices)
+        mine = oracle.pagerank_residual(pull_push, g.in_edges_idx(), g.in_degree(), g.in_neighbours(),
+                                        g.out_edges_idx(), g.out_degree(), g.out_neighbours(), 100, 1e-6)
+        assert ref["iterations"] == mine["iterations"], name
+        assert np.array_equal(ref["ranks"].view(np.uint32), mine["ranks"].view(np.uint32)), name
+        assert abs(ref["error_total"] - mine["error_total"]) <= 1e-12 + 1e-9 * abs(mine["error_total"]), name
+    capfd.readouterr()
