@@ -98,7 +98,7 @@ class PROpts(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("precision", C.c_int32), ("order", C.c_int32), ("quiet", C.c_int32),
         ("switch_residual", C.c_double), ("init_ranks", f32p), ("init_on_device", C.c_int32),
-        ("data_driven", C.c_int32),
+        ("data_driven", C.c_int32), ("direction", C.c_int32),
     ]
 
 
@@ -141,6 +141,7 @@ PUSHPULL_OF_PREC = {AG_PREC_FIXED64: 2, AG_PREC_FIXED32: 9, AG_PREC_FIXED16: 10,
 NARROW_FORM = {AG_PREC_FIXED32: (False, 32), AG_PREC_FIXED16: (False, 16), AG_PREC_FIXED8: (False, 8),
                AG_PREC_QUANT32: (True, 32), AG_PREC_QUANT16: (True, 16), AG_PREC_QUANT8: (True, 8)}
 AG_ORDER_FAST, AG_ORDER_EXACT = 0, 1
+AG_DIR_PULL, AG_DIR_PUSH, AG_DIR_PULL_PUSH = 0, 1, 2
 AG_SPMV_GRAPH_WEIGHTS, AG_SPMV_UNIT, AG_SPMV_EXACT = 0, 1, 2
 DAMP = np.float32(0.85)
 BASE_PR = np.float32(np.float32(1.0) - DAMP)
@@ -513,8 +514,8 @@ class DeviceGraph:
         return t, us.value
 
     def launch(self, iterations=20, epsilon=1e-4, precision=AG_PREC_FP32, order=AG_ORDER_FAST,
-               init_ranks=None, switch_residual=1e-4, data_driven=False) -> None:
-        o = make_opts(precision, order, init_ranks, switch_residual, data_driven=data_driven)
+               init_ranks=None, switch_residual=1e-4, data_driven=False, direction=AG_DIR_PULL) -> None:
+        o = make_opts(precision, order, init_ranks, switch_residual, data_driven=data_driven, direction=direction)
         self._keep_init = init_ranks
         check(lib.ag_pagerank_launch(self.h, iterations, epsilon, C.byref(o)), "ag_pagerank_launch")
 
@@ -533,8 +534,8 @@ class DeviceGraph:
         return ranks, res, hist
 
     def pagerank(self, iterations=20, epsilon=1e-4, precision=AG_PREC_FP32, order=AG_ORDER_FAST,
-                 init_ranks=None, switch_residual=1e-4, history=0, data_driven=False):
-        self.launch(iterations, epsilon, precision, order, init_ranks, switch_residual, data_driven)
+                 init_ranks=None, switch_residual=1e-4, history=0, data_driven=False, direction=AG_DIR_PULL):
+        self.launch(iterations, epsilon, precision, order, init_ranks, switch_residual, data_driven, direction)
         return self.fetch(history)
 
     def pagerank_f64(self, max_iterations=1000, tol=1e-13):
@@ -641,12 +642,13 @@ class MultiGraph:
 
 
 def make_opts(precision=AG_PREC_FP32, order=AG_ORDER_FAST, init_ranks=None, switch_residual=1e-4,
-              quiet=True, data_driven=False) -> PROpts:
+              quiet=True, data_driven=False, direction=AG_DIR_PULL) -> PROpts:
     o = PROpts()
     lib.ag_pr_opts_init(C.byref(o))
     o.precision = precision
     o.order = order
     o.data_driven = int(data_driven)
+    o.direction = direction
     o.quiet = int(quiet)
     o.switch_residual = switch_residual
     if init_ranks is not None:

@@ -103,7 +103,16 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
         printf(" -----------------------------------------------------\n");
         printf("| %-51s | \n", "               ---->>> B200 <<<----");
         printf(" -----------------------------------------------------\n");
-        if (o.precision >= AG_PREC_QUANT32 && o.precision <= AG_PREC_QUANT8)
+        if (o.direction == AG_DIR_PULL_PUSH)
+            printf("| %-51s | \n", "Starting Page Rank Pull-Push DD (tolerance/epsilon)");
+        else if (o.direction == AG_DIR_PUSH && o.data_driven)
+            printf("| %-51s | \n", "Starting Page Rank Push DD (tolerance/epsilon)");
+        else if (o.direction == AG_DIR_PUSH && o.precision == AG_PREC_QUANT32)
+            printf("| %-30s %-19s| \n", "Starting Page Rank Push Quant_32", "(tolerance/epsilon)");
+        else if (o.direction == AG_DIR_PUSH)
+            printf("| %-51s | \n", o.precision == AG_PREC_FIXED64 ? "Starting Page Rank Push FP (tolerance/epsilon)"
+                                                                 : "Starting Page Rank Push (tolerance/epsilon)");
+        else if (o.precision >= AG_PREC_QUANT32 && o.precision <= AG_PREC_QUANT8)
             /* the quantised forms' title layout (pageRank.c:2155) */
             printf("| %-30s %-19s| \n",
                    o.precision == AG_PREC_QUANT32   ? "Starting Page Rank Pull Quant_32"
@@ -122,7 +131,8 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
         printf(" -----------------------------------------------------\n");
         printf("| %-10s | %-8s | %-15s | %-9s | \n", "Iteration", "Active", "Error", "Time (S)");
         printf(" -----------------------------------------------------\n");
-        if (o.data_driven) /* every vertex starts on the worklist (pageRank.c:2857-2868) */
+        if (o.data_driven || o.direction == AG_DIR_PULL_PUSH)
+            /* every vertex starts on the worklist (pageRank.c:2857-2868, 3019-3033, 3182-3196) */
             printf("| %-10s | %-8u | %-15.13lf | %-9f | \n", "Init", graph->num_vertices, 0.0, 0.0);
     }
 
@@ -187,10 +197,12 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
     return stats;
 }
 
-/* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 is the pull,
- * 2, 9, 10, 11 the 64/32/16/8-bit fixed-point pulls, 4, 12, 13 the 32/16/8-bit
- * quantised pulls, 6 the data-driven pull; the other codes (the push
- * variants) run the FP32 pull, with a note on stderr */
+/* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 the pull,
+ * 1 the push, 2, 9, 10, 11 the 64/32/16/8-bit fixed-point pulls, 3 the
+ * fixed-point push, 4, 12, 13 the 32/16/8-bit quantised pulls, 5 the
+ * quantised push, 6 the data-driven pull, 7 the data-driven push, 8 the
+ * data-driven pull-push; other codes run the pull, as the reference's default
+ * case does, with a note on stderr */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
 {
     /* pull variants on the GPU: pushpull code, precision form, phase name of
@@ -198,13 +210,22 @@ struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct Graph
     static const struct
     {
         uint32_t pushpull;
-        int32_t precision;
+        int32_t precision, direction, data_driven;
         const char *phase;
     } forms[] = {
-        {2, AG_PREC_FIXED64, "pagerank-pull-fp64"},  {9, AG_PREC_FIXED32, "pagerank-pull-fp32"},
-        {10, AG_PREC_FIXED16, "pagerank-pull-fp16"}, {11, AG_PREC_FIXED8, "pagerank-pull-fp8"},
-        {4, AG_PREC_QUANT32, "pagerank-pull-quant32"}, {12, AG_PREC_QUANT16, "pagerank-pull-quant16"},
-        {13, AG_PREC_QUANT8, "pagerank-pull-quant8"},  {6, AG_PREC_FP32, "pagerank-pull-dd"},
+        {1, AG_PREC_FP32, AG_DIR_PUSH, 0, "pagerank-push"},
+        {2, AG_PREC_FIXED64, AG_DIR_PULL, 0, "pagerank-pull-fp64"},
+        {3, AG_PREC_FIXED64, AG_DIR_PUSH, 0, "pagerank-push-fp64"},
+        {4, AG_PREC_QUANT32, AG_DIR_PULL, 0, "pagerank-pull-quant32"},
+        {5, AG_PREC_QUANT32, AG_DIR_PUSH, 0, "pagerank-push-quant32"},
+        {6, AG_PREC_FP32, AG_DIR_PULL, 1, "pagerank-pull-dd"},
+        {7, AG_PREC_FP32, AG_DIR_PUSH, 1, "pagerank-push-dd"},
+        {8, AG_PREC_FP32, AG_DIR_PULL_PUSH, 1, "pagerank-pull-push-dd"},
+        {9, AG_PREC_FIXED32, AG_DIR_PULL, 0, "pagerank-pull-fp32"},
+        {10, AG_PREC_FIXED16, AG_DIR_PULL, 0, "pagerank-pull-fp16"},
+        {11, AG_PREC_FIXED8, AG_DIR_PULL, 0, "pagerank-pull-fp8"},
+        {12, AG_PREC_QUANT16, AG_DIR_PULL, 0, "pagerank-pull-quant16"},
+        {13, AG_PREC_QUANT8, AG_DIR_PULL, 0, "pagerank-pull-quant8"},
     };
     for (size_t i = 0; arguments && i < sizeof(forms) / sizeof(forms[0]); ++i) {
         if (arguments->pushpull != forms[i].pushpull)
@@ -214,7 +235,8 @@ struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct Graph
         ag_status_t st;
         ag_pr_opts_init(&o);
         o.precision = forms[i].precision;
-        o.data_driven = arguments->pushpull == 6;
+        o.direction = forms[i].direction;
+        o.data_driven = forms[i].data_driven;
         st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
         if (st != AG_OK)
             fail_exit(forms[i].phase, st);

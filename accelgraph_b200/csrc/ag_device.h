@@ -87,6 +87,13 @@
                              are updated; a change is signalled by the sign
                              bit of the contribution written                */
 
+/* push-direction and residual forms (ag_push.cu) */
+#define AG_PUSH_FLOAT 0    /* push, binary32 atomic adds                      */
+#define AG_PUSH_FIXED 1    /* push, 64-bit fixed-point integer adds           */
+#define AG_PUSH_QUANT 2    /* push, 32-bit quantised contributions            */
+#define AG_PUSH_DD 3       /* data-driven push (residuals, worklist)          */
+#define AG_PUSH_PULLPUSH 4 /* data-driven pull-push                           */
+#define AG_NUM_PUSH_FORMS 5
 #define AG_SPMV_W_GRAPH 0 /* multiply by the uploaded weight                */
 #define AG_SPMV_W_CONST 1 /* multiply by 0.0001f (graph without weights)    */
 #define AG_SPMV_W_UNIT 2  /* no multiply                                    */
@@ -181,6 +188,16 @@ typedef struct AgPullParams
     uint32_t *qmm;
     const uint64_t *x64;
     uint64_t *y64;
+    /* push and residual forms (ag_push.cu): the forward edge list sorted by
+     * source (device ids), two vertex vectors (contributions and next sums,
+     * or seed and pull sums), residuals, per-vertex deltas and the two
+     * worklists (2N bytes, one per pass parity) */
+    const uint32_t *fwd_src, *fwd_dst;
+    uint32_t E;
+    uint32_t honor_stop;   /* SpMV launches inside a solve loop: return once
+                              the loop has stopped (stream launches)         */
+    float *pa, *pb, *res, *delta;
+    uint8_t *wl;
     cudaGraphConditionalHandle cond;
 } AgPullParams;
 
@@ -263,6 +280,14 @@ size_t ag_fixed_smem_bytes(int bytes);
  * identity */
 cudaError_t ag_permute_uint_in(const uint32_t *perm, const void *x, void *y, uint32_t n, int bytes, cudaStream_t s);
 cudaError_t ag_permute_u64_out(const uint32_t *inv, const uint64_t *x, uint64_t *y, uint32_t n, cudaStream_t s);
+/* forward edge list from the device inverse CSR: (fwd_src, fwd_dst) sorted by
+ * source, each source's destinations in row order */
+cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t *ids, uint32_t n, uint32_t e,
+                             uint32_t *fwd_src, uint32_t *fwd_dst, cudaStream_t s);
+/* kernels of the push and residual forms (AG_PUSH_*): stage 0 init, 1 scatter
+ * or vertex phase, 2 update or edge phase, 3 quantiser (AG_PUSH_QUANT) or
+ * residual seed (AG_PUSH_DD, AG_PUSH_PULLPUSH) */
+const void *ag_push_kernel_ptr(int kind, int stage);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
 cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
                                      const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,

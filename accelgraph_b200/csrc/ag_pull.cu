@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
 
     /* stream launches (profiling) run a fixed number of kernels: the ones
      * after the loop has ended return at once */
-    if (MODE != AG_MODE_SPMV && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
+    if ((MODE != AG_MODE_SPMV || p.honor_stop) && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
         return;
     AgPass<MODE, PREC, EXACT> ps(p);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

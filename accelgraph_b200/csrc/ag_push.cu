@@ -1,0 +1,537 @@
+/*
+ * ag_push.cu -- push-direction and residual PageRank forms of the
+ * reference's dispatcher (02_capi_graph/src/algorithms/capi/pageRank.c):
+ *   pushpull 1  push, binary32                 :1111-1272
+ *   pushpull 3  push, 64-bit fixed point       :1992-2118
+ *   pushpull 5  push, 32-bit quantised         :2678-2809
+ *   pushpull 7  data-driven push (residuals)   :2971-3127
+ *   pushpull 8  data-driven pull-push          :3128-3325
+ *
+ * The reference runs these on many OpenMP threads (or the FPGA's push unit),
+ * with atomic or unsynchronised adds into the destination: their add order,
+ * and for the residual forms which updates a vertex sees, are not fixed.  The
+ * device forms here are instances of that behaviour:
+ *
+ * Push (1, 3, 5): one thread per forward edge (a source-sorted edge list
+ * built on the device from the relabelled inverse CSR) adds the source's
+ * contribution into next[destination] with an atomic add -- binary32, or
+ * 64-bit integer for the fixed-point form, whose sums are then exact and
+ * identical to the 64-bit fixed-point pull's.  An element-wise kernel then
+ * forms r' = base + damp * next (binary64 for fixed point, as the pull),
+ * the residual, the next contributions and clears next; its last CTA closes
+ * the pass.  The quantised form first replaces every contribution c by
+ * scale * q(c), the value the reference adds per edge (zero point 0).
+ *
+ * Residual forms (7, 8): a vertex phase takes each worklist vertex's
+ * residual (atomic exchange with 0, so that no concurrent add is lost),
+ * forms its new rank (7: r + residual; 8: base + damp * the pull over its
+ * in-edges of the contributions at the start of the pass -- the interleaving
+ * of the reference's loop in which every read precedes every write), adds
+ * |r'/n - r/n| to the pass's error and stores delta = damp * (residual /
+ * out_degree); an edge phase, one thread per forward edge of a worklist
+ * source, adds delta to the destination's residual (atomic, returning the
+ * previous value) and, when the residual crosses epsilon (|prev + delta| >=
+ * epsilon and prev <= epsilon), counts an activation and puts the
+ * destination on the next worklist (8 adds delta a second time, as the
+ * reference does).  The edge phase's last CTA closes the pass; the loop
+ * stops after a pass without activations.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cub/cub.cuh>
+
+#include "ag_device.h"
+#include "ag_mem.h"
+
+#define AG_PNW (AG_SBLK / 32)
+
+/* 64-bit fixed point of the fixed-point forms: 32 fractional bits */
+#define AG_PUSH_FX_ONE 4294967296.0
+
+__device__ __forceinline__ uint64_t ag_push_d2fixed(double x)
+{
+    return (uint64_t)__double2ll_rz(__dmul_rn(x, AG_PUSH_FX_ONE));
+}
+
+__device__ __forceinline__ double ag_push_fixed2d(uint64_t x)
+{
+    return __ddiv_rn(__ll2double_rn((long long)x), AG_PUSH_FX_ONE);
+}
+
+/* order-preserving keys of binary32 values and the 32-bit quantiser (the
+ * same definitions as the quantised pulls) */
+__device__ __forceinline__ uint32_t ag_push_fkey(float f)
+{
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float ag_push_fkey_value(uint32_t k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+__device__ __forceinline__ float ag_push_quant_scale(const uint32_t *mm, uint32_t slot)
+{
+    const uint32_t kmin = mm[slot], kmax = mm[2 + slot];
+    if (kmin > kmax)
+        return 0.0f;
+    return __fdiv_rn(__fsub_rn(ag_push_fkey_value(kmax), ag_push_fkey_value(kmin)), (float)0xFFFFFFFFull);
+}
+
+__device__ __forceinline__ uint32_t ag_push_quantize(float x, float scale)
+{
+    if (!(scale > 0.0f))
+        return 0u;
+    const float q = rintf(__fdiv_rn(x, scale));
+    if (!(q > 0.0f))
+        return 0u;
+    if (q >= (float)0xFFFFFFFFull)
+        return 0xFFFFFFFFu;
+    return (uint32_t)q;
+}
+
+__device__ __forceinline__ double ag_push_warp_sum_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ag_push_warp_sum_u(uint32_t v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+/* the CTA's sum of one double per thread, valid in thread 0 */
+__device__ double ag_push_block_sum_d(double v)
+{
+    __shared__ double s_v[AG_PNW];
+    v = ag_push_warp_sum_d(v);
+    if ((threadIdx.x & 31) == 0)
+        s_v[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < AG_PNW; ++w)
+            t += s_v[w];
+    return t;
+}
+
+/* Close a pass: every thread of the CTA calls this after its last element
+ * with its share of the pass's error and activity (and, for the quantised
+ * push, the min/max keys of the next contributions).  The CTA's totals go to
+ * the control block; the last CTA to arrive records the pass, clears the
+ * quantised form's slot of this pass, decides whether another pass runs and
+ * sets the loop condition.  err_per_n: the error total is the sum divided by
+ * N (the plain and push forms) rather than the sum itself (residual forms). */
+__device__ void ag_push_close_pass(const AgPullParams &p, double err, uint32_t active, bool quant, uint32_t mn,
+                                   uint32_t mx, bool err_per_n)
+{
+    __shared__ double s_e[AG_PNW];
+    __shared__ uint32_t s_a[AG_PNW], s_mn[AG_PNW], s_mx[AG_PNW];
+    __shared__ uint32_t s_last;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    err = ag_push_warp_sum_d(err);
+    active = ag_push_warp_sum_u(active);
+    if (quant) {
+        mn = __reduce_min_sync(0xffffffffu, mn);
+        mx = __reduce_max_sync(0xffffffffu, mx);
+    }
+    if (lane == 0) {
+        s_e[warp] = err;
+        s_a[warp] = active;
+        s_mn[warp] = mn;
+        s_mx[warp] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double be = 0.0;
+        uint32_t ba = 0, bmn = 0xFFFFFFFFu, bmx = 0u;
+        for (int w = 0; w < AG_PNW; ++w) {
+            be += s_e[w];
+            ba += s_a[w];
+            bmn = min(bmn, s_mn[w]);
+            bmx = max(bmx, s_mx[w]);
+        }
+        if (be != 0.0)
+            atomicAdd(&p.ctl->err_acc, be);
+        if (ba)
+            atomicAdd(&p.ctl->active_acc, ba);
+        if (quant) {
+            const uint32_t nslot = (p.ctl->iter + 1u) & 1u;
+            if (bmn != 0xFFFFFFFFu)
+                atomicMin(&p.qmm[nslot], bmn);
+            if (bmx)
+                atomicMax(&p.qmm[2 + nslot], bmx);
+        }
+        __threadfence();
+        const uint32_t ticket = atomicAdd(&p.ctl->done_ctas, 1u);
+        s_last = (ticket == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        AgControl *c = p.ctl;
+        volatile AgControl *vc = c;
+        const uint32_t P = vc->iter;
+        const uint32_t act = vc->active_acc;
+        const double e = err_per_n ? vc->err_acc / (double)p.N : vc->err_acc;
+        if (P < AG_MAX_HISTORY) {
+            c->hist_active[P] = act;
+            c->hist_err[P] = e;
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            c->hist_t[P] = t;
+        }
+        if (quant) {
+            p.qmm[P & 1u] = 0xFFFFFFFFu;
+            p.qmm[2 + (P & 1u)] = 0u;
+        }
+        const bool conv = act == 0;
+        c->prev_err = e;
+        c->last_err_sum = vc->err_acc;
+        c->iter = P + 1;
+        c->converged = conv ? 1u : 0u;
+        const bool cont = !conv && (P + 1 < vc->max_iter);
+        c->active_acc = 0;
+        c->err_acc = 0.0;
+        c->done_ctas = 0;
+        c->stop = cont ? 0u : 1u;
+        __threadfence();
+        if (p.use_cond)
+            cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
+    }
+}
+
+__device__ __forceinline__ bool ag_push_stopped(const AgPullParams &p)
+{
+    return !p.use_cond && *((volatile uint32_t *)&p.ctl->stop);
+}
+
+/* ---------------------------------------------------------------- init */
+__device__ void ag_push_reset_control(const AgPullParams &p, const AgRunConfig &run)
+{
+    AgControl *c = p.ctl;
+    c->iter = 0;
+    c->max_iter = run.max_iter;
+    c->active_acc = 0;
+    c->done_ctas = 0;
+    c->err_acc = 0.0;
+    c->eps = run.eps;
+    c->converged = 0;
+    c->mode_read = 0;
+    c->mode_write = 0;
+    c->switch_pass = 0;
+    c->switch_residual = run.switch_residual;
+    c->prev_err = 1e300;
+    c->rank_sum = 0.0;
+    c->use_init = run.use_init;
+    c->low_passes = 0;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    c->t0 = t;
+    c->stop = (run.max_iter > 0 && p.N > 0) ? 0u : 1u;
+    if (p.use_cond)
+        cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
+}
+
+/* push forms: r = base (or the warm start), next = 0, first contributions
+ * (quantised: binary32 and their min/max keys in slot 0, which the graph
+ * clears first) */
+template <int KIND>
+__global__ void __launch_bounds__(AG_SBLK) ag_push_init_kernel(const AgPullParams p, const AgRunConfig run)
+{
+    __shared__ uint32_t s_mn[AG_PNW], s_mx[AG_PNW];
+    uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
+        p.rank[v] = r0;
+        const uint32_t od = p.outdeg[v];
+        if (KIND == AG_PUSH_FIXED) {
+            p.c64_0[v] = od ? ag_push_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
+            p.c64_1[v] = 0ull;
+        } else {
+            const float c = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
+            p.pa[v] = c;
+            p.pb[v] = 0.0f;
+            if (KIND == AG_PUSH_QUANT) {
+                const uint32_t k = ag_push_fkey(c);
+                mn = min(mn, k);
+                mx = max(mx, k);
+            }
+        }
+    }
+    if (KIND == AG_PUSH_QUANT) {
+        mn = __reduce_min_sync(0xffffffffu, mn);
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if ((threadIdx.x & 31) == 0) {
+            s_mn[threadIdx.x >> 5] = mn;
+            s_mx[threadIdx.x >> 5] = mx;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < AG_PNW; ++w) {
+                mn = min(mn, s_mn[w]);
+                mx = max(mx, s_mx[w]);
+            }
+            if (mn != 0xFFFFFFFFu)
+                atomicMin(&p.qmm[0], mn);
+            if (mx)
+                atomicMax(&p.qmm[2], mx);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ag_push_reset_control(p, run);
+}
+
+/* residual forms: x[v] = 1 / out_degree[v] (0 without out-edges), the
+ * vector whose stream-order in-row sums give the first residuals; the sums'
+ * vector starts at 0 */
+__global__ void __launch_bounds__(AG_SBLK) ag_residual_seed_kernel(const AgPullParams p)
+{
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        const uint32_t od = p.outdeg[v];
+        p.pa[v] = od ? __fdiv_rn(1.0f, __uint2float_rn(od)) : 0.0f;
+        p.pb[v] = 0.0f;
+    }
+}
+
+/* residual forms: res = ((1 - damp) * damp) * sum, r = base (or the warm
+ * start), every vertex on the first worklist, contributions r / out_degree
+ * for the pull-push form's first pull, control reset */
+__global__ void __launch_bounds__(AG_SBLK) ag_residual_init_kernel(const AgPullParams p, const AgRunConfig run)
+{
+    const float k = __fmul_rn(p.base, p.damp);
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        p.res[v] = __fmul_rn(k, p.pb[v]);
+        const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
+        p.rank[v] = r0;
+        const uint32_t od = p.outdeg[v];
+        p.pa[v] = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
+        p.wl[v] = 1;
+        p.wl[p.N + v] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ag_push_reset_control(p, run);
+}
+
+/* ---------------------------------------------------------------- push */
+/* quantised push: every contribution becomes scale * q(c), the value the
+ * reference adds along each of the source's edges */
+__global__ void __launch_bounds__(AG_SBLK) ag_push_quant_kernel(const AgPullParams p)
+{
+    if (ag_push_stopped(p))
+        return;
+    const float scale = ag_push_quant_scale(p.qmm, p.ctl->iter & 1u);
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK)
+        p.pa[v] = __fmul_rn(scale, __uint2float_rn(ag_push_quantize(p.pa[v], scale)));
+}
+
+/* one thread per forward edge: next[dst] += c[src] */
+template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_scatter_kernel(const AgPullParams p)
+{
+    if (ag_push_stopped(p))
+        return;
+    const uint64_t pol_first = ag_policy_evict_first();
+    const uint32_t stride = gridDim.x * AG_SBLK;
+    for (uint32_t j = blockIdx.x * AG_SBLK + threadIdx.x; j < p.E; j += stride) {
+        const uint32_t v = ag_ld_stream_u32(p.fwd_src + j, pol_first);
+        const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
+        if (KIND == AG_PUSH_FIXED)
+            atomicAdd((unsigned long long *)p.c64_1 + u, (unsigned long long)p.c64_0[v]);
+        else
+            atomicAdd(p.pb + u, p.pa[v]);
+    }
+}
+
+/* element-wise update of the push forms; the last CTA closes the pass */
+template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_update_kernel(const AgPullParams p)
+{
+    if (ag_push_stopped(p))
+        return;
+    const double eps = p.ctl->eps;
+    double my_err = 0.0;
+    uint32_t my_active = 0, mn = 0xFFFFFFFFu, mx = 0u;
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        float rn;
+        if (KIND == AG_PUSH_FIXED) {
+            const uint64_t s = p.c64_1[v];
+            p.c64_1[v] = 0ull;
+            rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_push_fixed2d(s))));
+        } else {
+            const float s = p.pb[v];
+            p.pb[v] = 0.0f;
+            rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
+        }
+        const float rp = p.rank[v];
+        const double err = (double)fabsf(__fsub_rn(rn, rp));
+        my_err += err;
+        my_active += (err >= eps) ? 1u : 0u;
+        p.rank[v] = rn;
+        const uint32_t od = p.outdeg[v];
+        if (KIND == AG_PUSH_FIXED) {
+            p.c64_0[v] = od ? ag_push_d2fixed((double)__fdiv_rn(rn, __uint2float_rn(od))) : 0ull;
+        } else {
+            const float c = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
+            p.pa[v] = c;
+            if (KIND == AG_PUSH_QUANT) {
+                const uint32_t k = ag_push_fkey(c);
+                mn = min(mn, k);
+                mx = max(mx, k);
+            }
+        }
+    }
+    ag_push_close_pass(p, my_err, my_active, KIND == AG_PUSH_QUANT, mn, mx, true);
+}
+
+/* ------------------------------------------------------------ residual */
+/* vertex phase: worklist vertices take their residual, form the new rank,
+ * add to the pass's error and store their delta; the previous pass's
+ * worklist (the buffer the edge phase fills next) is cleared */
+template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_vertex_kernel(const AgPullParams p)
+{
+    if (ag_push_stopped(p))
+        return;
+    const uint32_t pass = p.ctl->iter;
+    const uint8_t *wl_cur = p.wl + (size_t)(pass & 1u) * p.N;
+    uint8_t *wl_old = p.wl + (size_t)((pass + 1u) & 1u) * p.N;
+    const float fN = __uint2float_rn(p.N);
+    double my_err = 0.0;
+    for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
+        wl_old[v] = 0;
+        if (!wl_cur[v])
+            continue;
+        const float old = p.rank[v];
+        const float res = atomicExch(p.res + v, 0.0f);
+        /* pull-push: the pull over v's in-edges of the start-of-pass
+         * contributions (pb, from the pass's first kernel) */
+        const float rn = PULLPUSH ? __fadd_rn(p.base, __fmul_rn(p.damp, p.pb[v])) : __fadd_rn(res, old);
+        my_err += (double)fabsf(__fsub_rn(__fdiv_rn(rn, fN), __fdiv_rn(old, fN)));
+        p.rank[v] = rn;
+        const uint32_t od = p.outdeg[v];
+        /* without out-edges the delta is never read */
+        p.delta[v] = od ? __fmul_rn(p.damp, __fdiv_rn(res, __uint2float_rn(od))) : 0.0f;
+        if (PULLPUSH)
+            p.pa[v] = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
+    }
+    /* the error joins the pass's record (one atomic per CTA); the edge phase
+     * closes the pass */
+    const double e = ag_push_block_sum_d(my_err);
+    if (threadIdx.x == 0 && e != 0.0)
+        atomicAdd(&p.ctl->err_acc, e);
+}
+
+/* edge phase: one thread per forward edge of a worklist source */
+template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_edge_kernel(const AgPullParams p)
+{
+    if (ag_push_stopped(p))
+        return;
+    const uint32_t pass = p.ctl->iter;
+    const uint8_t *wl_cur = p.wl + (size_t)(pass & 1u) * p.N;
+    uint8_t *wl_next = p.wl + (size_t)((pass + 1u) & 1u) * p.N;
+    const double eps = p.ctl->eps;
+    const uint64_t pol_first = ag_policy_evict_first();
+    uint32_t my_act = 0;
+    const uint32_t stride = gridDim.x * AG_SBLK;
+    for (uint32_t j = blockIdx.x * AG_SBLK + threadIdx.x; j < p.E; j += stride) {
+        const uint32_t v = ag_ld_stream_u32(p.fwd_src + j, pol_first);
+        if (!wl_cur[v])
+            continue;
+        const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
+        const float dl = p.delta[v];
+        const float prev = atomicAdd(p.res + u, dl);
+        if ((double)fabsf(__fadd_rn(prev, dl)) >= eps && (double)prev <= eps) {
+            ++my_act;
+            if (PULLPUSH)
+                atomicAdd(p.res + u, dl);
+            wl_next[u] = 1;
+        }
+    }
+    ag_push_close_pass(p, 0.0, my_act, false, 0xFFFFFFFFu, 0u, false);
+}
+
+/* --------------------------------------------------- forward edge list */
+/* rows[j] = the row holding in-edge j (binary search of the row starts) */
+__global__ void ag_edge_rows_kernel(const uint32_t *row_off, uint32_t n, uint32_t e, uint32_t *rows)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < e; j += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n; /* row_off[lo] <= j < row_off[hi] */
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(row_off + mid) <= j)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        rows[j] = lo;
+    }
+}
+
+extern "C" cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t *ids, uint32_t n, uint32_t e,
+                                        uint32_t *fwd_src, uint32_t *fwd_dst, cudaStream_t s)
+{
+    if (e == 0)
+        return cudaSuccess;
+    uint32_t *rows = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < (uint64_t)n)
+        ++bits;
+    cudaError_t err = cudaMallocAsync((void **)&rows, (size_t)e * 4, s);
+    if (err != cudaSuccess)
+        return err;
+    unsigned blocks = (e + 255) / 256;
+    if (blocks > 148 * 32)
+        blocks = 148 * 32;
+    ag_edge_rows_kernel<<<blocks, 256, 0, s>>>(row_off, n, e, rows);
+    err = cudaGetLastError();
+    /* stable by source: each source's destinations stay in row order */
+    if (err == cudaSuccess)
+        err = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, ids, fwd_src, rows, fwd_dst, (int)e, 0, bits, s);
+    if (err == cudaSuccess)
+        err = cudaMallocAsync(&tmp, tmp_bytes, s);
+    if (err == cudaSuccess)
+        err = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, ids, fwd_src, rows, fwd_dst, (int)e, 0, bits, s);
+    if (tmp)
+        cudaFreeAsync(tmp, s);
+    cudaFreeAsync(rows, s);
+    return err;
+}
+
+extern "C" const void *ag_push_kernel_ptr(int kind, int stage)
+{
+    /* stage 0 init, 1 scatter / vertex phase, 2 update / edge phase,
+     * 3 quantiser (kind 2) or seed (kinds 3, 4) */
+    switch (kind) {
+    case AG_PUSH_FLOAT:
+        return stage == 0   ? (const void *)ag_push_init_kernel<AG_PUSH_FLOAT>
+               : stage == 1 ? (const void *)ag_push_scatter_kernel<AG_PUSH_FLOAT>
+                            : (const void *)ag_push_update_kernel<AG_PUSH_FLOAT>;
+    case AG_PUSH_FIXED:
+        return stage == 0   ? (const void *)ag_push_init_kernel<AG_PUSH_FIXED>
+               : stage == 1 ? (const void *)ag_push_scatter_kernel<AG_PUSH_FIXED>
+                            : (const void *)ag_push_update_kernel<AG_PUSH_FIXED>;
+    case AG_PUSH_QUANT:
+        return stage == 0   ? (const void *)ag_push_init_kernel<AG_PUSH_QUANT>
+               : stage == 1 ? (const void *)ag_push_scatter_kernel<AG_PUSH_QUANT>
+               : stage == 2 ? (const void *)ag_push_update_kernel<AG_PUSH_QUANT>
+                            : (const void *)ag_push_quant_kernel;
+    case AG_PUSH_DD:
+        return stage == 0   ? (const void *)ag_residual_init_kernel
+               : stage == 1 ? (const void *)ag_residual_vertex_kernel<false>
+               : stage == 2 ? (const void *)ag_residual_edge_kernel<false>
+                            : (const void *)ag_residual_seed_kernel;
+    default:
+        return stage == 0   ? (const void *)ag_residual_init_kernel
+               : stage == 1 ? (const void *)ag_residual_vertex_kernel<true>
+               : stage == 2 ? (const void *)ag_residual_edge_kernel<true>
+                            : (const void *)ag_residual_seed_kernel;
+    }
+}

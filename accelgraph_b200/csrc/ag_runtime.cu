@@ -357,6 +357,13 @@ struct ag_graph_s
     uint32_t *qmm;
     AgExec exe_int[AG_NUM_INT_FORMS];
     int have_exe_int[AG_NUM_INT_FORMS];
+    /* push and residual forms: forward edge list sorted by source, vertex
+     * vectors, residuals, deltas, the two worklists, one launch graph per form */
+    uint32_t *fwd_src, *fwd_dst;
+    float *pa, *pb, *res, *delta;
+    uint8_t *wl;
+    AgExec exe_push[AG_NUM_PUSH_FORMS];
+    int have_exe_push[AG_NUM_PUSH_FORMS];
     int have_exe_dd[2];
     cudaEvent_t ev0, ev1;
     int launched;
@@ -416,6 +423,11 @@ static void drop_execs(ag_graph_s *g)
             free_exec(&g->exe_int[b]);
             g->have_exe_int[b] = 0;
         }
+    for (int b = 0; b < AG_NUM_PUSH_FORMS; ++b)
+        if (g->have_exe_push[b]) {
+            free_exec(&g->exe_push[b]);
+            g->have_exe_push[b] = 0;
+        }
 }
 
 extern "C" ag_status_t ag_graph_release(ag_graph_t g)
@@ -430,6 +442,13 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->hub_part64);
     dev_free(g->cqf);
     dev_free(g->qmm);
+    dev_free(g->fwd_src);
+    dev_free(g->fwd_dst);
+    dev_free(g->pa);
+    dev_free(g->pb);
+    dev_free(g->res);
+    dev_free(g->delta);
+    dev_free(g->wl);
     dev_free(g->row_off);
     dev_free(g->ids);
     dev_free(g->perm);
@@ -937,6 +956,14 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.hub_part64 = g->hub_part64;
     p.cqf = g->cqf;
     p.qmm = g->qmm;
+    p.fwd_src = g->fwd_src;
+    p.fwd_dst = g->fwd_dst;
+    p.E = g->E;
+    p.pa = g->pa;
+    p.pb = g->pb;
+    p.res = g->res;
+    p.delta = g->delta;
+    p.wl = g->wl;
     p.base = 1.0f - Damp; /* pageRank.c:57-58: base_pr = 1.0f - damp */
     p.damp = Damp;
     return p;
@@ -1110,6 +1137,282 @@ static ag_status_t ensure_fixed(ag_graph_s *g, int quant = 0)
     return AG_OK;
 }
 
+/* push and residual forms: the forward edge list (built once from the
+ * device inverse CSR) and the vectors each form needs, made on first use */
+static ag_status_t ensure_push(ag_graph_s *g, int kind)
+{
+    ag_status_t st = AG_OK;
+    if (kind == AG_PUSH_FIXED || kind == AG_PUSH_QUANT) {
+        st = ensure_fixed(g, kind == AG_PUSH_QUANT);
+        if (st != AG_OK)
+            return st;
+    }
+    if (!g->fwd_src) {
+        g->fwd_src = (uint32_t *)dev_alloc(g, (size_t)g->E * 4 + 16, &st);
+        g->fwd_dst = (uint32_t *)dev_alloc(g, (size_t)g->E * 4 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        AG_CUDA(ag_forward_build(g->row_off, g->ids, g->N, g->E, g->fwd_src, g->fwd_dst, g_ctx.stream));
+        drop_execs(g);
+    }
+    if (!g->pa) {
+        g->pa = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        g->pb = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        drop_execs(g);
+    }
+    if ((kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH) && !g->res) {
+        g->res = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        g->delta = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        g->wl = (uint8_t *)dev_alloc(g, (size_t)g->N * 2 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        drop_execs(g);
+    }
+    return AG_OK;
+}
+
+/* parameters of an SpMV launch inside a push-family solve: y = pb, the unit
+ * row sums of x = pa (EXACT: stream order) */
+static AgPullParams push_spmv_params(ag_graph_s *g, int exact)
+{
+    AgPullParams q = base_params(g, exact);
+    q.x = g->pa;
+    q.rank = g->pb;
+    q.wmode = AG_SPMV_W_UNIT;
+    q.honor_stop = 1;
+    return q;
+}
+
+static size_t push_spmv_smem(const AgPullParams &q) { return (size_t)AG_STAGE_BYTES + (size_t)q.hot_n * 4; }
+
+static dim3 push_edge_grid(const ag_graph_s *g)
+{
+    return dim3((unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)g->E + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 32)));
+}
+
+/* The push form's graph: [qmm clears] init, WHILE { [quantiser] scatter,
+ * update }, normalise; the residual forms: seed, stream-order SpMV (first
+ * residuals), init, WHILE { [SpMV of the contributions] vertex phase, edge
+ * phase }, normalise. */
+static ag_status_t build_exec_push(ag_graph_s *g, int kind)
+{
+    AgExec *x = &g->exe_push[kind];
+    memset(x, 0, sizeof(*x));
+    AG_CUDA(cudaGraphCreate(&x->graph, 0));
+    AG_CUDA(cudaGraphConditionalHandleCreate(&x->cond, x->graph, 1, cudaGraphCondAssignDefault));
+    x->params = base_params(g, 0);
+    x->params.cond = x->cond;
+    x->params.use_cond = 1;
+    const bool residual = kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH;
+    const dim3 eg = elem_grid(g), blk(AG_SBLK), edge_grid = push_edge_grid(g);
+    void *pargs[1] = {&x->params};
+
+    cudaGraphNode_t prev[2];
+    int nprev = 0;
+    if (kind == AG_PUSH_QUANT) {
+        cudaMemsetParams ms = {};
+        ms.dst = g->qmm;
+        ms.elementSize = 4;
+        ms.width = 2;
+        ms.height = 1;
+        ms.value = 0xFFFFFFFFu;
+        AG_CUDA(cudaGraphAddMemsetNode(&prev[nprev++], x->graph, nullptr, 0, &ms));
+        ms.dst = g->qmm + 2;
+        ms.value = 0u;
+        AG_CUDA(cudaGraphAddMemsetNode(&prev[nprev++], x->graph, nullptr, 0, &ms));
+    }
+    AgPullParams seed_spmv = push_spmv_params(g, 1), loop_spmv = push_spmv_params(g, 0);
+    seed_spmv.honor_stop = 0;
+    if (residual) {
+        cudaKernelNodeParams ks = {};
+        ks.func = (void *)ag_push_kernel_ptr(kind, 3);
+        ks.gridDim = eg;
+        ks.blockDim = blk;
+        ks.kernelParams = pargs;
+        cudaGraphNode_t nseed, nspmv;
+        AG_CUDA(cudaGraphAddKernelNode(&nseed, x->graph, nullptr, 0, &ks));
+        void *sargs[1] = {&seed_spmv};
+        const void *ksp = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 1);
+        const size_t ssm = push_spmv_smem(seed_spmv);
+        if (seed_spmv.ntasks) {
+            cudaKernelNodeParams kv = {};
+            kv.func = (void *)ksp;
+            kv.gridDim = dim3(pull_grid(ksp, seed_spmv.ntasks, ssm));
+            kv.blockDim = dim3(AG_BLK);
+            kv.sharedMemBytes = (unsigned)ssm;
+            kv.kernelParams = sargs;
+            AG_CUDA(cudaGraphAddKernelNode(&nspmv, x->graph, &nseed, 1, &kv));
+            prev[nprev++] = nspmv;
+        } else {
+            prev[nprev++] = nseed;
+        }
+    }
+    AgRunConfig run;
+    memset(&run, 0, sizeof(run));
+    void *init_args[2] = {&x->params, &run};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *)ag_push_kernel_ptr(kind, 0);
+    kp.gridDim = eg;
+    kp.blockDim = blk;
+    kp.kernelParams = init_args;
+    AG_CUDA(cudaGraphAddKernelNode(&x->init_node, x->graph, nprev ? prev : nullptr, (size_t)nprev, &kp));
+
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = x->cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    AG_CUDA(cudaGraphAddNode(&wnode, x->graph, &x->init_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+    cudaGraphNode_t last = nullptr;
+    auto add = [&](const void *func, dim3 grid, dim3 block, size_t smem, void **args) -> cudaError_t {
+        cudaKernelNodeParams kn = {};
+        kn.func = (void *)func;
+        kn.gridDim = grid;
+        kn.blockDim = block;
+        kn.sharedMemBytes = (unsigned)smem;
+        kn.kernelParams = args;
+        cudaGraphNode_t n;
+        cudaError_t e = cudaGraphAddKernelNode(&n, body, last ? &last : nullptr, last ? 1 : 0, &kn);
+        if (e == cudaSuccess)
+            last = n;
+        return e;
+    };
+    void *largs[1] = {&loop_spmv};
+    if (kind == AG_PUSH_QUANT)
+        AG_CUDA(add(ag_push_kernel_ptr(kind, 3), eg, blk, 0, pargs));
+    if (kind == AG_PUSH_PULLPUSH && loop_spmv.ntasks) {
+        const void *ksp = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 0);
+        const size_t lsm = push_spmv_smem(loop_spmv);
+        AG_CUDA(add(ksp, dim3(pull_grid(ksp, loop_spmv.ntasks, lsm)), dim3(AG_BLK), lsm, largs));
+    }
+    AG_CUDA(add(ag_push_kernel_ptr(kind, 1), residual ? eg : edge_grid, blk, 0, pargs));
+    AG_CUDA(add(ag_push_kernel_ptr(kind, 2), residual ? edge_grid : eg, blk, 0, pargs));
+
+    void *norm_args[1] = {&x->params};
+    cudaKernelNodeParams kn = {};
+    kn.func = (void *)ag_normalize_kernel_ptr();
+    kn.gridDim = eg;
+    kn.blockDim = blk;
+    kn.kernelParams = norm_args;
+    cudaGraphNode_t nnode;
+    AG_CUDA(cudaGraphAddKernelNode(&nnode, x->graph, &wnode, 1, &kn));
+    AG_CUDA(cudaGraphInstantiate(&x->exec, x->graph, 0));
+    g->have_exe_push[kind] = 1;
+    return AG_OK;
+}
+
+/* the same kernels as separate launches (profiling form; passes after the
+ * loop stops return at once) */
+static ag_status_t push_stream_launch(ag_graph_s *g, int kind, const AgRunConfig &run)
+{
+    cudaStream_t s = g_ctx.stream;
+    AgPullParams sp = base_params(g, 0);
+    sp.use_cond = 0;
+    const bool residual = kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH;
+    const dim3 eg = elem_grid(g), blk(AG_SBLK), edge_grid = push_edge_grid(g);
+    void *pa[1] = {&sp};
+    AgRunConfig r = run;
+    void *ia[2] = {&sp, &r};
+    AgPullParams seed_spmv = push_spmv_params(g, 1), loop_spmv = push_spmv_params(g, 0);
+    seed_spmv.honor_stop = 0;
+    void *sa[1] = {&seed_spmv}, *la[1] = {&loop_spmv};
+    const void *kse = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 1), *ksl = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 0);
+    if (kind == AG_PUSH_QUANT) {
+        AG_CUDA(cudaMemsetAsync(g->qmm, 0xFF, 8, s));
+        AG_CUDA(cudaMemsetAsync(g->qmm + 2, 0, 8, s));
+    }
+    if (residual) {
+        AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 3), eg, blk, pa, 0, s));
+        if (seed_spmv.ntasks)
+            AG_CUDA(cudaLaunchKernel(kse, dim3(pull_grid(kse, seed_spmv.ntasks, push_spmv_smem(seed_spmv))),
+                                     dim3(AG_BLK), sa, push_spmv_smem(seed_spmv), s));
+    }
+    AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 0), eg, blk, ia, 0, s));
+    for (uint32_t i = 0; i < run.max_iter; ++i) {
+        if (kind == AG_PUSH_QUANT)
+            AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 3), eg, blk, pa, 0, s));
+        if (kind == AG_PUSH_PULLPUSH && loop_spmv.ntasks)
+            AG_CUDA(cudaLaunchKernel(ksl, dim3(pull_grid(ksl, loop_spmv.ntasks, push_spmv_smem(loop_spmv))),
+                                     dim3(AG_BLK), la, push_spmv_smem(loop_spmv), s));
+        AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 1), residual ? eg : edge_grid, blk, pa, 0, s));
+        AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 2), residual ? edge_grid : eg, blk, pa, 0, s));
+    }
+    AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), eg, blk, pa, 0, s));
+    return AG_OK;
+}
+
+/* push-direction and residual solves (ag_pr_opts.direction != AG_DIR_PULL) */
+static ag_status_t push_launch(ag_graph_s *g, const ag_pr_opts &o, uint32_t max_iterations, double epsilon)
+{
+    int kind;
+    if (o.direction == AG_DIR_PULL_PUSH)
+        kind = AG_PUSH_PULLPUSH;
+    else if (o.data_driven)
+        kind = AG_PUSH_DD;
+    else if (o.precision == AG_PREC_FP32)
+        kind = AG_PUSH_FLOAT;
+    else if (o.precision == AG_PREC_FIXED64)
+        kind = AG_PUSH_FIXED;
+    else if (o.precision == AG_PREC_QUANT32)
+        kind = AG_PUSH_QUANT;
+    else
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the push runs in FP32, 64-bit fixed point or 32-bit quantised");
+    if ((kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH) && o.precision != AG_PREC_FP32)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the data-driven push and pull-push run in FP32");
+    if (g->ngraphs || g->norm_n || g->c_base)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "the push forms run on a whole graph");
+    ag_status_t st = ensure_push(g, kind);
+    if (st != AG_OK)
+        return st;
+    if (o.init_ranks && !g->init_buf) {
+        g->init_buf = (float *)dev_alloc(g, (size_t)g->N * 4 + 16, &st);
+        if (st != AG_OK)
+            return st;
+        drop_execs(g);
+    }
+    if (!g->have_exe_push[kind]) {
+        st = build_exec_push(g, kind);
+        if (st != AG_OK)
+            return st;
+    }
+    AgExec *x = &g->exe_push[kind];
+    cudaStream_t s = g_ctx.stream;
+    if (o.init_ranks && g->N)
+        AG_CUDA(cudaMemcpyAsync(g->init_buf, o.init_ranks, (size_t)g->N * 4,
+                                o.init_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    AgRunConfig run;
+    memset(&run, 0, sizeof(run));
+    run.max_iter = std::min<uint32_t>(max_iterations, AG_MAX_HISTORY);
+    run.use_init = o.init_ranks ? 1u : 0u;
+    run.eps = epsilon;
+    run.switch_residual = 1e-4;
+    void *init_args[2] = {&x->params, &run};
+    cudaKernelNodeParams kp;
+    AG_CUDA(cudaGraphKernelNodeGetParams(x->init_node, &kp));
+    kp.kernelParams = init_args;
+    AG_CUDA(cudaGraphExecKernelNodeSetParams(x->exec, x->init_node, &kp));
+    AG_CUDA(cudaEventRecord(g->ev0, s));
+    const char *mode = getenv("AG_LAUNCH_MODE");
+    if (mode && strcmp(mode, "stream") == 0) {
+        st = push_stream_launch(g, kind, run);
+        if (st != AG_OK)
+            return st;
+    } else {
+        AG_CUDA(cudaGraphLaunch(x->exec, s));
+    }
+    AG_CUDA(cudaEventRecord(g->ev1, s));
+    g->launched = 1;
+    g->last_prec = o.precision;
+    g->last_exact = 0;
+    return AG_OK;
+}
+
 extern "C" void ag_pr_opts_init(ag_pr_opts *o)
 {
     if (!o)
@@ -1133,6 +1436,10 @@ extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations,
         memcpy(&o, opts, std::min<size_t>(sizeof(o), opts->struct_size ? opts->struct_size : sizeof(o)));
     if (o.precision < 0 || o.precision > AG_PREC_QUANT8)
         return ag_set_error(AG_ERR_INVALID_ARG, "unknown precision %d", o.precision);
+    if (o.direction < AG_DIR_PULL || o.direction > AG_DIR_PULL_PUSH)
+        return ag_set_error(AG_ERR_INVALID_ARG, "unknown direction %d", o.direction);
+    if (o.direction != AG_DIR_PULL)
+        return push_launch(g, o, max_iterations, epsilon);
     if (g->ngraphs && (o.precision != AG_PREC_FP32 || o.init_ranks || o.data_driven))
         return ag_set_error(AG_ERR_UNSUPPORTED, "a graph union runs the FP32 form without a warm start");
     const int dd = o.data_driven ? 1 : 0;

@@ -226,6 +226,15 @@ ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, dou
 #define AG_PREC_QUANT16 8
 #define AG_PREC_QUANT8  9
 
+/* Direction of a solve.  The push and residual forms (pageRank.c:1111-1272,
+ * 1992-2118, 2678-2809, 2971-3325) add along forward edges with atomic adds,
+ * as the reference's threads do: their binary32 sums are not in a fixed order
+ * (the 64-bit fixed-point push is exact and equals the fixed-point pull), and
+ * the residual forms' worklists depend on the interleaving. */
+#define AG_DIR_PULL      0
+#define AG_DIR_PUSH      1
+#define AG_DIR_PULL_PUSH 2
+
 #define AG_ORDER_FAST  0 /* rows of <= 32 in-edges summed in stream order,
                             longer rows by a fixed lane-strided tree         */
 #define AG_ORDER_EXACT 1 /* every row summed in stream order: bit-identical
@@ -250,6 +259,11 @@ typedef struct ag_pr_opts
                                   a rank is replaced only when it moves by at
                                   least epsilon, which activates its
                                   out-neighbours; FP32, one graph              */
+    int32_t direction;         /* AG_DIR_*: AG_DIR_PUSH runs the push forms
+                                  (pushpull 1, 3, 5 with precision FP32,
+                                  FIXED64, QUANT32; with data_driven the
+                                  data-driven push, pushpull 7), AG_DIR_PULL_PUSH
+                                  the data-driven pull-push (pushpull 8)      */
 } ag_pr_opts;
 
 typedef struct ag_pr_result

@@ -1,0 +1,148 @@
+"""Push-direction and residual PageRank forms on the GPU: the reference's push
+(pushpull 1, pageRank.c:1111-1272), 64-bit fixed-point push (3, :1992-2118),
+32-bit quantised push (5, :2678-2809), data-driven push (7, :2971-3127) and
+data-driven pull-push (8, :3128-3325).
+
+The device adds along forward edges with atomic adds, as the reference's
+threads do, so only the integer form has a fixed result: the fixed-point push
+equals the oracle (its single-thread instance, itself equal to the 64-bit
+fixed-point pull) bit for bit.  The binary32 forms are held to the oracle by
+tolerance: ranks within 1e-5 relative L1, iteration counts within a tenth (at
+least 3).  The residual forms, whose worklists depend on the interleaving, are
+held to the FP64 fixpoint: their error is within ten times the oracle
+instance's (at least 2e-5 relative L1), and they converge within three times
+the oracle's iterations."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+
+def _push_ref(oracle, g, kind, iterations, eps):
+    return oracle.pagerank_push(kind, g.out_edges_idx(), g.out_degree(), g.out_neighbours(), iterations, eps)
+
+
+def _residual_ref(oracle, g, pull_push, iterations, eps):
+    return oracle.pagerank_residual(pull_push, g.in_edges_idx(), g.in_degree(), g.in_neighbours(),
+                                    g.out_edges_idx(), g.out_degree(), g.out_neighbours(), iterations, eps)
+
+
+def _graphs(ag):
+    yield "rmat12_ef16", ag.Graph.rmat(12, 16, seed=61)
+    yield "er4099_d6", ag.Graph.er(4099, 6, seed=2)
+    src = np.array([0, 0, 1, 2, 2, 3, 5, 5, 5, 7, 8, 8], np.uint32)
+    dst = np.array([1, 2, 2, 0, 3, 3, 1, 2, 4, 7, 9, 0], np.uint32)
+    yield "small_mixed", ag.Graph.from_edges(11, src, dst)
+    yield "no_edges", ag.Graph.from_edges(7, np.zeros(0, np.uint32), np.zeros(0, np.uint32))
+
+
+@pytest.mark.parametrize("launch", ["graph", "stream"])
+def test_fixed_push_matches_oracle_bits(gpu, oracle, launch, monkeypatch):
+    ag = gpu
+    if launch == "stream":
+        monkeypatch.setenv("AG_LAUNCH_MODE", "stream")
+    for name, g in _graphs(ag):
+        ref = _push_ref(oracle, g, oracle.PUSH_FIXED64, 200, 1e-6)
+        r, res, hist = ag.DeviceGraph(g).pagerank(200, 1e-6, precision=ag.AG_PREC_FIXED64,
+                                                  direction=ag.AG_DIR_PUSH, history=200)
+        assert res.iterations == ref["iterations"], name
+        assert np.array_equal(hist["active"], ref["active"]), name
+        assert np.array_equal(r.view(np.uint32), ref["ranks"].view(np.uint32)), name
+
+
+@pytest.mark.parametrize("prec,kind", [(0, 0), (7, 2)])
+def test_float_push_matches_oracle(gpu, oracle, prec, kind):
+    ag = gpu
+    for name, g in _graphs(ag):
+        ref = _push_ref(oracle, g, kind, 300, 1e-6)
+        r, res, _ = ag.DeviceGraph(g).pagerank(300, 1e-6, precision=prec, direction=ag.AG_DIR_PUSH)
+        assert abs(res.iterations - ref["iterations"]) <= max(3, ref["iterations"] // 10), name
+        assert _rel(r, ref["ranks"]) <= 1e-5, name
+
+
+@pytest.mark.parametrize("pull_push", [False, True])
+def test_residual_forms_converge_to_fixpoint(gpu, oracle, pull_push):
+    ag = gpu
+    for name, g in _graphs(ag):
+        ref = _residual_ref(oracle, g, pull_push, 400, 1e-6)
+        dg = ag.DeviceGraph(g)
+        f64, _ = dg.pagerank_f64(5000, 1e-13)
+        direction = ag.AG_DIR_PULL_PUSH if pull_push else ag.AG_DIR_PUSH
+        r, res, hist = dg.pagerank(400, 1e-6, data_driven=True, direction=direction, history=400)
+        assert res.converged, name
+        assert res.iterations <= 3 * ref["iterations"] + 10, name
+        assert _rel(r, f64) <= max(10 * _rel(ref["ranks"], f64), 2e-5), name
+        assert hist["active"][-1] == 0 and (len(hist["active"]) == 1 or hist["active"][0] > 0), name
+
+
+def test_residual_stream_launch(gpu, oracle, monkeypatch):
+    """The profiling launch (separate kernels, passes after the stop returning
+    at once) solves to the same tolerance."""
+    ag = gpu
+    g = ag.Graph.rmat(11, 8, seed=9)
+    dg = ag.DeviceGraph(g)
+    f64, _ = dg.pagerank_f64(5000, 1e-13)
+    monkeypatch.setenv("AG_LAUNCH_MODE", "stream")
+    for direction in (ag.AG_DIR_PUSH, ag.AG_DIR_PULL_PUSH):
+        ref = _residual_ref(oracle, g, direction == ag.AG_DIR_PULL_PUSH, 400, 1e-6)
+        r, res, _ = dg.pagerank(400, 1e-6, data_driven=True, direction=direction)
+        assert res.converged
+        assert _rel(r, f64) <= max(10 * _rel(ref["ranks"], f64), 2e-5)
+
+
+@pytest.mark.parametrize("pushpull", [1, 3, 5, 7, 8])
+def test_push_dispatch(gpu, oracle, pushpull, capfd):
+    """pageRankGraphCSR with the reference's push codes runs the form and
+    prints its title."""
+    ag = gpu
+    g = ag.Graph.rmat(12, 8, seed=78)
+    args = ag.default_arguments(300, 1e-6)
+    args.pushpull = pushpull
+    st = ag.lib.pageRankGraphCSR(C.byref(args), g.ptr)
+    ranks = ag.stats_ranks(st)
+    iters = st.contents.iterations
+    ag.lib.freePageRankStats(st)
+    out = capfd.readouterr().out
+    title = {1: "Starting Page Rank Push (tolerance/epsilon)", 3: "Starting Page Rank Push FP (tolerance/epsilon)",
+             5: "Starting Page Rank Push Quant_32", 7: "Starting Page Rank Push DD (tolerance/epsilon)",
+             8: "Starting Page Rank Pull-Push DD (tolerance/epsilon)"}[pushpull]
+    assert title in out
+    if pushpull == 3:
+        ref = _push_ref(oracle, g, oracle.PUSH_FIXED64, 300, 1e-6)
+        assert iters == ref["iterations"] and np.array_equal(ranks.view(np.uint32), ref["ranks"].view(np.uint32))
+    elif pushpull in (1, 5):
+        ref = _push_ref(oracle, g, 0 if pushpull == 1 else 2, 300, 1e-6)
+        assert _rel(ranks, ref["ranks"]) <= 1e-5
+    else:
+        ref = _residual_ref(oracle, g, pushpull == 8, 300, 1e-6)
+        assert _rel(ranks, ref["ranks"]) <= 1e-4
+    assert abs(float(np.sum(ranks, dtype=np.float64)) - float(np.sum(ref["ranks"], dtype=np.float64))) < 1e-3
+
+
+def test_push_forms_reject_unsupported(gpu):
+    """Narrow precisions have no push form in the reference, and a row
+    partition holds only its rows: both are refused with AG_ERR_UNSUPPORTED."""
+    ag = gpu
+    g = ag.Graph.rmat(10, 8, seed=1)
+    dg = ag.DeviceGraph(g)
+    o = ag.make_opts(ag.AG_PREC_QUANT16, direction=ag.AG_DIR_PUSH)
+    assert ag.lib.ag_pagerank_launch(dg.h, 10, 1e-4, C.byref(o)) == ag.AG_ERR_UNSUPPORTED
+    from accelgraph_b200.distributed import partition_bounds
+    bounds, slice_ = partition_bounds(g.in_degree(), 2)
+    h = C.c_void_p()
+    ag.check(ag.lib.ag_graph_upload_rows(g.ptr, bounds.ctypes.data_as(C.POINTER(C.c_uint32)), 2, 0, slice_, 0,
+                                         C.byref(h)), "ag_graph_upload_rows")
+    try:
+        for direction in (ag.AG_DIR_PUSH, ag.AG_DIR_PULL_PUSH):
+            o = ag.make_opts(direction=direction, data_driven=True)
+            assert ag.lib.ag_pagerank_launch(h, 10, 1e-4, C.byref(o)) == ag.AG_ERR_UNSUPPORTED
+    finally:
+        ag.lib.ag_graph_release(h)
