@@ -14,13 +14,18 @@
  *
  * Push (1, 3, 5): one thread per forward edge (a source-sorted edge list
  * built on the device from the relabelled inverse CSR) adds the source's
- * contribution into next[destination] with an atomic add -- binary32, or
- * 64-bit integer for the fixed-point form, whose sums are then exact and
- * identical to the 64-bit fixed-point pull's.  An element-wise kernel then
- * forms r' = base + damp * next (binary64 for fixed point, as the pull),
- * the residual, the next contributions and clears next; its last CTA closes
- * the pass.  The quantised form first replaces every contribution c by
- * scale * q(c), the value the reference adds per edge (zero point 0).
+ * contribution into next[destination] with an atomic add.  The fixed-point
+ * form adds 64-bit integers, whose sums are exact and identical to the 64-bit
+ * fixed-point pull's.  The binary32 forms add into a binary64 accumulator,
+ * rounded once to binary32 by the update: atomic binary32 adds land in a new
+ * order every pass, and a rank whose ulp exceeds epsilon (un-normalised hub
+ * ranks) would then change by an ulp every pass and never pass the residual
+ * test, whereas the binary64 sum's order moves only bits that the rounding
+ * drops.  An element-wise kernel then forms r' = base + damp * next (binary64
+ * for fixed point, as the pull), the residual, the next contributions and
+ * clears next; its last CTA closes the pass.  The quantised form first
+ * replaces every contribution c by scale * q(c), the value the reference adds
+ * per edge (zero point 0).
  *
  * Residual forms (7, 8): a vertex phase takes each worklist vertex's
  * residual (atomic exchange with 0, so that no concurrent add is lost),
@@ -33,8 +38,10 @@
  * previous value) and, when the residual crosses epsilon (|prev + delta| >=
  * epsilon and prev <= epsilon), counts an activation and puts the
  * destination on the next worklist (8 adds delta a second time, as the
- * reference does).  The edge phase's last CTA closes the pass; the loop
- * stops after a pass without activations.
+ * reference does).  A self-edge adds nothing: the reference sets the
+ * residual to 0 after the vertex's own adds, so only its crossing test, made
+ * on the residual the vertex phase took, remains.  The edge phase's last CTA
+ * closes the pass; the loop stops after a pass without activations.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -253,13 +260,12 @@ __global__ void __launch_bounds__(AG_SBLK) ag_push_init_kernel(const AgPullParam
         const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
         p.rank[v] = r0;
         const uint32_t od = p.outdeg[v];
+        p.c64_1[v] = 0ull; /* the next sums: 64-bit integer or binary64 zero */
         if (KIND == AG_PUSH_FIXED) {
             p.c64_0[v] = od ? ag_push_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
-            p.c64_1[v] = 0ull;
         } else {
             const float c = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
             p.pa[v] = c;
-            p.pb[v] = 0.0f;
             if (KIND == AG_PUSH_QUANT) {
                 const uint32_t k = ag_push_fkey(c);
                 mn = min(mn, k);
@@ -333,7 +339,8 @@ __global__ void __launch_bounds__(AG_SBLK) ag_push_quant_kernel(const AgPullPara
         p.pa[v] = __fmul_rn(scale, __uint2float_rn(ag_push_quantize(p.pa[v], scale)));
 }
 
-/* one thread per forward edge: next[dst] += c[src] */
+/* one thread per forward edge: next[dst] += c[src] (64-bit integer, or
+ * binary64 for the binary32 forms) */
 template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_scatter_kernel(const AgPullParams p)
 {
     if (ag_push_stopped(p))
@@ -346,7 +353,7 @@ template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_scatter_k
         if (KIND == AG_PUSH_FIXED)
             atomicAdd((unsigned long long *)p.c64_1 + u, (unsigned long long)p.c64_0[v]);
         else
-            atomicAdd(p.pb + u, p.pa[v]);
+            atomicAdd(reinterpret_cast<double *>(p.c64_1) + u, (double)p.pa[v]);
     }
 }
 
@@ -365,8 +372,9 @@ template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_update_ke
             p.c64_1[v] = 0ull;
             rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_push_fixed2d(s))));
         } else {
-            const float s = p.pb[v];
-            p.pb[v] = 0.0f;
+            double *nd = reinterpret_cast<double *>(p.c64_1);
+            const float s = __double2float_rn(nd[v]);
+            nd[v] = 0.0;
             rn = __fadd_rn(p.base, __fmul_rn(p.damp, s));
         }
         const float rp = p.rank[v];
@@ -392,8 +400,9 @@ template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_update_ke
 
 /* ------------------------------------------------------------ residual */
 /* vertex phase: worklist vertices take their residual, form the new rank,
- * add to the pass's error and store their delta; the previous pass's
- * worklist (the buffer the edge phase fills next) is cleared */
+ * add to the pass's error and store their delta and the residual taken (pb,
+ * for the crossing test of a self-edge); the previous pass's worklist (the
+ * buffer the edge phase fills next) is cleared */
 template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_vertex_kernel(const AgPullParams p)
 {
     if (ag_push_stopped(p))
@@ -414,6 +423,7 @@ template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_
         const float rn = PULLPUSH ? __fadd_rn(p.base, __fmul_rn(p.damp, p.pb[v])) : __fadd_rn(res, old);
         my_err += (double)fabsf(__fsub_rn(__fdiv_rn(rn, fN), __fdiv_rn(old, fN)));
         p.rank[v] = rn;
+        p.pb[v] = res;
         const uint32_t od = p.outdeg[v];
         /* without out-edges the delta is never read */
         p.delta[v] = od ? __fmul_rn(p.damp, __fdiv_rn(res, __uint2float_rn(od))) : 0.0f;
@@ -445,10 +455,10 @@ template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_
             continue;
         const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
         const float dl = p.delta[v];
-        const float prev = atomicAdd(p.res + u, dl);
+        const float prev = u == v ? p.pb[v] : atomicAdd(p.res + u, dl);
         if ((double)fabsf(__fadd_rn(prev, dl)) >= eps && (double)prev <= eps) {
             ++my_act;
-            if (PULLPUSH)
+            if (PULLPUSH && u != v)
                 atomicAdd(p.res + u, dl);
             wl_next[u] = 1;
         }

@@ -1142,7 +1142,8 @@ static ag_status_t ensure_fixed(ag_graph_s *g, int quant = 0)
 static ag_status_t ensure_push(ag_graph_s *g, int kind)
 {
     ag_status_t st = AG_OK;
-    if (kind == AG_PUSH_FIXED || kind == AG_PUSH_QUANT) {
+    if (kind == AG_PUSH_FLOAT || kind == AG_PUSH_FIXED || kind == AG_PUSH_QUANT) {
+        /* 64-bit next sums (and the quantised form's min/max slots) */
         st = ensure_fixed(g, kind == AG_PUSH_QUANT);
         if (st != AG_OK)
             return st;

@@ -228,9 +228,10 @@ ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, dou
 
 /* Direction of a solve.  The push and residual forms (pageRank.c:1111-1272,
  * 1992-2118, 2678-2809, 2971-3325) add along forward edges with atomic adds,
- * as the reference's threads do: their binary32 sums are not in a fixed order
- * (the 64-bit fixed-point push is exact and equals the fixed-point pull), and
- * the residual forms' worklists depend on the interleaving. */
+ * as the reference's threads do.  The 64-bit fixed-point push is exact and
+ * equals the fixed-point pull; the binary32 pushes sum in binary64 (rounded
+ * once to binary32), so they differ from a sequential binary32 sum in the
+ * last bits; the residual forms' worklists depend on the interleaving. */
 #define AG_DIR_PULL      0
 #define AG_DIR_PUSH      1
 #define AG_DIR_PULL_PUSH 2
