@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--workload", default="pagerank",
                    choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe",
-                            "data-driven", "fixed-point"],
+                            "data-driven", "fixed-point", "push"],
                    help="pagerank: the headline line (driver contract); the others measure the other forms")
     p.add_argument("--graphs", type=int, default=256, help="multigraph: number of graphs")
     p.add_argument("--train-graphs", type=int, default=200, help="warmstart: training graphs")
@@ -601,6 +601,59 @@ def run_fixed_point(a):
     print(json.dumps(out), flush=True)
 
 
+def run_push(a):
+    """The reference's push and residual forms against the FP32 pull on the
+    same graph: push (pushpull 1), 64-bit fixed-point push (3), 32-bit
+    quantised push (5), data-driven push (7) and pull-push (8).  Per form: time
+    to epsilon on the device (or to the iteration cap), passes, time per pass,
+    accuracy against the FP64 fixpoint, and the single-thread CPU oracle of
+    the same form timed on a bounded sample of its iterations."""
+    import time
+    import oracle
+    ag = _gpu_setup()
+    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
+    N, E = g.num_vertices, g.num_edges
+    dg = ag.DeviceGraph(g)
+    r64, _ = dg.pagerank_f64(5000, 1e-13)
+    out = {"workload": f"push-direction and residual PageRank to eps {a.epsilon:g}, RMAT s{a.scale} ef{a.edge_factor}",
+           "N": N, "E": E, "bytes_per_pass": "push: 8E (edge list) + 4E of gathered contributions (mostly "
+           "repeats of one source) + N(12..28); residual: 4E + 8E for worklist sources"}
+    forms = (("pull_fp32", dict()), ("push_fp32", dict(direction=ag.AG_DIR_PUSH)),
+             ("push_fixed64", dict(direction=ag.AG_DIR_PUSH, precision=ag.AG_PREC_FIXED64)),
+             ("push_quant32", dict(direction=ag.AG_DIR_PUSH, precision=ag.AG_PREC_QUANT32)),
+             ("push_dd", dict(direction=ag.AG_DIR_PUSH, data_driven=True)),
+             ("pull_push_dd", dict(direction=ag.AG_DIR_PULL_PUSH, data_driven=True)))
+    t_build = time.perf_counter()
+    dg.pagerank(1, a.epsilon, direction=ag.AG_DIR_PUSH)  # builds the forward edge list once
+    out["forward_list_build_s"] = time.perf_counter() - t_build
+    for name, kw in forms:
+        dg.pagerank(a.iterations, a.epsilon, **kw)
+        best = None
+        for _ in range(max(1, a.steps)):
+            r, res, _ = dg.pagerank(a.iterations, a.epsilon, **kw)
+            if best is None or res.device_ms < best[1].device_ms:
+                best = (r, res)
+        r, res = best
+        rl, mx = _rel(r, r64)
+        out[name] = {"device_ms_to_eps": res.device_ms, "passes": res.passes, "iterations": res.iterations,
+                     "converged": res.converged, "pass_us": res.device_ms * 1e3 / max(res.passes, 1),
+                     "rel_l1_vs_fp64": rl, "max_abs_vs_fp64": mx}
+        if name != "pull_fp32":
+            out[name]["time_vs_pull"] = out["pull_fp32"]["device_ms_to_eps"] / res.device_ms
+    sample = 3
+    for name, fn in (("push_fp32", lambda: oracle.pagerank_push(0, g.out_edges_idx(), g.out_degree(),
+                                                                 g.out_neighbours(), sample, a.epsilon)),
+                     ("push_dd", lambda: oracle.pagerank_residual(False, g.in_edges_idx(), g.in_degree(),
+                                                                  g.in_neighbours(), g.out_edges_idx(),
+                                                                  g.out_degree(), g.out_neighbours(), sample,
+                                                                  a.epsilon))):
+        t0 = time.perf_counter()
+        fn()
+        out[name]["cpu_oracle"] = {"seconds_per_iteration": (time.perf_counter() - t0) / sample, "threads": 1,
+                                   "sample": f"first {sample} iterations"}
+    print(json.dumps(out), flush=True)
+
+
 def run_rows(a):
     """One graph split by rows over all ranks (NCCL all-gather per pass);
     strong scaling: the whole job solves one graph."""
@@ -665,7 +718,7 @@ def main():
     else:
         {"spmv": run_spmv, "precision": run_precision, "ppr": run_ppr, "multigraph": run_multigraph,
          "warmstart": run_warmstart, "gather-probe": run_gather_probe,
-         "data-driven": run_data_driven, "fixed-point": run_fixed_point}[a.workload](a)
+         "data-driven": run_data_driven, "fixed-point": run_fixed_point, "push": run_push}[a.workload](a)
 
 
 if __name__ == "__main__":
