@@ -567,30 +567,51 @@ __global__ void __launch_bounds__(AG_SBLK) ag_int_init_kernel(const AgPullParams
 }
 
 /* quantise the binary32 contributions with the scale of this pass's min/max
- * slot: four per thread, one 4-, 8- or 16-byte store */
+ * slot.  One wave of CTAs; each thread takes groups of four contributions,
+ * AG_QK groups a round, and issues all of a round's 16-byte loads before it
+ * needs the scale, so that the loads are in flight together; each group is
+ * stored with one 4-, 8- or 16-byte store. */
+#define AG_QK 4
 template <typename T> __global__ void __launch_bounds__(AG_SBLK) ag_quant_kernel(const AgPullParams p)
 {
     if (!p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
         return;
-    const float scale = ag_quant_scale<T>(p.qmm, p.ctl->iter & 1u);
     T *q = reinterpret_cast<T *>(p.c64_0);
     const uint32_t n4 = p.N >> 2;
     const uint32_t stride = gridDim.x * AG_SBLK;
-    for (uint32_t i = blockIdx.x * AG_SBLK + threadIdx.x; i < n4; i += stride) {
-        const float4 f = __ldg(reinterpret_cast<const float4 *>(p.cqf) + i);
-        const T a = ag_quantize<T>(f.x, scale), b = ag_quantize<T>(f.y, scale);
-        const T c = ag_quantize<T>(f.z, scale), d = ag_quantize<T>(f.w, scale);
-        if constexpr (sizeof(T) == 4)
-            reinterpret_cast<uint4 *>(q)[i] = make_uint4(a, b, c, d);
-        else if constexpr (sizeof(T) == 2)
-            reinterpret_cast<uint2 *>(q)[i] = make_uint2((uint32_t)a | ((uint32_t)b << 16), (uint32_t)c | ((uint32_t)d << 16));
-        else
-            reinterpret_cast<uint32_t *>(q)[i] =
-                (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)c << 16) | ((uint32_t)d << 24);
+    const float4 *src = reinterpret_cast<const float4 *>(p.cqf);
+    bool have_scale = false;
+    float scale = 0.0f;
+    for (uint32_t i0 = blockIdx.x * AG_SBLK + threadIdx.x; i0 < n4; i0 += AG_QK * stride) {
+        float4 f[AG_QK];
+#pragma unroll
+        for (int k = 0; k < AG_QK; ++k)
+            if (i0 + k * stride < n4)
+                f[k] = __ldg(src + i0 + k * stride);
+        if (!have_scale) {
+            scale = ag_quant_scale<T>(p.qmm, p.ctl->iter & 1u);
+            have_scale = true;
+        }
+#pragma unroll
+        for (int k = 0; k < AG_QK; ++k) {
+            const uint32_t i = i0 + k * stride;
+            if (i >= n4)
+                break;
+            const T a = ag_quantize<T>(f[k].x, scale), b = ag_quantize<T>(f[k].y, scale);
+            const T c = ag_quantize<T>(f[k].z, scale), d = ag_quantize<T>(f[k].w, scale);
+            if constexpr (sizeof(T) == 4)
+                reinterpret_cast<uint4 *>(q)[i] = make_uint4(a, b, c, d);
+            else if constexpr (sizeof(T) == 2)
+                reinterpret_cast<uint2 *>(q)[i] =
+                    make_uint2((uint32_t)a | ((uint32_t)b << 16), (uint32_t)c | ((uint32_t)d << 16));
+            else
+                reinterpret_cast<uint32_t *>(q)[i] =
+                    (uint32_t)a | ((uint32_t)b << 8) | ((uint32_t)c << 16) | ((uint32_t)d << 24);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x < (p.N & 3u)) {
         const uint32_t v = (n4 << 2) + threadIdx.x;
-        q[v] = ag_quantize<T>(p.cqf[v], scale);
+        q[v] = ag_quantize<T>(p.cqf[v], ag_quant_scale<T>(p.qmm, p.ctl->iter & 1u));
     }
 }
 

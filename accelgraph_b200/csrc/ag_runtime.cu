@@ -992,13 +992,13 @@ static dim3 elem_grid(const ag_graph_s *g)
         1, std::min<uint64_t>(((uint64_t)g->N + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8)));
 }
 
-/* the quantiser: one group of four contributions per thread, so that every
- * load is in flight at once (its divisions are long dependent chains) */
+/* the quantiser: one wave of CTAs (each thread issues several groups' loads
+ * at once) */
 static dim3 quant_grid(const ag_graph_s *g)
 {
     const uint64_t groups = ((uint64_t)g->N + 3) / 4;
     return dim3((unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((groups + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 64)));
+        1, std::min<uint64_t>((groups + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 8)));
 }
 
 /* prec: AG_PREC_* (the integer forms take both orders through one graph) */
