@@ -46,80 +46,11 @@
 #include <type_traits>
 
 #include "ag_device.h"
+#include "ag_intpass.h"
 #include "ag_mem.h"
 
-#define AG_FX_ONE 4294967296.0 /* 2^32: 64-bit fixed-point unit */
 #define AG_INT_FIXED 0
 #define AG_INT_QUANT 1
-
-__device__ __forceinline__ uint64_t ag_d2fixed(double x)
-{
-    return (uint64_t)__double2ll_rz(__dmul_rn(x, AG_FX_ONE));
-}
-
-__device__ __forceinline__ double ag_fixed2d(uint64_t x)
-{
-    return __ddiv_rn(__ll2double_rn((long long)x), AG_FX_ONE);
-}
-
-/* W-bit fixed point, W/2 fractional bits: the exact binary32 product
- * truncated toward zero, kept modulo 2^W; back: the 64-bit sum rounded once
- * to binary32, scaled by 2^-(W/2) (exact) */
-template <typename T> __device__ __forceinline__ T ag_to_fixed(float x)
-{
-    constexpr float one = (float)(1u << (4 * sizeof(T)));
-    return (T)(unsigned long long)__float2ll_rz(__fmul_rn(x, one));
-}
-
-template <typename T> __device__ __forceinline__ float ag_from_fixed(uint64_t s)
-{
-    constexpr float one = (float)(1u << (4 * sizeof(T)));
-    return __fdiv_rn(__ull2float_rn(s), one);
-}
-
-/* order-preserving 32-bit keys of binary32 values (for atomic min/max) */
-__device__ __forceinline__ uint32_t ag_fkey(float f)
-{
-    const uint32_t b = __float_as_uint(f);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-__device__ __forceinline__ float ag_fkey_value(uint32_t k)
-{
-    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
-}
-
-/* scale of the contributions whose min/max keys are in slot `slot`
- * (mm[0..1] minimum keys, mm[2..3] maximum keys); 0 for an empty slot */
-template <typename T> __device__ __forceinline__ float ag_quant_scale(const uint32_t *mm, uint32_t slot)
-{
-    constexpr float levels = (float)((1ull << (8 * sizeof(T))) - 1ull);
-    const uint32_t kmin = mm[slot], kmax = mm[2 + slot];
-    if (kmin > kmax)
-        return 0.0f;
-    return __fdiv_rn(__fsub_rn(ag_fkey_value(kmax), ag_fkey_value(kmin)), levels);
-}
-
-template <typename T> __device__ __forceinline__ T ag_quantize(float x, float scale)
-{
-    constexpr unsigned long long top = (1ull << (8 * sizeof(T))) - 1ull;
-    if (!(scale > 0.0f))
-        return (T)0;
-    const float q = rintf(__fdiv_rn(x, scale));
-    if (!(q > 0.0f))
-        return (T)0;
-    if (q >= (float)top)
-        return (T)top;
-    return (T)(unsigned long long)q;
-}
-
-__device__ __forceinline__ uint64_t ag_warp_sum_u64(uint64_t v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 /* one warp's stage: a row item's AG_WCAP in-edges start anywhere in their
  * first 16-byte quad, so they span up to AG_WCAP + 3 slots */
@@ -151,10 +82,6 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
     constexpr uint32_t HOT = AG_FX_HOT_BYTES / sizeof(T);
     /* staged values: one element each, so 32 bits hold the narrow ones */
     using S = typename std::conditional<sizeof(T) == 8, uint64_t, uint32_t>::type;
-    __shared__ double s_redd[AG_WARPS];
-    __shared__ uint32_t s_redu[AG_WARPS];
-    __shared__ uint32_t s_mn[AG_WARPS], s_mx[AG_WARPS];
-    __shared__ uint32_t s_last;
     if (!GATHER && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
         return;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -414,85 +341,7 @@ __global__ void __launch_bounds__(AG_BLK, 1) ag_int_kernel(const AgPullParams p)
     /* close the pass: CTA totals (and the quantised forms' min/max keys of
      * the next contributions), then the last CTA records the pass and sets
      * the loop condition */
-    {
-        double e = my_err;
-        uint32_t a = my_active;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            e += __shfl_xor_sync(0xffffffffu, e, o);
-            a += __shfl_xor_sync(0xffffffffu, a, o);
-        }
-        if (QUANT) {
-            my_mn = __reduce_min_sync(0xffffffffu, my_mn);
-            my_mx = __reduce_max_sync(0xffffffffu, my_mx);
-        }
-        if (lane == 0) {
-            s_redd[warp] = e;
-            s_redu[warp] = a;
-            s_mn[warp] = my_mn;
-            s_mx[warp] = my_mx;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double be = 0.0;
-            uint32_t ba = 0, bmn = 0xFFFFFFFFu, bmx = 0u;
-            for (int w = 0; w < AG_WARPS; ++w) {
-                be += s_redd[w];
-                ba += s_redu[w];
-                bmn = min(bmn, s_mn[w]);
-                bmx = max(bmx, s_mx[w]);
-            }
-            if (be != 0.0)
-                atomicAdd(&p.ctl->err_acc, be);
-            if (ba)
-                atomicAdd(&p.ctl->active_acc, ba);
-            if (QUANT) {
-                const uint32_t nslot = (pass + 1u) & 1u;
-                if (bmn != 0xFFFFFFFFu)
-                    atomicMin(&p.qmm[nslot], bmn);
-                if (bmx)
-                    atomicMax(&p.qmm[2 + nslot], bmx);
-            }
-            __threadfence();
-            const uint32_t ticket = atomicAdd(&p.ctl->done_ctas, 1u);
-            s_last = (ticket == gridDim.x - 1) ? 1u : 0u;
-        }
-        __syncthreads();
-    }
-    if (s_last && tid == 0) {
-        __threadfence();
-        AgControl *c = p.ctl;
-        volatile AgControl *vc = c;
-        const uint32_t P = vc->iter;
-        const uint32_t active = vc->active_acc;
-        const double err = vc->err_acc / (double)p.N;
-        if (P < AG_MAX_HISTORY) {
-            c->hist_active[P] = active;
-            c->hist_err[P] = err;
-            unsigned long long t;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            c->hist_t[P] = t;
-        }
-        if (QUANT) {
-            /* every CTA read this pass's slot at its start: free it for the
-             * pass after next */
-            p.qmm[P & 1u] = 0xFFFFFFFFu;
-            p.qmm[2 + (P & 1u)] = 0u;
-        }
-        const bool conv = active == 0;
-        c->prev_err = err;
-        c->last_err_sum = vc->err_acc;
-        c->iter = P + 1;
-        c->converged = conv ? 1u : 0u;
-        const bool cont = !conv && (P + 1 < vc->max_iter);
-        c->active_acc = 0;
-        c->err_acc = 0.0;
-        c->done_ctas = 0;
-        c->stop = cont ? 0u : 1u;
-        __threadfence();
-        if (p.use_cond)
-            cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
-    }
+    ag_close_pass<AG_WARPS>(p, my_err, my_active, QUANT, my_mn, my_mx, true);
 }
 
 /* init: r = base (or the warm start), first contributions (quantised forms:
@@ -503,7 +352,6 @@ __global__ void __launch_bounds__(AG_SBLK) ag_int_init_kernel(const AgPullParams
 {
     constexpr bool WIDE = sizeof(T) == 8;
     constexpr bool QUANT = KIND == AG_INT_QUANT;
-    __shared__ uint32_t s_mn[AG_SBLK / 32], s_mx[AG_SBLK / 32];
     uint32_t mn = 0xFFFFFFFFu, mx = 0u;
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
         const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
@@ -521,49 +369,10 @@ __global__ void __launch_bounds__(AG_SBLK) ag_int_init_kernel(const AgPullParams
             reinterpret_cast<T *>(p.c64_0)[v] = od ? ag_to_fixed<T>(__fdiv_rn(r0, __uint2float_rn(od))) : (T)0;
         }
     }
-    if (QUANT) {
-        mn = __reduce_min_sync(0xffffffffu, mn);
-        mx = __reduce_max_sync(0xffffffffu, mx);
-        if ((threadIdx.x & 31) == 0) {
-            s_mn[threadIdx.x >> 5] = mn;
-            s_mx[threadIdx.x >> 5] = mx;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < AG_SBLK / 32; ++w) {
-                mn = min(mn, s_mn[w]);
-                mx = max(mx, s_mx[w]);
-            }
-            if (mn != 0xFFFFFFFFu)
-                atomicMin(&p.qmm[0], mn);
-            if (mx)
-                atomicMax(&p.qmm[2], mx);
-        }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        AgControl *c = p.ctl;
-        c->iter = 0;
-        c->max_iter = run.max_iter;
-        c->active_acc = 0;
-        c->done_ctas = 0;
-        c->err_acc = 0.0;
-        c->eps = run.eps;
-        c->converged = 0;
-        c->mode_read = 0;
-        c->mode_write = 0;
-        c->switch_pass = 0;
-        c->switch_residual = run.switch_residual;
-        c->prev_err = 1e300;
-        c->rank_sum = 0.0;
-        c->use_init = run.use_init;
-        c->low_passes = 0;
-        unsigned long long t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        c->t0 = t;
-        c->stop = (run.max_iter > 0 && p.N > 0) ? 0u : 1u;
-        if (p.use_cond)
-            cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
-    }
+    if (QUANT)
+        ag_fold_minmax_slot0<AG_SBLK / 32>(p.qmm, mn, mx);
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        ag_reset_control(p, run);
 }
 
 /* quantise the binary32 contributions with the scale of this pass's min/max

@@ -49,65 +49,12 @@
 #include <cub/cub.cuh>
 
 #include "ag_device.h"
+#include "ag_intpass.h"
 #include "ag_mem.h"
 
 #define AG_PNW (AG_SBLK / 32)
 
-/* 64-bit fixed point of the fixed-point forms: 32 fractional bits */
-#define AG_PUSH_FX_ONE 4294967296.0
-
-__device__ __forceinline__ uint64_t ag_push_d2fixed(double x)
-{
-    return (uint64_t)__double2ll_rz(__dmul_rn(x, AG_PUSH_FX_ONE));
-}
-
-__device__ __forceinline__ double ag_push_fixed2d(uint64_t x)
-{
-    return __ddiv_rn(__ll2double_rn((long long)x), AG_PUSH_FX_ONE);
-}
-
-/* order-preserving keys of binary32 values and the 32-bit quantiser (the
- * same definitions as the quantised pulls) */
-__device__ __forceinline__ uint32_t ag_push_fkey(float f)
-{
-    const uint32_t b = __float_as_uint(f);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-__device__ __forceinline__ float ag_push_fkey_value(uint32_t k)
-{
-    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
-}
-
-__device__ __forceinline__ float ag_push_quant_scale(const uint32_t *mm, uint32_t slot)
-{
-    const uint32_t kmin = mm[slot], kmax = mm[2 + slot];
-    if (kmin > kmax)
-        return 0.0f;
-    return __fdiv_rn(__fsub_rn(ag_push_fkey_value(kmax), ag_push_fkey_value(kmin)), (float)0xFFFFFFFFull);
-}
-
-__device__ __forceinline__ uint32_t ag_push_quantize(float x, float scale)
-{
-    if (!(scale > 0.0f))
-        return 0u;
-    const float q = rintf(__fdiv_rn(x, scale));
-    if (!(q > 0.0f))
-        return 0u;
-    if (q >= (float)0xFFFFFFFFull)
-        return 0xFFFFFFFFu;
-    return (uint32_t)q;
-}
-
 __device__ __forceinline__ double ag_push_warp_sum_d(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__device__ __forceinline__ uint32_t ag_push_warp_sum_u(uint32_t v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -130,131 +77,18 @@ __device__ double ag_push_block_sum_d(double v)
     return t;
 }
 
-/* Close a pass: every thread of the CTA calls this after its last element
- * with its share of the pass's error and activity (and, for the quantised
- * push, the min/max keys of the next contributions).  The CTA's totals go to
- * the control block; the last CTA to arrive records the pass, clears the
- * quantised form's slot of this pass, decides whether another pass runs and
- * sets the loop condition.  err_per_n: the error total is the sum divided by
- * N (the plain and push forms) rather than the sum itself (residual forms). */
-__device__ void ag_push_close_pass(const AgPullParams &p, double err, uint32_t active, bool quant, uint32_t mn,
-                                   uint32_t mx, bool err_per_n)
-{
-    __shared__ double s_e[AG_PNW];
-    __shared__ uint32_t s_a[AG_PNW], s_mn[AG_PNW], s_mx[AG_PNW];
-    __shared__ uint32_t s_last;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    err = ag_push_warp_sum_d(err);
-    active = ag_push_warp_sum_u(active);
-    if (quant) {
-        mn = __reduce_min_sync(0xffffffffu, mn);
-        mx = __reduce_max_sync(0xffffffffu, mx);
-    }
-    if (lane == 0) {
-        s_e[warp] = err;
-        s_a[warp] = active;
-        s_mn[warp] = mn;
-        s_mx[warp] = mx;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double be = 0.0;
-        uint32_t ba = 0, bmn = 0xFFFFFFFFu, bmx = 0u;
-        for (int w = 0; w < AG_PNW; ++w) {
-            be += s_e[w];
-            ba += s_a[w];
-            bmn = min(bmn, s_mn[w]);
-            bmx = max(bmx, s_mx[w]);
-        }
-        if (be != 0.0)
-            atomicAdd(&p.ctl->err_acc, be);
-        if (ba)
-            atomicAdd(&p.ctl->active_acc, ba);
-        if (quant) {
-            const uint32_t nslot = (p.ctl->iter + 1u) & 1u;
-            if (bmn != 0xFFFFFFFFu)
-                atomicMin(&p.qmm[nslot], bmn);
-            if (bmx)
-                atomicMax(&p.qmm[2 + nslot], bmx);
-        }
-        __threadfence();
-        const uint32_t ticket = atomicAdd(&p.ctl->done_ctas, 1u);
-        s_last = (ticket == gridDim.x - 1) ? 1u : 0u;
-    }
-    __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        AgControl *c = p.ctl;
-        volatile AgControl *vc = c;
-        const uint32_t P = vc->iter;
-        const uint32_t act = vc->active_acc;
-        const double e = err_per_n ? vc->err_acc / (double)p.N : vc->err_acc;
-        if (P < AG_MAX_HISTORY) {
-            c->hist_active[P] = act;
-            c->hist_err[P] = e;
-            unsigned long long t;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            c->hist_t[P] = t;
-        }
-        if (quant) {
-            p.qmm[P & 1u] = 0xFFFFFFFFu;
-            p.qmm[2 + (P & 1u)] = 0u;
-        }
-        const bool conv = act == 0;
-        c->prev_err = e;
-        c->last_err_sum = vc->err_acc;
-        c->iter = P + 1;
-        c->converged = conv ? 1u : 0u;
-        const bool cont = !conv && (P + 1 < vc->max_iter);
-        c->active_acc = 0;
-        c->err_acc = 0.0;
-        c->done_ctas = 0;
-        c->stop = cont ? 0u : 1u;
-        __threadfence();
-        if (p.use_cond)
-            cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
-    }
-}
-
 __device__ __forceinline__ bool ag_push_stopped(const AgPullParams &p)
 {
     return !p.use_cond && *((volatile uint32_t *)&p.ctl->stop);
 }
 
 /* ---------------------------------------------------------------- init */
-__device__ void ag_push_reset_control(const AgPullParams &p, const AgRunConfig &run)
-{
-    AgControl *c = p.ctl;
-    c->iter = 0;
-    c->max_iter = run.max_iter;
-    c->active_acc = 0;
-    c->done_ctas = 0;
-    c->err_acc = 0.0;
-    c->eps = run.eps;
-    c->converged = 0;
-    c->mode_read = 0;
-    c->mode_write = 0;
-    c->switch_pass = 0;
-    c->switch_residual = run.switch_residual;
-    c->prev_err = 1e300;
-    c->rank_sum = 0.0;
-    c->use_init = run.use_init;
-    c->low_passes = 0;
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    c->t0 = t;
-    c->stop = (run.max_iter > 0 && p.N > 0) ? 0u : 1u;
-    if (p.use_cond)
-        cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
-}
-
 /* push forms: r = base (or the warm start), next = 0, first contributions
  * (quantised: binary32 and their min/max keys in slot 0, which the graph
  * clears first) */
 template <int KIND>
 __global__ void __launch_bounds__(AG_SBLK) ag_push_init_kernel(const AgPullParams p, const AgRunConfig run)
 {
-    __shared__ uint32_t s_mn[AG_PNW], s_mx[AG_PNW];
     uint32_t mn = 0xFFFFFFFFu, mx = 0u;
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK) {
         const float r0 = run.use_init ? p.init_ranks[p.perm ? p.perm[v] : v] : p.base;
@@ -262,38 +96,21 @@ __global__ void __launch_bounds__(AG_SBLK) ag_push_init_kernel(const AgPullParam
         const uint32_t od = p.outdeg[v];
         p.c64_1[v] = 0ull; /* the next sums: 64-bit integer or binary64 zero */
         if (KIND == AG_PUSH_FIXED) {
-            p.c64_0[v] = od ? ag_push_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
+            p.c64_0[v] = od ? ag_d2fixed((double)__fdiv_rn(r0, __uint2float_rn(od))) : 0ull;
         } else {
             const float c = od ? __fdiv_rn(r0, __uint2float_rn(od)) : 0.0f;
             p.pa[v] = c;
             if (KIND == AG_PUSH_QUANT) {
-                const uint32_t k = ag_push_fkey(c);
+                const uint32_t k = ag_fkey(c);
                 mn = min(mn, k);
                 mx = max(mx, k);
             }
         }
     }
-    if (KIND == AG_PUSH_QUANT) {
-        mn = __reduce_min_sync(0xffffffffu, mn);
-        mx = __reduce_max_sync(0xffffffffu, mx);
-        if ((threadIdx.x & 31) == 0) {
-            s_mn[threadIdx.x >> 5] = mn;
-            s_mx[threadIdx.x >> 5] = mx;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < AG_PNW; ++w) {
-                mn = min(mn, s_mn[w]);
-                mx = max(mx, s_mx[w]);
-            }
-            if (mn != 0xFFFFFFFFu)
-                atomicMin(&p.qmm[0], mn);
-            if (mx)
-                atomicMax(&p.qmm[2], mx);
-        }
-    }
+    if (KIND == AG_PUSH_QUANT)
+        ag_fold_minmax_slot0<AG_PNW>(p.qmm, mn, mx);
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        ag_push_reset_control(p, run);
+        ag_reset_control(p, run);
 }
 
 /* residual forms: x[v] = 1 / out_degree[v] (0 without out-edges), the
@@ -324,7 +141,7 @@ __global__ void __launch_bounds__(AG_SBLK) ag_residual_init_kernel(const AgPullP
         p.wl[p.N + v] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        ag_push_reset_control(p, run);
+        ag_reset_control(p, run);
 }
 
 /* ---------------------------------------------------------------- push */
@@ -334,9 +151,9 @@ __global__ void __launch_bounds__(AG_SBLK) ag_push_quant_kernel(const AgPullPara
 {
     if (ag_push_stopped(p))
         return;
-    const float scale = ag_push_quant_scale(p.qmm, p.ctl->iter & 1u);
+    const float scale = ag_quant_scale<uint32_t>(p.qmm, p.ctl->iter & 1u);
     for (uint32_t v = blockIdx.x * AG_SBLK + threadIdx.x; v < p.N; v += gridDim.x * AG_SBLK)
-        p.pa[v] = __fmul_rn(scale, __uint2float_rn(ag_push_quantize(p.pa[v], scale)));
+        p.pa[v] = __fmul_rn(scale, __uint2float_rn(ag_quantize<uint32_t>(p.pa[v], scale)));
 }
 
 /* one thread per forward edge: next[dst] += c[src] (64-bit integer, or
@@ -370,7 +187,7 @@ template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_update_ke
         if (KIND == AG_PUSH_FIXED) {
             const uint64_t s = p.c64_1[v];
             p.c64_1[v] = 0ull;
-            rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_push_fixed2d(s))));
+            rn = __double2float_rn(__dadd_rn((double)p.base, __dmul_rn((double)p.damp, ag_fixed2d(s))));
         } else {
             double *nd = reinterpret_cast<double *>(p.c64_1);
             const float s = __double2float_rn(nd[v]);
@@ -384,18 +201,18 @@ template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_update_ke
         p.rank[v] = rn;
         const uint32_t od = p.outdeg[v];
         if (KIND == AG_PUSH_FIXED) {
-            p.c64_0[v] = od ? ag_push_d2fixed((double)__fdiv_rn(rn, __uint2float_rn(od))) : 0ull;
+            p.c64_0[v] = od ? ag_d2fixed((double)__fdiv_rn(rn, __uint2float_rn(od))) : 0ull;
         } else {
             const float c = od ? __fdiv_rn(rn, __uint2float_rn(od)) : 0.0f;
             p.pa[v] = c;
             if (KIND == AG_PUSH_QUANT) {
-                const uint32_t k = ag_push_fkey(c);
+                const uint32_t k = ag_fkey(c);
                 mn = min(mn, k);
                 mx = max(mx, k);
             }
         }
     }
-    ag_push_close_pass(p, my_err, my_active, KIND == AG_PUSH_QUANT, mn, mx, true);
+    ag_close_pass<AG_PNW>(p, my_err, my_active, KIND == AG_PUSH_QUANT, mn, mx, true);
 }
 
 /* ------------------------------------------------------------ residual */
@@ -463,7 +280,7 @@ template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_
             wl_next[u] = 1;
         }
     }
-    ag_push_close_pass(p, 0.0, my_act, false, 0xFFFFFFFFu, 0u, false);
+    ag_close_pass<AG_PNW>(p, 0.0, my_act, false, 0xFFFFFFFFu, 0u, false);
 }
 
 /* --------------------------------------------------- forward edge list */
