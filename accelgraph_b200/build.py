@@ -75,7 +75,7 @@ def build(force: bool = False, verbose: bool = False, out: Path | None = None, d
         objs.append(str(obj))
     for src in CU_SOURCES:
         obj = build_dir / (src + ".o")
-        _run([nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-Wall", *inc, *dflags, "-c",
+        _run([nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-Wall,-fopenmp", *inc, *dflags, "-c",
               str(CSRC / src), "-o", str(obj)], verbose)
         objs.append(str(obj))
     tmp = lib.with_suffix(".so.tmp")

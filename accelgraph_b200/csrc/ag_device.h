@@ -289,6 +289,11 @@ cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t *ids, uint3
  * residual seed (AG_PUSH_DD, AG_PUSH_PULLPUSH) */
 const void *ag_push_kernel_ptr(int kind, int stage);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
+cudaError_t ag_relabel_layout(const uint32_t *off_old, const uint32_t *outdeg_old, uint32_t n, uint32_t *perm,
+                              uint32_t *inv, uint32_t *off_new, uint32_t *outdeg_new, cudaStream_t s);
+cudaError_t ag_relabel_rows(const uint32_t *perm, const uint32_t *inv, const uint32_t *off_old, const uint32_t *off_new,
+                            const uint32_t *ids_old, uint32_t *ids_new, const float *w_old, float *w_new, uint32_t n,
+                            uint32_t e, cudaStream_t s);
 cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
                                      const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,
                                      uint32_t *inv, uint32_t *off_new, uint32_t *ids_new, float *w_new,

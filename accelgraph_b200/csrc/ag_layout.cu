@@ -133,14 +133,14 @@ static unsigned grid_for(uint64_t n, unsigned per_block)
     return g ? (unsigned)g : 1u;
 }
 
-/* Build the relabelled device CSR.  Inputs (device): off_old[n+1], ids_old[e],
- * w_old[e] (or NULL), outdeg_old[n].  Outputs (device, allocated by the
- * caller): perm[n], inv[n], off_new[n+1], ids_new[e], w_new[e] (or NULL),
- * outdeg_new[n].  Scratch is taken from the stream-ordered pool. */
-extern "C" cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
-                                                const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,
-                                                uint32_t *inv, uint32_t *off_new, uint32_t *ids_new, float *w_new,
-                                                uint32_t *outdeg_new, cudaStream_t s)
+/* The relabelled layout, from the degrees alone.  Inputs (device):
+ * off_old[n+1], outdeg_old[n].  Outputs (device, allocated by the caller):
+ * perm[n], inv[n], off_new[n+1], outdeg_new[n].  Scratch is taken from the
+ * stream-ordered pool.  It needs no in-edge, so it can run while the in-edges
+ * are still being copied to the device. */
+extern "C" cudaError_t ag_relabel_layout(const uint32_t *off_old, const uint32_t *outdeg_old, uint32_t n,
+                                         uint32_t *perm, uint32_t *inv, uint32_t *off_new, uint32_t *outdeg_new,
+                                         cudaStream_t s)
 {
     cudaError_t err;
     if (n == 0)
@@ -180,9 +180,6 @@ extern "C" cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const u
         if (err != cudaSuccess)
             goto done;
     }
-    if (e > 0)
-        ag_copy_rows_kernel<<<grid_for(((uint64_t)e + AG_COPY_SEG - 1) / AG_COPY_SEG * 32, 256), 256, 0, s>>>(
-            perm, inv, off_old, off_new, ids_old, ids_new, w_old, w_new, n, e);
     err = cudaGetLastError();
 done:
     if (iota)
@@ -194,6 +191,31 @@ done:
     if (tmp)
         cudaFreeAsync(tmp, s);
     return err;
+}
+
+/* The relabelled rows: every row copied to its new place, its in-neighbour
+ * ids mapped through inv (and its weights copied), in stream order. */
+extern "C" cudaError_t ag_relabel_rows(const uint32_t *perm, const uint32_t *inv, const uint32_t *off_old,
+                                       const uint32_t *off_new, const uint32_t *ids_old, uint32_t *ids_new,
+                                       const float *w_old, float *w_new, uint32_t n, uint32_t e, cudaStream_t s)
+{
+    if (n == 0 || e == 0)
+        return cudaSuccess;
+    ag_copy_rows_kernel<<<grid_for(((uint64_t)e + AG_COPY_SEG - 1) / AG_COPY_SEG * 32, 256), 256, 0, s>>>(
+        perm, inv, off_old, off_new, ids_old, ids_new, w_old, w_new, n, e);
+    return cudaGetLastError();
+}
+
+/* Layout and rows in one call (device-resident inputs). */
+extern "C" cudaError_t ag_relabel_by_out_degree(const uint32_t *off_old, const uint32_t *ids_old, const float *w_old,
+                                                const uint32_t *outdeg_old, uint32_t n, uint32_t e, uint32_t *perm,
+                                                uint32_t *inv, uint32_t *off_new, uint32_t *ids_new, float *w_new,
+                                                uint32_t *outdeg_new, cudaStream_t s)
+{
+    cudaError_t err = ag_relabel_layout(off_old, outdeg_old, n, perm, inv, off_new, outdeg_new, s);
+    if (err != cudaSuccess)
+        return err;
+    return ag_relabel_rows(perm, inv, off_old, off_new, ids_old, ids_new, w_old, w_new, n, e, s);
 }
 
 extern "C" cudaError_t ag_permute_in(const uint32_t *perm, const float *x, float *x_new, uint32_t n, cudaStream_t s)

@@ -15,6 +15,7 @@
  * exiting.
  */
 #include <cuda_runtime.h>
+#include <omp.h>
 #include <stdarg.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -226,6 +227,24 @@ static ag_status_t event_wait(cudaEvent_t ev, double timeout_s)
     }
 }
 
+/* host memcpy split over up to 16 OpenMP threads (one thread copies about
+ * 10 GB/s; the device link moves about 50 GB/s) */
+static void par_memcpy(void *dst, const void *src, size_t n)
+{
+    const int nt = std::min(16, omp_get_max_threads());
+    if (n < ((size_t)1 << 20) || nt <= 1) {
+        memcpy(dst, src, n);
+        return;
+    }
+    const size_t piece = ((n + (size_t)nt - 1) / (size_t)nt + 4095) & ~(size_t)4095;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int t = 0; t < nt; ++t) {
+        const size_t a = (size_t)t * piece;
+        if (a < n)
+            memcpy((unsigned char *)dst + a, (const unsigned char *)src + a, std::min(piece, n - a));
+    }
+}
+
 /* Copy `bytes` of device memory to host memory `dst` on the library stream
  * and wait for it (bounded).  A page-locked destination is copied directly;
  * a pageable one goes through two page-locked chunks, so that the device
@@ -276,7 +295,7 @@ static ag_status_t copy_to_host(void *dst, const void *src, size_t bytes)
         ag_status_t st = event_wait(g_stage.ev[k & 1], 0);
         if (st != AG_OK)
             return st;
-        memcpy(d + k * AG_STAGE_CHUNK, g_stage.buf + (k & 1) * AG_STAGE_CHUNK, len(k));
+        par_memcpy(d + k * AG_STAGE_CHUNK, g_stage.buf + (k & 1) * AG_STAGE_CHUNK, len(k));
     }
     return AG_OK;
 }
@@ -563,6 +582,29 @@ extern "C" ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t fl
     return upload_impl(graph, flags, nullptr, 0, 0, out);
 }
 
+/* The upload's copy stream (one per device): the in-edge copies of a host
+ * graph run on it while the library stream lays out the relabelled rows and
+ * plans the work lists from the degrees.  ev[0] orders it after the
+ * library stream's allocations, ev[1] the library stream after its copies. */
+static struct
+{
+    int device;
+    cudaStream_t stream;
+    cudaEvent_t ev[2];
+} g_copy = {-1, nullptr, {nullptr, nullptr}};
+
+static ag_status_t copy_stream_ensure(void)
+{
+    if (g_copy.stream && g_copy.device == g_ctx.device)
+        return AG_OK;
+    g_copy.stream = nullptr; /* a stream of another device is left to it */
+    AG_CUDA(cudaStreamCreateWithFlags(&g_copy.stream, cudaStreamNonBlocking));
+    AG_CUDA(cudaEventCreateWithFlags(&g_copy.ev[0], cudaEventDisableTiming));
+    AG_CUDA(cudaEventCreateWithFlags(&g_copy.ev[1], cudaEventDisableTiming));
+    g_copy.device = g_ctx.device;
+    return AG_OK;
+}
+
 /* gather_n: length of the vector the in-edges index (0: num_vertices).
  * dev: the graph's CSR already in device memory (built by ag_graph_build);
  * `graph` is then unused, and the device arrays are copied, not checked. */
@@ -623,6 +665,9 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         g->outdeg = outdeg_old;
         g->w = w_old;
     }
+    /* in-edges of a host graph travel on the copy stream */
+    if (st == AG_OK && !dev)
+        st = copy_stream_ensure();
     if (st != AG_OK) {
         if (relabel) {
             dev_free(off_old);
@@ -633,11 +678,19 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         ag_graph_release(g);
         return st;
     }
+    cudaStream_t cs = dev ? s : g_copy.stream;
+    /* every exit before the join waits for the copy stream first: neither the
+     * caller's arrays nor the device buffers it writes may go while it runs */
+    auto join_copies = [&]() {
+        if (cs != s)
+            cudaStreamSynchronize(cs);
+    };
 #define UP(call)                                                                                 \
     do {                                                                                         \
         cudaError_t e_ = (call);                                                                 \
         if (e_ != cudaSuccess) {                                                                 \
             cudaGetLastError();                                                                  \
+            join_copies();                                                                       \
             st = ag_set_error(AG_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
             if (relabel) {                                                                       \
                 dev_free(off_old);                                                               \
@@ -651,6 +704,7 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
     } while (0)
 #define UPFAIL(status)                                                                           \
     do {                                                                                         \
+        join_copies();                                                                           \
         st = (status);                                                                           \
         if (relabel) {                                                                           \
             dev_free(off_old);                                                                   \
@@ -681,11 +735,14 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
          * on the same stream).  Every error path below waits for the stream
          * before the caller's arrays can be freed (ag_graph_release does). */
         const bool guess_contiguous = N == 0 || iv->edges_idx[0] == 0;
+        /* the copy stream starts after the library stream's allocations */
+        UP(cudaEventRecord(g_copy.ev[0], s));
+        UP(cudaStreamWaitEvent(cs, g_copy.ev[0], 0));
         if (guess_contiguous) {
             if (E)
-                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, cs));
             if (want_w && E)
-                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, cs));
         }
         if (N)
             UP(cudaMemcpyAsync(outdeg_old, fv->out_degree, (size_t)N * 4, cudaMemcpyHostToDevice, s));
@@ -729,12 +786,12 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         } else {
             UP(cudaMemcpyAsync(off_old, off.data(), (size_t)(N + 1) * 4, cudaMemcpyHostToDevice, s));
         }
-        UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, s));
+        UP(cudaMemsetAsync(ids_old + E, 0, (size_t)(g->E4 - E) * 4, cs));
         if (contiguous) {
             if (!guess_contiguous && E)
-                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+                UP(cudaMemcpyAsync(ids_old, iel->edges_array_dest, (size_t)E * 4, cudaMemcpyHostToDevice, cs));
             if (!guess_contiguous && want_w && E)
-                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, s));
+                UP(cudaMemcpyAsync(w_old, iel->edges_array_weight, (size_t)E * 4, cudaMemcpyHostToDevice, cs));
         } else {
             std::vector<uint32_t> packed(E);
             std::vector<float> packw(want_w ? E : 0);
@@ -745,49 +802,26 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
                     memcpy(packw.data() + off[v], iel->edges_array_weight + b, (size_t)d * 4);
             }
             if (E)
-                UP(cudaMemcpyAsync(ids_old, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+                UP(cudaMemcpyAsync(ids_old, packed.data(), (size_t)E * 4, cudaMemcpyHostToDevice, cs));
             if (want_w && E)
-                UP(cudaMemcpyAsync(w_old, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
-            UP(cudaStreamSynchronize(s)); /* the packed copies are stack-owned */
+                UP(cudaMemcpyAsync(w_old, packw.data(), (size_t)E * 4, cudaMemcpyHostToDevice, cs));
+            UP(cudaStreamSynchronize(cs)); /* the packed copies are stack-owned */
         }
         if (want_w)
-            UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, s));
+            UP(cudaMemsetAsync(w_old + E, 0, (size_t)(g->E4 - E) * 4, cs));
+        UP(cudaEventRecord(g_copy.ev[1], cs));
     }
     UP(cudaMemsetAsync(g->ctl, 0, sizeof(AgControl), s));
     UP(cudaMemsetAsync(g->flag, 0, 4, s));
     UP(cudaMemsetAsync(g->flag + 1, 0xFF, 4, s));
-    /* every in-edge must name a vertex < N before anything reads through it */
-    if (!(flags & AG_UPLOAD_TRUSTED)) {
-        uint32_t hflag[2] = {0, 0};
-        UP(ag_validate_ids(ids_old, E, gather_n ? gather_n : N, g->flag, s));
-        UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
-        UP(cudaStreamSynchronize(s));
-        if (hflag[0]) {
-            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1],
-                              gather_n ? gather_n : N);
-            if (relabel) {
-                dev_free(off_old);
-                dev_free(ids_old);
-                dev_free(outdeg_old);
-                dev_free(w_old);
-            }
-            ag_graph_release(g);
-            return st;
-        }
-    }
+
+    /* While the in-edges travel: the relabelled layout, the tunables and the
+     * work lists need only the degrees. */
     if (relabel) {
         UP(cudaMemsetAsync(g->ids + E, 0, (size_t)(g->E4 - E) * 4, s));
         if (want_w)
             UP(cudaMemsetAsync(g->w + E, 0, (size_t)(g->E4 - E) * 4, s));
-        UP(ag_relabel_by_out_degree(off_old, ids_old, w_old, outdeg_old, N, E, g->perm, g->inv, g->row_off, g->ids,
-                                    g->w, g->outdeg, s));
-        dev_free(off_old);
-        dev_free(ids_old);
-        dev_free(outdeg_old);
-        dev_free(w_old);
-        g->device_bytes -= (uint64_t)(N + 1) * 4 + (uint64_t)g->E4 * 4 * (want_w ? 2 : 1) + (uint64_t)N * 4 + 16;
-        off_old = ids_old = outdeg_old = nullptr;
-        w_old = nullptr;
+        UP(ag_relabel_layout(off_old, outdeg_old, N, g->perm, g->inv, g->row_off, g->outdeg, s));
     }
     {
         /* tunables (the defaults were measured best on R-MAT s20/s22):
@@ -809,23 +843,51 @@ static ag_status_t upload_impl(const struct GraphCSR *graph, uint32_t flags, con
         g->tiles.hot_entries = g->hot_n;
         g->tiles.warm_entries = g->warm_n;
     }
-
     if (ngraphs) {
         g->ngraphs = ngraphs;
         g->gstart_host = new std::vector<uint32_t>(gstart_host, gstart_host + ngraphs + 1);
         g->gstart = (uint32_t *)dev_alloc(g, (size_t)(ngraphs + 1) * 4, &st);
         g->g_u32 = (uint32_t *)dev_alloc(g, (size_t)ngraphs * 4 * 4, &st);
         g->g_f64 = (double *)dev_alloc(g, (size_t)ngraphs * 2 * 8, &st);
-        if (st != AG_OK) {
-            ag_graph_release(g);
-            return st;
-        }
+        if (st != AG_OK)
+            UPFAIL(st);
         UP(cudaMemcpyAsync(g->gstart, gstart_host, (size_t)(ngraphs + 1) * 4, cudaMemcpyHostToDevice, s));
     }
     st = plan_device(g, g->tiles.task_edges, g->tiles.hub_chunk);
-    if (st != AG_OK) {
-        ag_graph_release(g);
-        return st;
+    if (st != AG_OK)
+        UPFAIL(st);
+
+    /* the in-edges have arrived */
+    if (cs != s)
+        UP(cudaStreamWaitEvent(s, g_copy.ev[1], 0));
+    /* every in-edge must name a vertex < N before anything reads through it */
+    if (!(flags & AG_UPLOAD_TRUSTED)) {
+        uint32_t hflag[2] = {0, 0};
+        UP(ag_validate_ids(ids_old, E, gather_n ? gather_n : N, g->flag, s));
+        UP(cudaMemcpyAsync(hflag, g->flag, 8, cudaMemcpyDeviceToHost, s));
+        UP(cudaStreamSynchronize(s));
+        if (hflag[0]) {
+            st = ag_set_error(AG_ERR_INVALID_GRAPH, "in-edge %u names a vertex >= %u", hflag[1],
+                              gather_n ? gather_n : N);
+            if (relabel) {
+                dev_free(off_old);
+                dev_free(ids_old);
+                dev_free(outdeg_old);
+                dev_free(w_old);
+            }
+            ag_graph_release(g);
+            return st;
+        }
+    }
+    if (relabel) {
+        UP(ag_relabel_rows(g->perm, g->inv, off_old, g->row_off, ids_old, g->ids, w_old, g->w, N, E, s));
+        dev_free(off_old);
+        dev_free(ids_old);
+        dev_free(outdeg_old);
+        dev_free(w_old);
+        g->device_bytes -= (uint64_t)(N + 1) * 4 + (uint64_t)g->E4 * 4 * (want_w ? 2 : 1) + (uint64_t)N * 4 + 16;
+        off_old = ids_old = outdeg_old = nullptr;
+        w_old = nullptr;
     }
     UP(cudaEventCreate(&g->ev0));
     UP(cudaEventCreate(&g->ev1));
