@@ -288,6 +288,9 @@ cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t *ids, uint3
  * or vertex phase, 2 update or edge phase, 3 quantiser (AG_PUSH_QUANT) or
  * residual seed (AG_PUSH_DD, AG_PUSH_PULLPUSH) */
 const void *ag_push_kernel_ptr(int kind, int stage);
+/* CTA size and dynamic shared memory of the push scatter and of the residual
+ * edge phase */
+void ag_push_scatter_shape(unsigned *threads, size_t *smem);
 cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t N, uint32_t *flag, cudaStream_t s);
 cudaError_t ag_relabel_layout(const uint32_t *off_old, const uint32_t *outdeg_old, uint32_t n, uint32_t *perm,
                               uint32_t *inv, uint32_t *off_new, uint32_t *outdeg_new, cudaStream_t s);

@@ -53,6 +53,10 @@
 #include "ag_mem.h"
 
 #define AG_PNW (AG_SBLK / 32)
+#define AG_PUSH_BLK 1024     /* threads of a scatter CTA (one per SM)        */
+#define AG_PUSH_HOT 8192u    /* destinations summed in shared memory (64 KB) */
+#define AG_RES_HOT 8192u     /* residual destinations summed in shared memory
+                                (32 KB; the same table space) */
 
 __device__ __forceinline__ double ag_push_warp_sum_d(double v)
 {
@@ -156,21 +160,44 @@ __global__ void __launch_bounds__(AG_SBLK) ag_push_quant_kernel(const AgPullPara
         p.pa[v] = __fmul_rn(scale, __uint2float_rn(ag_quantize<uint32_t>(p.pa[v], scale)));
 }
 
-/* one thread per forward edge: next[dst] += c[src] (64-bit integer, or
- * binary64 for the binary32 forms) */
-template <int KIND> __global__ void __launch_bounds__(AG_SBLK) ag_push_scatter_kernel(const AgPullParams p)
+/* One thread per forward edge: next[dst] += c[src] (64-bit integer, or
+ * binary64 for the binary32 forms).  The first AG_PUSH_HOT destinations (the
+ * most-read vertices after the relabelling by out-degree, and in power-law
+ * graphs the in-hubs) are summed first in a shared-memory table of the CTA
+ * and added to next once per CTA: adds to one hub otherwise queue at the one
+ * L2 slice that holds it.  A persistent grid of AG_PUSH_BLK-thread CTAs. */
+template <int KIND> __global__ void __launch_bounds__(AG_PUSH_BLK) ag_push_scatter_kernel(const AgPullParams p)
 {
+    extern __shared__ __align__(16) unsigned long long ag_push_hot[];
     if (ag_push_stopped(p))
         return;
+    const uint32_t hot_n = min(p.N, (uint32_t)AG_PUSH_HOT);
+    for (uint32_t i = threadIdx.x; i < hot_n; i += AG_PUSH_BLK)
+        ag_push_hot[i] = 0ull;
+    __syncthreads();
     const uint64_t pol_first = ag_policy_evict_first();
-    const uint32_t stride = gridDim.x * AG_SBLK;
-    for (uint32_t j = blockIdx.x * AG_SBLK + threadIdx.x; j < p.E; j += stride) {
+    const uint32_t stride = gridDim.x * AG_PUSH_BLK;
+    for (uint32_t j = blockIdx.x * AG_PUSH_BLK + threadIdx.x; j < p.E; j += stride) {
         const uint32_t v = ag_ld_stream_u32(p.fwd_src + j, pol_first);
         const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
+        if (KIND == AG_PUSH_FIXED) {
+            const unsigned long long c = p.c64_0[v];
+            atomicAdd(u < hot_n ? ag_push_hot + u : (unsigned long long *)p.c64_1 + u, c);
+        } else {
+            const double c = (double)p.pa[v];
+            atomicAdd(u < hot_n ? reinterpret_cast<double *>(ag_push_hot) + u : reinterpret_cast<double *>(p.c64_1) + u,
+                      c);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < hot_n; i += AG_PUSH_BLK) {
+        const unsigned long long t = ag_push_hot[i];
+        if (t == 0ull) /* +0.0 or integer 0: nothing to add */
+            continue;
         if (KIND == AG_PUSH_FIXED)
-            atomicAdd((unsigned long long *)p.c64_1 + u, (unsigned long long)p.c64_0[v]);
+            atomicAdd((unsigned long long *)p.c64_1 + i, t);
         else
-            atomicAdd(reinterpret_cast<double *>(p.c64_1) + u, (double)p.pa[v]);
+            atomicAdd(reinterpret_cast<double *>(p.c64_1) + i, __longlong_as_double((long long)t));
     }
 }
 
@@ -254,33 +281,65 @@ template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_
         atomicAdd(&p.ctl->err_acc, e);
 }
 
-/* edge phase: one thread per forward edge of a worklist source */
-template <bool PULLPUSH> __global__ void __launch_bounds__(AG_SBLK) ag_residual_edge_kernel(const AgPullParams p)
+/* Edge phase: one thread per forward edge of a worklist source (a
+ * persistent grid of AG_PUSH_BLK-thread CTAs).  In the data-driven push the
+ * first AG_RES_HOT destinations (the in-hubs of power-law graphs) are summed
+ * first in a shared-memory table of the CTA and added to the residual once per
+ * CTA, with the crossing test on that add: residuals only grow within a pass,
+ * so exactly one add takes a residual across epsilon whether the adds come
+ * one edge at a time or one CTA at a time, and the activations and the next
+ * worklist are the same.  The pull-push adds each crossing edge's delta a
+ * second time, so every one of its edges adds on its own. */
+template <bool PULLPUSH> __global__ void __launch_bounds__(AG_PUSH_BLK) ag_residual_edge_kernel(const AgPullParams p)
 {
+    extern __shared__ __align__(16) unsigned long long ag_push_hot[];
+    float *hot = reinterpret_cast<float *>(ag_push_hot);
     if (ag_push_stopped(p))
         return;
     const uint32_t pass = p.ctl->iter;
     const uint8_t *wl_cur = p.wl + (size_t)(pass & 1u) * p.N;
     uint8_t *wl_next = p.wl + (size_t)((pass + 1u) & 1u) * p.N;
     const double eps = p.ctl->eps;
+    const uint32_t hot_n = PULLPUSH ? 0u : min(p.N, (uint32_t)AG_RES_HOT);
+    for (uint32_t i = threadIdx.x; i < hot_n; i += AG_PUSH_BLK)
+        hot[i] = 0.0f;
+    __syncthreads();
     const uint64_t pol_first = ag_policy_evict_first();
     uint32_t my_act = 0;
-    const uint32_t stride = gridDim.x * AG_SBLK;
-    for (uint32_t j = blockIdx.x * AG_SBLK + threadIdx.x; j < p.E; j += stride) {
+    auto crosses = [&](float prev, float add) {
+        return (double)fabsf(__fadd_rn(prev, add)) >= eps && (double)prev <= eps;
+    };
+    const uint32_t stride = gridDim.x * AG_PUSH_BLK;
+    for (uint32_t j = blockIdx.x * AG_PUSH_BLK + threadIdx.x; j < p.E; j += stride) {
         const uint32_t v = ag_ld_stream_u32(p.fwd_src + j, pol_first);
         if (!wl_cur[v])
             continue;
         const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
         const float dl = p.delta[v];
+        if (u < hot_n && u != v) {
+            atomicAdd(hot + u, dl);
+            continue;
+        }
         const float prev = u == v ? p.pb[v] : atomicAdd(p.res + u, dl);
-        if ((double)fabsf(__fadd_rn(prev, dl)) >= eps && (double)prev <= eps) {
+        if (crosses(prev, dl)) {
             ++my_act;
             if (PULLPUSH && u != v)
                 atomicAdd(p.res + u, dl);
             wl_next[u] = 1;
         }
     }
-    ag_close_pass<AG_PNW>(p, 0.0, my_act, false, 0xFFFFFFFFu, 0u, false);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < hot_n; i += AG_PUSH_BLK) {
+        const float t = hot[i];
+        if (t == 0.0f)
+            continue;
+        const float prev = atomicAdd(p.res + i, t);
+        if (crosses(prev, t)) {
+            ++my_act;
+            wl_next[i] = 1;
+        }
+    }
+    ag_close_pass<AG_PUSH_BLK / 32>(p, 0.0, my_act, false, 0xFFFFFFFFu, 0u, false);
 }
 
 /* --------------------------------------------------- forward edge list */
@@ -330,6 +389,14 @@ extern "C" cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t 
         cudaFreeAsync(tmp, s);
     cudaFreeAsync(rows, s);
     return err;
+}
+
+/* launch shape of the push scatter and of the residual edge phase: threads
+ * per CTA, dynamic shared memory */
+extern "C" void ag_push_scatter_shape(unsigned *threads, size_t *smem)
+{
+    *threads = AG_PUSH_BLK;
+    *smem = (size_t)AG_PUSH_HOT * 8;
 }
 
 extern "C" const void *ag_push_kernel_ptr(int kind, int stage)

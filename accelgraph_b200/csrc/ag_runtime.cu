@@ -1250,10 +1250,32 @@ static AgPullParams push_spmv_params(ag_graph_s *g, int exact)
 
 static size_t push_spmv_smem(const AgPullParams &q) { return (size_t)AG_STAGE_BYTES + (size_t)q.hot_n * 4; }
 
-static dim3 push_edge_grid(const ag_graph_s *g)
+/* launch shape of the push scatter: a persistent grid at the kernel's
+ * occupancy, with its shared-memory table */
+struct PushScatterShape
 {
-    return dim3((unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>(((uint64_t)g->E + AG_SBLK - 1) / AG_SBLK, (uint64_t)g_ctx.num_sms * 32)));
+    dim3 grid, block;
+    size_t smem;
+};
+
+static ag_status_t push_scatter_shape(int kind, PushScatterShape *sh)
+{
+    unsigned threads = 0;
+    size_t smem = 0;
+    ag_push_scatter_shape(&threads, &smem);
+    /* the push scatter (stage 1) or the residual forms' edge phase (stage 2) */
+    const bool residual = kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH;
+    const void *k = ag_push_kernel_ptr(kind, residual ? 2 : 1);
+    AG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (int)threads, smem) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    sh->grid = dim3((unsigned)(nb * g_ctx.num_sms));
+    sh->block = dim3(threads);
+    sh->smem = smem;
+    return AG_OK;
 }
 
 /* The push form's graph: [qmm clears] init, WHILE { [quantiser] scatter,
@@ -1270,7 +1292,7 @@ static ag_status_t build_exec_push(ag_graph_s *g, int kind)
     x->params.cond = x->cond;
     x->params.use_cond = 1;
     const bool residual = kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH;
-    const dim3 eg = elem_grid(g), blk(AG_SBLK), edge_grid = push_edge_grid(g);
+    const dim3 eg = elem_grid(g), blk(AG_SBLK);
     void *pargs[1] = {&x->params};
 
     cudaGraphNode_t prev[2];
@@ -1354,8 +1376,17 @@ static ag_status_t build_exec_push(ag_graph_s *g, int kind)
         const size_t lsm = push_spmv_smem(loop_spmv);
         AG_CUDA(add(ksp, dim3(pull_grid(ksp, loop_spmv.ntasks, lsm)), dim3(AG_BLK), lsm, largs));
     }
-    AG_CUDA(add(ag_push_kernel_ptr(kind, 1), residual ? eg : edge_grid, blk, 0, pargs));
-    AG_CUDA(add(ag_push_kernel_ptr(kind, 2), residual ? edge_grid : eg, blk, 0, pargs));
+    PushScatterShape sh;
+    ag_status_t sst = push_scatter_shape(kind, &sh);
+    if (sst != AG_OK)
+        return sst;
+    if (residual) {
+        AG_CUDA(add(ag_push_kernel_ptr(kind, 1), eg, blk, 0, pargs));
+        AG_CUDA(add(ag_push_kernel_ptr(kind, 2), sh.grid, sh.block, sh.smem, pargs));
+    } else {
+        AG_CUDA(add(ag_push_kernel_ptr(kind, 1), sh.grid, sh.block, sh.smem, pargs));
+        AG_CUDA(add(ag_push_kernel_ptr(kind, 2), eg, blk, 0, pargs));
+    }
 
     void *norm_args[1] = {&x->params};
     cudaKernelNodeParams kn = {};
@@ -1378,7 +1409,7 @@ static ag_status_t push_stream_launch(ag_graph_s *g, int kind, const AgRunConfig
     AgPullParams sp = base_params(g, 0);
     sp.use_cond = 0;
     const bool residual = kind == AG_PUSH_DD || kind == AG_PUSH_PULLPUSH;
-    const dim3 eg = elem_grid(g), blk(AG_SBLK), edge_grid = push_edge_grid(g);
+    const dim3 eg = elem_grid(g), blk(AG_SBLK);
     void *pa[1] = {&sp};
     AgRunConfig r = run;
     void *ia[2] = {&sp, &r};
@@ -1386,6 +1417,10 @@ static ag_status_t push_stream_launch(ag_graph_s *g, int kind, const AgRunConfig
     seed_spmv.honor_stop = 0;
     void *sa[1] = {&seed_spmv}, *la[1] = {&loop_spmv};
     const void *kse = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 1), *ksl = ag_pull_kernel_ptr(AG_MODE_SPMV, 0, 0);
+    PushScatterShape sh;
+    ag_status_t sst = push_scatter_shape(kind, &sh);
+    if (sst != AG_OK)
+        return sst;
     if (kind == AG_PUSH_QUANT) {
         AG_CUDA(cudaMemsetAsync(g->qmm, 0xFF, 8, s));
         AG_CUDA(cudaMemsetAsync(g->qmm + 2, 0, 8, s));
@@ -1403,8 +1438,13 @@ static ag_status_t push_stream_launch(ag_graph_s *g, int kind, const AgRunConfig
         if (kind == AG_PUSH_PULLPUSH && loop_spmv.ntasks)
             AG_CUDA(cudaLaunchKernel(ksl, dim3(pull_grid(ksl, loop_spmv.ntasks, push_spmv_smem(loop_spmv))),
                                      dim3(AG_BLK), la, push_spmv_smem(loop_spmv), s));
-        AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 1), residual ? eg : edge_grid, blk, pa, 0, s));
-        AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 2), residual ? edge_grid : eg, blk, pa, 0, s));
+        if (residual) {
+            AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 1), eg, blk, pa, 0, s));
+            AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 2), sh.grid, sh.block, pa, sh.smem, s));
+        } else {
+            AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 1), sh.grid, sh.block, pa, sh.smem, s));
+            AG_CUDA(cudaLaunchKernel(ag_push_kernel_ptr(kind, 2), eg, blk, pa, 0, s));
+        }
     }
     AG_CUDA(cudaLaunchKernel(ag_normalize_kernel_ptr(), eg, blk, pa, 0, s));
     return AG_OK;
