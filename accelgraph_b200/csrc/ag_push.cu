@@ -180,13 +180,20 @@ template <int KIND> __global__ void __launch_bounds__(AG_PUSH_BLK) ag_push_scatt
     for (uint32_t j = blockIdx.x * AG_PUSH_BLK + threadIdx.x; j < p.E; j += stride) {
         const uint32_t v = ag_ld_stream_u32(p.fwd_src + j, pol_first);
         const uint32_t u = ag_ld_stream_u32(p.fwd_dst + j, pol_first);
+        /* separate shared and global adds: a pointer to either would make a
+         * generic atomic that returns its value instead of a reduction */
         if (KIND == AG_PUSH_FIXED) {
             const unsigned long long c = p.c64_0[v];
-            atomicAdd(u < hot_n ? ag_push_hot + u : (unsigned long long *)p.c64_1 + u, c);
+            if (u < hot_n)
+                atomicAdd(ag_push_hot + u, c);
+            else
+                atomicAdd((unsigned long long *)p.c64_1 + u, c);
         } else {
             const double c = (double)p.pa[v];
-            atomicAdd(u < hot_n ? reinterpret_cast<double *>(ag_push_hot) + u : reinterpret_cast<double *>(p.c64_1) + u,
-                      c);
+            if (u < hot_n)
+                atomicAdd(reinterpret_cast<double *>(ag_push_hot) + u, c);
+            else
+                atomicAdd(reinterpret_cast<double *>(p.c64_1) + u, c);
         }
     }
     __syncthreads();
