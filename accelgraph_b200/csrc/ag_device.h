@@ -38,9 +38,10 @@
 #define AG_TSEQ 32        /* FAST order: rows up to this length summed by
                              one lane in stream order                       */
 #ifndef AG_WHUB
-#define AG_WHUB 2048      /* FAST order: rows longer than this are split
-                             into chunks of AG_WHUB in-edges on separate
-                             warps; EXACT order keeps them on one warp      */
+#define AG_WHUB 2048      /* rows longer than this are split into chunks of
+                             AG_WHUB in-edges on separate warps (EXACT
+                             order: the chunks stage their values and the
+                             last one sums the row in stream order)         */
 #endif
 #define AG_STAGE_BYTES (AG_WARPS * AG_WCAP * 4)
 #if AG_CTAS_PER_SM == 1
@@ -154,6 +155,8 @@ typedef struct AgPullParams
     uint16_t *c16_0, *c16_1;
     float *hub_part;
     uint32_t *hub_cnt;
+    float *hub_vals;       /* EXACT order: hub rows' gathered values, at chunk
+                              slot x whub + offset in the row                  */
     AgControl *ctl;
     const AgRunConfig *cfg;
     const float *init_ranks;
@@ -254,8 +257,8 @@ void ag_csr_free_device(AgDevCSR *c, cudaStream_t s);
  * is stream-ordered: wait on the stream before reading them) */
 cudaError_t ag_plan_count(const uint32_t *row_off, uint32_t n, uint32_t cap, uint32_t whub, const uint32_t *gstart,
                           uint32_t ngraphs, AgPlanState *ps, uint32_t *totals_host, cudaStream_t s);
-/* write both lists: fast holds hub + long + row items, exact holds
- * long + split rows + row items */
+/* write both lists (the same items: hub chunks, long rows, row items; the
+ * kernel's order decides how each is summed) */
 cudaError_t ag_plan_write(AgPlanState *ps, const uint32_t *totals, uint4 *fast, uint4 *exact, cudaStream_t s);
 void ag_plan_release(AgPlanState *ps, cudaStream_t s);
 cudaError_t ag_set_u32(uint32_t *p, uint32_t v, cudaStream_t s);

@@ -6,9 +6,9 @@
  * the counts are scanned, and a second walk writes every item at its final
  * position.  The lists, the item kinds and their order are those of the
  * pull kernel's contract:
- *   FAST  : hub chunks (rows above hub_chunk in-edges, split in chunks),
- *           then long rows (above task_edges), then row items;
- *   EXACT : every row above task_edges as one long item, then row items.
+ *   FAST and EXACT (the same list): hub chunks (rows above hub_chunk
+ *           in-edges, split in chunks), then long rows (above task_edges),
+ *           then row items.  The kernel's order decides how each is summed.
  * A row item packs at most AG_WROWS consecutive rows of at most task_edges
  * in-edges each and together; it never crosses the first row of a graph of
  * a block-diagonal union, nor a segment boundary (a segment holds 512 rows,
@@ -60,12 +60,11 @@ __global__ void ag_plan_kernel(const AgPlanArgs a, uint32_t *cnt, const uint32_t
     uint32_t r = seg * AG_PLAN_SEG;
     const uint32_t rend = min(a.n, r + AG_PLAN_SEG);
     uint32_t nh = 0, nl = 0, nw = 0, nhr = 0;
-    uint32_t hb = 0, lb = 0, wb = 0, hrb = 0;
+    uint32_t hb = 0, lb = 0, wb = 0;
     if (WRITE) {
         hb = scan[seg];
         lb = scan[stride + seg];
         wb = scan[2 * stride + seg];
-        hrb = scan[3 * stride + seg];
     }
     uint32_t gi = a.gstart ? ag_plan_next_graph(a, r) : 0;
     while (r < rend) {
@@ -78,17 +77,18 @@ __global__ void ag_plan_kernel(const AgPlanArgs a, uint32_t *cnt, const uint32_t
                     const uint32_t pbase = hb + nh;
                     for (uint32_t c = 0; c < nch; ++c) {
                         const uint32_t cb = o0 + c * a.whub;
-                        fast[pbase + c] =
+                        const uint4 it =
                             make_uint4((AG_T_HUB << 30) | r, pbase | (c << AG_SLOT_BITS), cb, min(o1, cb + a.whub));
+                        fast[pbase + c] = it;
+                        exact[pbase + c] = it;
                     }
-                    exact[lb + hrb + nl + nhr] = lng;
                 }
                 nh += nch;
                 ++nhr;
             } else {
                 if (WRITE) {
                     fast[tot.hub_items + lb + nl] = lng;
-                    exact[lb + hrb + nl + nhr] = lng;
+                    exact[tot.hub_items + lb + nl] = lng;
                 }
                 ++nl;
             }
@@ -116,7 +116,7 @@ __global__ void ag_plan_kernel(const AgPlanArgs a, uint32_t *cnt, const uint32_t
         if (WRITE) {
             const uint4 it = make_uint4((AG_T_ROWS << 30) | rb, r, eb, ee);
             fast[tot.hub_items + tot.long_items + wb + nw] = it;
-            exact[tot.long_items + tot.hub_rows + wb + nw] = it;
+            exact[tot.hub_items + tot.long_items + wb + nw] = it;
         }
         ++nw;
     }

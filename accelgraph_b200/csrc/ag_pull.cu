@@ -32,7 +32,9 @@
  *          straight from memory + xor tree.
  *   hub  : longer rows split into hub-chunk-sized pieces on separate warps;
  *          the last chunk to arrive sums the chunk partials in chunk order.
- * In EXACT order every row is summed in stream order by one lane.
+ * In EXACT order every row is summed in stream order by one lane; a hub
+ * row's chunks store their gathered values in a staging array, and the last
+ * chunk to arrive adds them in stream order.
  * All reductions have a fixed order: results do not depend on scheduling.
  */
 #include <cuda_bf16.h>
@@ -436,6 +438,80 @@ struct AgPass
         return s;
     }
 
+    /* EXACT-order hub chunk: the gathered values of in-edges [eb, ee) of a
+     * row starting at o0, stored at dst[j - o0] (coalesced) */
+    __device__ __forceinline__ void stage_global(float *dst, uint32_t o0, uint32_t eb, uint32_t ee, uint32_t lane,
+                                                 const Pair &first) const
+    {
+        const uint32_t q1 = (ee + 3u) >> 2;
+        uint32_t qa = (eb >> 2) + lane;
+        Pair cur = first;
+        while (qa < q1) {
+            const Pair nx = load_pair(qa + 64, q1);
+            float v[8];
+            bool in[8];
+            gather8(cur, qa, eb, ee, v, in);
+            const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (in[k])
+                    dst[ja + k - o0] = v[k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (in[4 + k])
+                    dst[jb + k - o0] = v[4 + k];
+            cur = nx;
+            qa += 64;
+        }
+    }
+
+    /* EXACT-order hub row: the stream-order sum of its n staged values
+     * src[0, n) on one warp.  Every lane runs the same chain: value i of a
+     * 256-value block comes from the lane that loaded it by a shuffle, so the
+     * warp never diverges and nothing passes through shared memory; the two
+     * blocks after the current one are loading (from L2, coalesced) while it
+     * is added.  Elements past n are skipped by a warp-uniform test. */
+    __device__ __forceinline__ float ordered_chain(const float *src, uint32_t n, uint32_t lane, uint32_t &neg) const
+    {
+        float s = 0.0f;
+        float a[8], b[8];
+        auto load = [&](float *r, uint32_t cb) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t j = cb + lane + 32u * k;
+                r[k] = j < n ? __ldcg(src + j) : 0.0f;
+            }
+        };
+        load(a, 0);
+        load(b, 256u);
+        for (uint32_t cb = 0; cb < n; cb += 256u) {
+            float c[8];
+            if (cb + 512u < n)
+                load(c, cb + 512u);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    float v = __shfl_sync(0xffffffffu, a[k], i);
+                    const uint32_t idx = cb + 32u * k + i;
+                    if (idx < n) {
+                        if (MODE == AG_MODE_DD) {
+                            neg |= dd_neg(v);
+                            v = fabsf(v);
+                        }
+                        s = idx == 0 ? v : __fadd_rn(s, v);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                a[k] = b[k];
+                b[k] = c[k];
+            }
+        }
+        return s;
+    }
+
     /* stream-order sum of in-edges [eb, ee) on one warp: stage AG_WCAP
      * values at a time, lane 0 adds them one by one (EXACT order) */
     __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
@@ -688,8 +764,46 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             }
             __syncwarp();
             pf = pn;
+        } else if (EXACT) {
+            /* hub chunk, EXACT order: the chunk's values go to the staging
+             * array at their place in the row; the row's last chunk to arrive
+             * sums the whole row in stream order */
+            const uint32_t pbase = task.y & AG_SLOT_MASK, chunk = task.y >> AG_SLOT_BITS;
+            const uint32_t o0 = eb - chunk * p.whub;
+            float *row_vals = p.hub_vals + (size_t)pbase * p.whub;
+            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            ps.stage_global(row_vals, o0, eb, ee, lane, pf);
+            __threadfence();
+            __syncwarp();
+            uint32_t last = 0;
+            const uint32_t deg = p.row_off[r0 + 1] - o0;
+            if (lane == 0) {
+                const uint32_t nch = (deg + p.whub - 1) / p.whub;
+                last = atomicAdd(&p.hub_cnt[pbase], 1u) == nch - 1 ? 1u : 0u;
+            }
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                uint32_t neg = 0;
+                const float tot = ps.ordered_chain(row_vals, deg, lane, neg);
+                if (lane == 0) {
+                    p.hub_cnt[pbase] = 0;
+                    float rp = 0.0f;
+                    uint32_t od = 0;
+                    if (MODE != AG_MODE_SPMV) {
+                        rp = p.rank[r0];
+                        od = p.outdeg[r0];
+                    }
+                    if (MODE == AG_MODE_DD)
+                        ps.finish_dd(r0, tot, rp, od, ps.dd_all || neg);
+                    else
+                        ps.finish(r0, tot, rp, od);
+                }
+            }
+            __syncwarp();
+            pf = pn;
         } else {
-            /* hub chunk (FAST order only) */
+            /* hub chunk, FAST order: chunk partials, added in chunk order */
             const uint32_t pbase = task.y & AG_SLOT_MASK, chunk = task.y >> AG_SLOT_BITS;
             uint32_t deg = 0;
             if (lane == 0)

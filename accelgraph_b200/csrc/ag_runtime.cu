@@ -358,6 +358,7 @@ struct ag_graph_s
     uint16_t *c16[2];
     float *hub_part;
     uint32_t *hub_cnt;
+    float *hub_vals; /* EXACT order: staged values of hub rows */
     AgControl *ctl;
     float *init_buf;
     uint32_t *flag;
@@ -490,6 +491,7 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->c16[1]);
     dev_free(g->hub_part);
     dev_free(g->hub_cnt);
+    dev_free(g->hub_vals);
     dev_free(g->ctl);
     dev_free(g->init_buf);
     dev_free(g->flag);
@@ -504,9 +506,10 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
 }
 
 /* Work lists of the fused pull kernel (one item per warp), planned on the
- * device from the device row offsets (ag_plan.cu).  FAST order: rows longer
- * than `cap` in-edges run on their own warp, rows longer than `whub` are split
- * into whub-edge chunks; EXACT order keeps every long row on one warp.  Other
+ * device from the device row offsets (ag_plan.cu).  Rows longer than `cap`
+ * in-edges run on their own warp, rows longer than `whub` are split into
+ * whub-edge chunks (in EXACT order the chunks stage their values and the last
+ * one sums the row in stream order).  Other
  * rows are packed into items of <= AG_WROWS consecutive rows holding <= cap
  * in-edges.  Heavy items come first so that they start early.  On success the
  * lists replace the graph's current ones. */
@@ -537,11 +540,14 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
         ag_plan_release(&ps, s);
         return ag_set_error(AG_ERR_UNSUPPORTED, "%u hub chunks exceed the hub split limits", tot[0]);
     }
-    const uint32_t nf = tot[0] + tot[1] + tot[2], ne = tot[1] + tot[3] + tot[2];
+    const uint32_t nf = tot[0] + tot[1] + tot[2], ne = nf;
     uint4 *tdf = (uint4 *)dev_alloc(g, (size_t)nf * sizeof(uint4), &st);
     uint4 *tde = (uint4 *)dev_alloc(g, (size_t)ne * sizeof(uint4), &st);
     float *hp = (float *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
     uint32_t *hc = (uint32_t *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
+    /* EXACT order stages a hub row's gathered values here (chunk slot x
+     * chunk size + offset in the row) before summing them in stream order */
+    float *hv = (float *)dev_alloc(g, (size_t)tot[0] * whub * 4 + 16, &st);
     if (st == AG_OK) {
         e = ag_plan_write(&ps, tot, tdf, tde, s);
         if (e == cudaSuccess)
@@ -557,16 +563,19 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
         dev_free(tde);
         dev_free(hp);
         dev_free(hc);
+        dev_free(hv);
         return st;
     }
     dev_free(g->tasks_fast);
     dev_free(g->tasks_exact);
     dev_free(g->hub_part);
     dev_free(g->hub_cnt);
+    dev_free(g->hub_vals);
     g->tasks_fast = tdf;
     g->tasks_exact = tde;
     g->hub_part = hp;
     g->hub_cnt = hc;
+    g->hub_vals = hv;
     g->ntasks_fast = nf;
     g->ntasks_exact = ne;
     g->nparts = tot[0];
@@ -992,6 +1001,7 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.c16_1 = g->c16[1];
     p.hub_part = g->hub_part;
     p.hub_cnt = g->hub_cnt;
+    p.hub_vals = g->hub_vals;
     p.ctl = g->ctl;
     p.init_ranks = g->init_buf;
     p.perm = g->perm;
