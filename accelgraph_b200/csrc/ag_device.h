@@ -43,6 +43,14 @@
                              order: the chunks stage their values and the
                              last one sums the row in stream order)         */
 #endif
+#ifndef AG_STEAL_MIN
+#define AG_STEAL_MIN 32768 /* EXACT order: the warp that sums a hub row of at
+                              least this many in-edges gives the rest of its
+                              work list away to warps that run out of work */
+#endif
+#define AG_STEAL_CAP 256  /* donors per pass                                 */
+#define AG_STEAL_PROBES 8 /* donor entries a warp out of work tries          */
+#define AG_STEAL_WORDS (2 + 2 * AG_STEAL_CAP)
 #define AG_STAGE_BYTES (AG_WARPS * AG_WCAP * 4)
 #if AG_CTAS_PER_SM == 1
 #define AG_SMEM_MAX 232448 /* shared memory per CTA: the 227 KB maximum     */
@@ -157,6 +165,11 @@ typedef struct AgPullParams
     uint32_t *hub_cnt;
     float *hub_vals;       /* EXACT order: hub rows' gathered values, at chunk
                               slot x whub + offset in the row                  */
+    uint32_t *steal;       /* EXACT order, AG_STEAL_WORDS words: [0] donors
+                              of this pass, [1] warps done with their items,
+                              then per donor its first given item + 1 (0: not
+                              yet published) and its claim counter; the last
+                              warp done resets them                           */
     AgControl *ctl;
     const AgRunConfig *cfg;
     const float *init_ranks;

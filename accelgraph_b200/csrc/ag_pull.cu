@@ -547,6 +547,57 @@ struct AgPass
 
 extern __shared__ __align__(128) unsigned char ag_dsmem[];
 
+/* EXACT-order work sharing.  A warp that sums a long hub row in stream order
+ * would still own every nwarps-th item after it, and the pass would wait for
+ * it.  So before the sum it publishes the rest of its stride as a donor
+ * entry; warps that have run out of items claim them one at a time with an
+ * atomic counter, and so does the donor once its sum is done.  State lives
+ * in lane 0 of each warp. */
+struct AgSteal
+{
+    int donor = -1;        /* this warp's donor entry                        */
+    bool stealing = false; /* the warp's own stride is used up               */
+    uint32_t probe = 0;    /* donor entries found empty so far               */
+};
+
+/* item k of donor d (nwarps apart), or ntasks once the entry is used up */
+static __device__ __forceinline__ uint32_t ag_steal_claim(uint32_t *steal, uint32_t d, uint32_t nwarps,
+                                                          uint32_t ntasks)
+{
+    volatile uint32_t *vs = steal;
+    const uint32_t b1 = vs[2 + 2 * d], k = vs[3 + 2 * d];
+    if (b1 == 0 || (uint64_t)(b1 - 1u) + (uint64_t)k * nwarps >= ntasks)
+        return ntasks;
+    const uint64_t item = (b1 - 1u) + (uint64_t)atomicAdd(steal + 3 + 2 * d, 1u) * nwarps;
+    return item < ntasks ? (uint32_t)item : ntasks;
+}
+
+/* the item after t for warp w (lane 0): its own stride, then its donor
+ * entry, then other donors' entries (at most AG_STEAL_PROBES of them,
+ * starting at one picked by w); ntasks when there is none */
+static __device__ __forceinline__ uint32_t ag_steal_next(uint32_t *steal, AgSteal &st, uint32_t t, uint32_t w,
+                                                         uint32_t nwarps, uint32_t ntasks)
+{
+    if (st.donor >= 0) {
+        const uint32_t it = ag_steal_claim(steal, (uint32_t)st.donor, nwarps, ntasks);
+        if (it < ntasks)
+            return it;
+        st.donor = -1;
+        st.stealing = true;
+    } else if (!st.stealing) {
+        if ((uint64_t)t + nwarps < ntasks)
+            return t + nwarps;
+        st.stealing = true;
+    }
+    const uint32_t n = min(*((volatile uint32_t *)steal), (uint32_t)AG_STEAL_CAP);
+    for (; st.probe < min(n, (uint32_t)AG_STEAL_PROBES); ++st.probe) {
+        const uint32_t it = ag_steal_claim(steal, (w + st.probe) % n, nwarps, ntasks);
+        if (it < ntasks)
+            return it;
+    }
+    return ntasks;
+}
+
 template <int MODE, int PREC, bool EXACT>
 __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const AgPullParams p)
 {
@@ -598,8 +649,14 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
     uint32_t t = blockIdx.x * AG_WARPS + warp;
     uint4 task = t < p.ntasks ? p.tasks[t] : make_uint4(0, 0, 0, 0);
     typename AgPass<MODE, PREC, EXACT>::Pair pf = ps.prefetch(task.z, task.w, lane);
+    AgSteal steal;
     while (t < p.ntasks) {
-        const uint32_t tn = t + nwarps;
+        uint32_t tn = t + nwarps;
+        if (EXACT) {
+            if (lane == 0)
+                tn = ag_steal_next(p.steal, steal, t, blockIdx.x * AG_WARPS + warp, nwarps, p.ntasks);
+            tn = __shfl_sync(0xffffffffu, tn, 0);
+        }
         const uint4 task_n = tn < p.ntasks ? p.tasks[tn] : make_uint4(0, 0, 0, 0);
         const uint32_t kind = task.x >> 30;
         const uint32_t r0 = task.x & AG_ROW_MASK;
@@ -784,6 +841,17 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             last = __shfl_sync(0xffffffffu, last, 0);
             if (last) {
                 __threadfence();
+                if (lane == 0 && deg >= AG_STEAL_MIN && steal.donor < 0 && !steal.stealing &&
+                    (uint64_t)tn + nwarps < p.ntasks) {
+                    /* give away the items after the next one */
+                    const uint32_t d = atomicAdd(p.steal, 1u);
+                    if (d < AG_STEAL_CAP) {
+                        p.steal[3 + 2 * d] = 0;
+                        __threadfence();
+                        atomicExch(p.steal + 2 + 2 * d, tn + nwarps + 1u);
+                        steal.donor = (int)d;
+                    }
+                }
                 uint32_t neg = 0;
                 const float tot = ps.ordered_chain(row_vals, deg, lane, neg);
                 if (lane == 0) {
@@ -866,6 +934,19 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         }
         task = task_n;
         t = tn;
+    }
+
+    if (EXACT && lane == 0) {
+        /* the last warp out clears the donor table for the next pass */
+        __threadfence();
+        if (atomicAdd(p.steal + 1, 1u) == nwarps - 1) {
+            const uint32_t n = min(*((volatile uint32_t *)p.steal), (uint32_t)AG_STEAL_CAP);
+            for (uint32_t d = 0; d < n; ++d)
+                p.steal[2 + 2 * d] = 0;
+            p.steal[0] = 0;
+            p.steal[1] = 0;
+            __threadfence();
+        }
     }
 
     if (MODE == AG_MODE_SPMV)

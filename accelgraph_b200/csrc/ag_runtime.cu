@@ -544,14 +544,16 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
     uint4 *tdf = (uint4 *)dev_alloc(g, (size_t)nf * sizeof(uint4), &st);
     uint4 *tde = (uint4 *)dev_alloc(g, (size_t)ne * sizeof(uint4), &st);
     float *hp = (float *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
-    uint32_t *hc = (uint32_t *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
+    /* hub arrival counters, then the EXACT order's donor table */
+    const size_t hc_bytes = ((size_t)tot[0] + 4 + AG_STEAL_WORDS) * 4;
+    uint32_t *hc = (uint32_t *)dev_alloc(g, hc_bytes, &st);
     /* EXACT order stages a hub row's gathered values here (chunk slot x
      * chunk size + offset in the row) before summing them in stream order */
     float *hv = (float *)dev_alloc(g, (size_t)tot[0] * whub * 4 + 16, &st);
     if (st == AG_OK) {
         e = ag_plan_write(&ps, tot, tdf, tde, s);
         if (e == cudaSuccess)
-            e = cudaMemsetAsync(hc, 0, (size_t)tot[0] * 4 + 16, s);
+            e = cudaMemsetAsync(hc, 0, hc_bytes, s);
         if (e != cudaSuccess) {
             cudaGetLastError();
             st = ag_set_error(AG_ERR_CUDA, "work-list planning failed: %s", cudaGetErrorString(e));
@@ -1002,6 +1004,7 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.hub_part = g->hub_part;
     p.hub_cnt = g->hub_cnt;
     p.hub_vals = g->hub_vals;
+    p.steal = g->hub_cnt + g->nparts + 4;
     p.ctl = g->ctl;
     p.init_ranks = g->init_buf;
     p.perm = g->perm;

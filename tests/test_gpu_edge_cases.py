@@ -71,6 +71,74 @@ def test_one_huge_hub_row(gpu, oracle):
         assert _rel(r, r64) <= _rel(ref["ranks"], r64) + 1e-6, dd
 
 
+def test_exact_order_hub_rows_give_their_work_away(gpu, oracle):
+    """Four hub rows of 9,000 to 150,000 in-edges among 600,000 short rows,
+    about four row items per warp.  A warp that sums a hub row of at least
+    32,768 in-edges in stream order gives the rest of its work list to warps
+    that run out of items.  Every row is still summed once, in stream order,
+    so EXACT PageRank over many passes (the donor table is cleared between
+    passes) and an EXACT weighted product equal the oracle bit for bit."""
+    ag = gpu
+    n = 600_000
+    rng = np.random.default_rng(21)
+    src, dst = [rng.integers(0, n, 6 * n)], [rng.integers(0, n, 6 * n)]
+    for v, d in ((7, 150_000), (70_000, 40_000), (300_001, 9_000), (599_999, 20_000)):
+        src.append(rng.choice(n, size=d, replace=False))
+        dst.append(np.full(d, v))
+    src = np.concatenate(src).astype(np.uint32)
+    dst = np.concatenate(dst).astype(np.uint32)
+    w = rng.random(src.size, dtype=np.float32)
+    g = ag.Graph.from_edges(n, src, dst, w, ag.AG_BUILD_DEDUPE)
+    assert np.sort(g.in_degree())[-2] >= 32768
+    dg = ag.DeviceGraph(g, weights=True)
+    assert dg.tasks(True).shape[0] > 2 * 148 * 32
+    ref = _pull(oracle, g, 40, 1e-9)
+    r, res, _ = dg.pagerank(40, 1e-9, order=ag.AG_ORDER_EXACT)
+    assert res.iterations == ref["iterations"] and np.array_equal(r.view(np.uint32), ref["ranks"].view(np.uint32))
+    x = np.empty(n, np.float32)
+    ag.lib.ag_fill_uniform(x.ctypes.data_as(ag.f32p), n, 27491095 + 3)
+    yo = oracle.spmv_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.in_weights(), x)
+    for _ in range(3):
+        assert np.array_equal(dg.spmv(x, mode=ag.AG_SPMV_EXACT).view(np.uint32), yo.view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["mixed_signs", "ties", "magnitudes", "infinity"])
+def test_exact_order_sum_of_hard_values(gpu, oracle, kind):
+    """The EXACT order sums a row by integer steps in the last place of the
+    running sum and falls back to a binary32 add where a step leaves the
+    binade, rounds a tie, or meets a zero, tiny, huge or infinite sum.  Values
+    chosen to hit every case (signs that cancel, multiples of 1/8 that make
+    ties, magnitudes from 2^-140 to 1e30, +inf), on rows of 40 to 20,000
+    in-edges (per-lane sums, warp sums of row items, long rows and hub rows):
+    the unit-weight product equals the one-by-one binary32 sum bit for bit."""
+    ag = gpu
+    rng = np.random.default_rng(33)
+    n = 30_000
+    src, dst = [rng.integers(0, n, 4 * n)], [rng.integers(0, n, 4 * n)]
+    for v, d in enumerate((40, 100, 256, 300, 1000, 2048, 2100, 5000, 20_000, 33)):
+        src.append(rng.choice(n, size=d, replace=False))
+        dst.append(np.full(d, v))
+    g = ag.Graph.from_edges(n, np.concatenate(src).astype(np.uint32), np.concatenate(dst).astype(np.uint32), None,
+                            ag.AG_BUILD_DEDUPE)
+    if kind == "mixed_signs":
+        x = rng.uniform(-1, 1, n)
+    elif kind == "ties":
+        x = rng.integers(-8, 9, n) * 0.125
+        x[::5] = 2.0 ** rng.integers(-30, 10, x[::5].size)
+    elif kind == "magnitudes":
+        x = rng.standard_normal(n) * 10.0 ** rng.integers(-30, 31, n)
+        x[::11] = 2.0 ** -140
+        x[::13] = 0.0
+    else:
+        x = rng.random(n)
+        x[rng.integers(0, n, 40)] = np.inf
+    x = x.astype(np.float32)
+    y = ag.DeviceGraph(g).spmv(x, mode=ag.AG_SPMV_UNIT | ag.AG_SPMV_EXACT)
+    yo = oracle.gather(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), x)
+    assert not np.isnan(yo).any()
+    assert np.array_equal(y.view(np.uint32), yo.view(np.uint32))
+
+
 def test_dangling_vertices_and_row_item_limits(gpu, oracle):
     """Rows of exactly 256 and 257 in-edges (the row-item limit and the first
     long row), 32 and 33 (the per-lane stream-order limit), and vertices with
