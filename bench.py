@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--epsilon", type=float, default=1e-6)
     p.add_argument("--iterations", type=int, default=300)
     p.add_argument("--precision", type=int, default=0)
+    p.add_argument("--order", default="fast", choices=["fast", "exact"],
+                   help="pagerank: summation order (exact = the reference loop's, bit for bit)")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
@@ -110,6 +112,7 @@ def workload_config(a, world):
         "epsilon": a.epsilon,
         "iteration_cap": a.iterations,
         "precision": ["fp32", "bf16", "fp16"][a.precision],
+        "order": a.order,
         "l2": "inputs larger than L2 (neighbour ids 4E bytes > 126 MB)",
         "parallelism": f"replicas{world}" if world > 1 else "single",
     }
@@ -255,8 +258,9 @@ def run_b200(a):
     info = dg.info()
 
     # -------- device-resident solves (value)
+    order = ag.AG_ORDER_EXACT if a.order == "exact" else ag.AG_ORDER_FAST
     for _ in range(a.warmup):
-        dg.launch(a.iterations, a.epsilon, precision=a.precision)
+        dg.launch(a.iterations, a.epsilon, precision=a.precision, order=order)
     ranks_w, res_w, _ = dg.fetch()
     barrier()
     torch.cuda.synchronize()
@@ -265,7 +269,7 @@ def run_b200(a):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(a.steps):
-        dg.launch(a.iterations, a.epsilon, precision=a.precision)
+        dg.launch(a.iterations, a.epsilon, precision=a.precision, order=order)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
@@ -287,14 +291,14 @@ def run_b200(a):
     dev_pass = np.diff(np.concatenate([[0.0], np.cumsum(hist["seconds"])]))
     achieved = alg_bytes / pass_s / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_kind": peak_kind, "kernel": "ag_pull_kernel<PR,fp32,fast>",
+            "traffic": None, "peak_kind": peak_kind, "kernel": "ag_pull_kernel<PR,fp32,%s>" % a.order,
             "bytes_per_pass": alg_bytes, "pass_us": pass_s * 1e6,
             "pass_us_device_timer_median": float(np.median(dev_pass[1:]) * 1e6) if len(dev_pass) > 1 else None}
-    roof["traffic"] = profiled_traffic(a.scale, a.edge_factor)
+    roof["traffic"] = profiled_traffic(a.scale, a.edge_factor) if a.order == "fast" else None
 
     # -------- end to end through the C ABI (host buffers, pinned)
     args = ag.default_arguments(a.iterations, a.epsilon)
-    opts = ag.make_opts(precision=a.precision, quiet=True)
+    opts = ag.make_opts(precision=a.precision, order=order, quiet=True)
     out = C.POINTER(ag.PageRankStats)()
     ag.check(ag.lib.ag_pagerank_pull_ex(C.byref(args), g.ptr, C.byref(opts), C.byref(out)), "e2e warmup")
     ag.lib.freePageRankStats(out)
