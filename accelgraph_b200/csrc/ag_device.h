@@ -12,7 +12,9 @@
  *   c32[2][N]      float   contribution ping-pong buffers
  *   c16[2][N]      16-bit  low-precision contribution buffers (precision form)
  *   hub_part[H]    float   per-chunk partial sums of split rows
- *   hub_cnt[H]     uint32  arrival counters of split rows
+ *   hub_cnt[H]     uint32  arrival counters of split rows, then 4 spare words
+ *                          and the EXACT order's donor table (AG_STEAL_WORDS)
+ *   hub_vals[H*C]  float   EXACT order: hub rows' gathered values (C = chunk)
  *   ctl            AgControl  iteration state read and written on the device
  */
 #ifndef AG_DEVICE_H
