@@ -104,13 +104,12 @@ def test_exact_order_hub_rows_give_their_work_away(gpu, oracle):
 
 @pytest.mark.parametrize("kind", ["mixed_signs", "ties", "magnitudes", "infinity"])
 def test_exact_order_sum_of_hard_values(gpu, oracle, kind):
-    """The EXACT order sums a row by integer steps in the last place of the
-    running sum and falls back to a binary32 add where a step leaves the
-    binade, rounds a tie, or meets a zero, tiny, huge or infinite sum.  Values
-    chosen to hit every case (signs that cancel, multiples of 1/8 that make
-    ties, magnitudes from 2^-140 to 1e30, +inf), on rows of 40 to 20,000
-    in-edges (per-lane sums, warp sums of row items, long rows and hub rows):
-    the unit-weight product equals the one-by-one binary32 sum bit for bit."""
+    """EXACT-order sums of values where binary32 rounding is delicate: signs
+    that cancel, multiples of 1/8 that round ties, magnitudes from 2^-140 to
+    1e30, and +inf.  Rows of 33 to 20,000 in-edges take every summation path
+    (per-lane sums in row items, long rows, hub rows whose chunks stage their
+    values for one warp's chain).  The unit-weight product equals the
+    one-by-one binary32 sum bit for bit."""
     ag = gpu
     rng = np.random.default_rng(33)
     n = 30_000
