@@ -45,6 +45,9 @@
                              order: the chunks stage their values and the
                              last one sums the row in stream order)         */
 #endif
+#if AG_WHUB % 32 != 0
+#error "AG_WHUB must be a multiple of 32 (EXACT-order hub rows are read in 16-byte groups)"
+#endif
 #ifndef AG_STEAL_MIN
 #define AG_STEAL_MIN 32768 /* EXACT order: the warp that sums a hub row of at
                               least this many in-edges gives the rest of its

@@ -137,6 +137,9 @@ __device__ __forceinline__ uint32_t ag_warp_sum_u(uint32_t v)
     return v;
 }
 
+/* EXACT order: the first values of a long sum added one by one */
+#define AG_XSTART 32u
+
 /* ------------------------------------------------------------- kernel */
 template <int MODE, int PREC, bool EXACT>
 struct AgPass
@@ -465,83 +468,518 @@ struct AgPass
         }
     }
 
-    /* EXACT-order hub row: the stream-order sum of its n staged values
-     * src[0, n) on one warp.  Every lane runs the same chain: value i of a
-     * 256-value block comes from the lane that loaded it by a shuffle, so the
-     * warp never diverges and nothing passes through shared memory; the two
-     * blocks after the current one are loading (from L2, coalesced) while it
-     * is added.  Elements past n are skipped by a warp-uniform test. */
-    __device__ __forceinline__ float ordered_chain(const float *src, uint32_t n, uint32_t lane, uint32_t &neg) const
+    /* ---------------------------------------------------------------
+     * EXACT order on one warp: the stream-order binary32 sum
+     * ((v0 + v1) + v2) + ... of a long sequence, bit for bit, without a
+     * serial chain of adds.
+     *
+     * While the running sum s is a positive normal number of biased exponent
+     * e, it is M * 2^(e-150) with an integer M in [2^23, 2^24).  The binary32
+     * add s + v rounds to M' = M + round(x), x = v / 2^(e-150), as long as the
+     * exact sum stays in the binade.  round() is to nearest, and on a tie
+     * (x = k + 1/2) to the even M', so the step is k + ((M + k) & 1): it
+     * depends on M only through M's parity.  Within a binade the adds are
+     * therefore integer adds, which associate, and a tie is a two-state map
+     * of the parity, which composes associatively too.
+     *
+     * A round is 256 consecutive values; lane L holds positions 8L .. 8L+7
+     * (`in` marks the ones that belong to the sum).  Three ways, tried in
+     * order, each exact:
+     *  - exact_fast: every value non-negative and finite, no tie, and M plus
+     *    the round's total still in the binade.  The steps are >= 0, so every
+     *    partial M is too: s moves by one warp-reduced integer total.
+     *  - exact_seg: a warp scan of binary32 prefix sums predicts where the
+     *    sum enters a new binade (and which values are at least half the sum
+     *    before them).  Those values are added with binary32 adds, one by
+     *    one; the runs between them are integer sums at their binade's unit,
+     *    ties included.  The prediction is only a guess: each run must keep
+     *    M in its binade, and each binary32 add must land in the binade the
+     *    next run was computed for, or the round falls through.
+     *  - exact_slow: a warp scan of the integer steps gives every partial M;
+     *    the first value that breaks a condition (leaves the binade either
+     *    way, is a tie, is huge or not finite, or s is zero, subnormal or not
+     *    finite) takes a binary32 add and the scan resumes after it.
+     * Values are the caller's: magnitudes with their sign tags taken off in
+     * data-driven passes. */
+
+    /* s rebuilt from its sign and exponent bits and M (M in [2^23, 2^24)) */
+    static __device__ __forceinline__ float exact_make(uint32_t sgn_ex, uint32_t m)
     {
-        float s = 0.0f;
-        float a[8], b[8];
-        auto load = [&](float *r, uint32_t cb) {
+        return __uint_as_float(sgn_ex | (m & 0x7fffffu));
+    }
+
+    /* 2^(150-e) for a biased exponent e in [24, 254] */
+    static __device__ __forceinline__ float exact_scale(uint32_t e) { return __uint_as_float((277u - e) << 23); }
+
+    static __device__ __forceinline__ bool exact_fast(float &s, const float (&v)[8], const bool (&in)[8])
+    {
+        const uint32_t sb = __float_as_uint(s);
+        const uint32_t ex = sb >> 23; /* sign bit included: positive s only */
+        if (ex < 24u || ex >= 255u)
+            return false;
+        const float scale = exact_scale(ex);
+        uint32_t t = 0;
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            /* negative values (sign bit set) are left to the other ways */
+            const float x = in[k] ? __fmul_rn(v[k], scale) : 0.0f;
+            /* bitwise ors: no short-circuit branches per value */
+            bad |= !(x < 4194304.0f) | (in[k] & ((__float_as_uint(v[k]) >> 31) != 0u)) |
+                   (__fsub_rn(x, floorf(x)) == 0.5f);
+            t += (uint32_t)__float2int_rn(x);
+        }
+        /* not bad: every step is below 2^22, the total below 2^30 */
+        t = __reduce_add_sync(0xffffffffu, t);
+        const uint32_t m = ((sb & 0x7fffffu) | 0x800000u) + t;
+        if (__any_sync(0xffffffffu, bad) || m >= (1u << 24))
+            return false;
+        s = exact_make(ex << 23, m);
+        return true;
+    }
+
+    /* the parity map of a run: a[p] = its total step when M starts with
+     * parity p; (0, 0) is the empty run */
+    struct XMap
+    {
+        uint32_t a0, a1;
+    };
+
+    /* run x then run y */
+    static __device__ __forceinline__ XMap exact_compose(XMap x, XMap y)
+    {
+        XMap r;
+        r.a0 = x.a0 + ((x.a0 & 1u) ? y.a1 : y.a0);
+        r.a1 = x.a1 + ((x.a1 & 1u) ? y.a0 : y.a1);
+        return r;
+    }
+
+    /* the parity map of the whole warp's run of group g, in lane order */
+    static __device__ __forceinline__ XMap exact_warp_map(XMap m, uint32_t lane)
+    {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            XMap y;
+            y.a0 = __shfl_down_sync(0xffffffffu, m.a0, o);
+            y.a1 = __shfl_down_sync(0xffffffffu, m.a1, o);
+            if ((lane & (2u * o - 1u)) == 0)
+                m = exact_compose(m, y);
+        }
+        m.a0 = __shfl_sync(0xffffffffu, m.a0, 0);
+        m.a1 = __shfl_sync(0xffffffffu, m.a1, 0);
+        return m;
+    }
+
+    /* returned by exact_seg when it does not apply */
+    static __device__ __forceinline__ float exact_none() { return __uint_as_float(0x7fffffffu); }
+    static __device__ __forceinline__ bool exact_is_none(float s) { return __float_as_uint(s) == 0x7fffffffu; }
+
+    /* values and the `in` mask (bit k) by value: nothing goes through local
+     * memory at the call */
+    static __device__ __noinline__ float exact_seg(float s, float v0, float v1, float v2, float v3, float v4,
+                                                   float v5, float v6, float v7, uint32_t inm, uint32_t lane)
+    {
+        const float v[8] = {v0, v1, v2, v3, v4, v5, v6, v7};
+        bool in[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            in[k] = (inm >> k) & 1u;
+        if ((__float_as_uint(s) >> 23) < 24u || (__float_as_uint(s) >> 23) >= 255u)
+            return exact_none();
+        /* binary32 prefix sums: inclusive within the lane, then across lanes */
+        float loc[8];
+        float acc = 0.0f;
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            /* values must be non-negative and finite (+0 and -0 included) */
+            bad |= in[k] & !((v[k] >= 0.0f) & (v[k] < __int_as_float(0x7f800000)));
+            acc = __fadd_rn(acc, in[k] ? v[k] : 0.0f);
+            loc[k] = acc;
+        }
+        if (__any_sync(0xffffffffu, bad))
+            return exact_none();
+        float inc = acc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float y = __shfl_up_sync(0xffffffffu, inc, o);
+            if ((int)lane >= o)
+                inc = __fadd_rn(inc, y);
+        }
+        float excl = __shfl_up_sync(0xffffffffu, inc, 1);
+        if (lane == 0)
+            excl = 0.0f;
+        /* per value: the binade of the sum before and after it (predicted),
+         * whether it is added one by one, and its step */
+        uint32_t cnt = 0, ebin[8], eaft[8];
+        bool cross[8], tie[8];
+        uint32_t r[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float before = __fadd_rn(s, __fadd_rn(excl, k ? loc[k - 1] : 0.0f));
+            const float after = __fadd_rn(s, __fadd_rn(excl, loc[k]));
+            ebin[k] = __float_as_uint(before) >> 23;
+            eaft[k] = __float_as_uint(after) >> 23;
+            bad |= in[k] & (eaft[k] >= 255u);
+            const float x = __fmul_rn(v[k], exact_scale(min(ebin[k], 254u)));
+            const float fl = floorf(x);
+            const float fr = __fsub_rn(x, fl);
+            cross[k] = in[k] & ((eaft[k] != ebin[k]) | !(x < 4194304.0f));
+            tie[k] = in[k] & !cross[k] & (fr == 0.5f);
+            r[k] = (in[k] & !cross[k]) ? (uint32_t)__float2int_rz(fl) + (fr > 0.5f ? 1u : 0u) : 0u;
+            cnt += cross[k] ? 1u : 0u;
+        }
+        if (__any_sync(0xffffffffu, bad))
+            return exact_none();
+        /* group of each value: the one-by-one values before it (all lanes) */
+        uint32_t cinc = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, cinc, o);
+            if ((int)lane >= o)
+                cinc += y;
+        }
+        const uint32_t ncross = __shfl_sync(0xffffffffu, cinc, 31);
+        const uint32_t cbase = cinc - cnt;
+        const bool anytie = __any_sync(0xffffffffu, tie[0] | tie[1] | tie[2] | tie[3] | tie[4] | tie[5] | tie[6] |
+                                                        tie[7]);
+        uint32_t sb = __float_as_uint(s);
+        uint32_t ex = sb >> 23;
+        uint32_t m = (sb & 0x7fffffu) | 0x800000u;
+        for (uint32_t g = 0;; ++g) {
+            /* the run of group g, at binade ex */
+            uint32_t grp = cbase;
+            XMap mp = {0u, 0u};
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const uint32_t j = cb + lane + 32u * k;
-                r[k] = j < n ? __ldcg(src + j) : 0.0f;
+                /* selects, not branches: the lane's values of this run */
+                const bool take = (grp == g) & in[k] & !cross[k];
+                XMap e;
+                /* a tie's step is k + ((M + k) & 1), with r[k] = k */
+                e.a0 = take ? (tie[k] ? r[k] + (r[k] & 1u) : r[k]) : 0u;
+                e.a1 = take ? (tie[k] ? r[k] + ((r[k] + 1u) & 1u) : r[k]) : 0u;
+                bad |= take & (ebin[k] != ex);
+                if (anytie)
+                    mp = exact_compose(mp, e);
+                else
+                    mp.a0 += e.a0;
+                grp += cross[k] ? 1u : 0u;
             }
-        };
-        load(a, 0);
-        load(b, 256u);
-        for (uint32_t cb = 0; cb < n; cb += 256u) {
-            float c[8];
-            if (cb + 512u < n)
-                load(c, cb + 512u);
+            if (anytie)
+                mp = exact_warp_map(mp, lane);
+            else
+                mp.a0 = __reduce_add_sync(0xffffffffu, mp.a0);
+            if (__any_sync(0xffffffffu, bad))
+                return exact_none();
+            m += (anytie & ((m & 1u) != 0u)) ? mp.a1 : mp.a0;
+            if (m >= (1u << 24))
+                return exact_none();
+            s = exact_make(ex << 23, m);
+            if (g == ncross)
+                break;
+            /* the one-by-one value that ends group g */
+            grp = cbase;
+            float xv = 0.0f;
+            uint32_t xe = 0;
+            bool mine = false;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    float v = __shfl_sync(0xffffffffu, a[k], i);
-                    const uint32_t idx = cb + 32u * k + i;
-                    if (idx < n) {
-                        if (MODE == AG_MODE_DD) {
-                            neg |= dd_neg(v);
-                            v = fabsf(v);
-                        }
-                        s = idx == 0 ? v : __fadd_rn(s, v);
-                    }
-                }
+                const bool here = cross[k] & (grp == g);
+                xv = here ? v[k] : xv;
+                xe = here ? eaft[k] : xe;
+                mine |= here;
+                grp += cross[k] ? 1u : 0u;
             }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                a[k] = b[k];
-                b[k] = c[k];
-            }
+            const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
+            xv = __shfl_sync(0xffffffffu, xv, src);
+            xe = __shfl_sync(0xffffffffu, xe, src);
+            s = __fadd_rn(s, xv);
+            sb = __float_as_uint(s);
+            ex = sb >> 23;
+            if (ex != xe)
+                return exact_none();
+            m = (sb & 0x7fffffu) | 0x800000u;
         }
         return s;
     }
 
-    /* stream-order sum of in-edges [eb, ee) on one warp: stage AG_WCAP
-     * values at a time, lane 0 adds them one by one (EXACT order) */
-    __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
-                                                 uint32_t &neg) const
+    /* general way: adds, in position order, the lane's values v[k]
+     * (position 8 * lane + k) that have in[k] set */
+    static __device__ __noinline__ float exact_slow(float s, float v0, float v1, float v2, float v3, float v4,
+                                                    float v5, float v6, float v7, uint32_t inm, uint32_t lane)
+    {
+        const float v[8] = {v0, v1, v2, v3, v4, v5, v6, v7};
+        bool in[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            in[k] = (inm >> k) & 1u;
+        uint32_t cur = 0;
+        for (;;) {
+            bool ok[8], rem = false;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                ok[k] = in[k] & (8u * lane + k >= cur);
+                rem |= ok[k];
+            }
+            const unsigned rm = __ballot_sync(0xffffffffu, rem);
+            if (!rm)
+                return s;
+            const uint32_t sb = __float_as_uint(s);
+            const uint32_t ex = (sb >> 23) & 0xffu;
+            if (ex < 24u || ex == 255u) {
+                /* zero, tiny or not finite: one binary32 add of the first
+                 * remaining value */
+                const int src = __ffs(rm) - 1;
+                float x = 0.0f;
+                uint32_t fk = 8;
+#pragma unroll
+                for (int k = 7; k >= 0; --k)
+                    if (ok[k]) {
+                        x = v[k];
+                        fk = k;
+                    }
+                x = __shfl_sync(0xffffffffu, x, src);
+                fk = __shfl_sync(0xffffffffu, fk, src);
+                s = __fadd_rn(s, x);
+                cur = 8u * src + fk + 1u;
+                continue;
+            }
+            const uint32_t sgn = sb & 0x80000000u;
+            /* +-2^(150-e): values in units of s's last place, s's sign folded in */
+            const float scale = __uint_as_float(sgn | ((277u - ex) << 23));
+            const int m0 = (int)((sb & 0x7fffffu) | 0x800000u);
+            int r[8];
+            bool up[8], bad[8];
+            int t = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float x = ok[k] ? __fmul_rn(v[k], scale) : 0.0f;
+                const float fl = floorf(x);
+                const float fr = __fsub_rn(x, fl);
+                bad[k] = !(fabsf(x) < 4194304.0f) | (fr == 0.5f);
+                up[k] = fr > 0.5f;
+                r[k] = bad[k] ? 0 : __float2int_rz(fl) + (up[k] ? 1 : 0);
+                t += r[k];
+            }
+            int inc = t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                if ((int)lane >= o)
+                    inc += y;
+            }
+            /* M before each value; a value is out when it is bad, when the sum
+             * before it plus its floor falls below the binade, or when its
+             * rounded sum reaches the next binade */
+            int mj = m0 + inc - t, mb = mj;
+            uint32_t fk = 8;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int mn = mj + r[k];
+                const bool out = ok[k] & (bad[k] | (mn - (up[k] ? 1 : 0) < (1 << 23)) | (mn >= (1 << 24)));
+                if (out && fk == 8) {
+                    fk = k;
+                    mb = mj;
+                }
+                mj = mn;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, fk != 8);
+            if (!bal) {
+                const int mend = __shfl_sync(0xffffffffu, m0 + inc, 31);
+                return exact_make(sgn | (ex << 23), (uint32_t)mend);
+            }
+            const int src = __ffs(bal) - 1;
+            float x = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if ((uint32_t)k == fk)
+                    x = v[k];
+            x = __shfl_sync(0xffffffffu, x, src);
+            fk = __shfl_sync(0xffffffffu, fk, src);
+            mb = __shfl_sync(0xffffffffu, mb, src);
+            s = __fadd_rn(exact_make(sgn | (ex << 23), (uint32_t)mb), x);
+            cur = 8u * src + fk + 1u;
+        }
+    }
+
+    /* one round added to s (see above) */
+    static __device__ __forceinline__ float exact_round(float s, const float (&v)[8], const bool (&in)[8],
+                                                        uint32_t lane)
+    {
+        if (exact_fast(s, v, in))
+            return s;
+        uint32_t inm = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            inm |= in[k] ? 1u << k : 0u;
+        const float r = exact_seg(s, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], inm, lane);
+        if (!exact_is_none(r))
+            return r;
+        return exact_slow(s, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], inm, lane);
+    }
+
+    /* the start of a sequence: s = its first value plus the next ones, one by
+     * one, up to `cnt` (<= AG_XSTART) values (positions 0 .. cnt-1, held by
+     * lanes 0 .. 3), which then leave the round.  There the values are as
+     * large as the sum and the binade changes at almost every add. */
+    static __device__ __forceinline__ float exact_start(const float (&v)[8], bool (&in)[8], uint32_t cnt,
+                                                        uint32_t lane)
     {
         float s = 0.0f;
-        for (uint32_t cb = eb; cb < ee; cb += AG_WCAP) {
-            const uint32_t ce = min(ee, cb + (uint32_t)AG_WCAP);
-            stage(vals, cb, ce, lane, prefetch(cb, ce, lane));
-            __syncwarp();
-            if (lane == 0) {
-                uint32_t j = 0;
-                if (cb == eb) {
-                    s = vals[0];
-                    if (MODE == AG_MODE_DD) {
-                        neg |= dd_neg(s);
-                        s = fabsf(s);
-                    }
-                    j = 1;
-                }
-                for (; j < ce - cb; ++j) {
-                    const float v = vals[j];
-                    if (MODE == AG_MODE_DD)
-                        neg |= dd_neg(v);
-                    s = __fadd_rn(s, MODE == AG_MODE_DD ? fabsf(v) : v);
-                }
+#pragma unroll
+        for (uint32_t q = 0; q < AG_XSTART; ++q) {
+            const float x = __shfl_sync(0xffffffffu, v[q & 7u], (int)(q >> 3));
+            if (q < cnt)
+                s = q == 0 ? x : __fadd_rn(s, x);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k)
+            if (8u * lane + k < cnt)
+                in[k] = false;
+        return s;
+    }
+
+    /* the caller's value of a gathered element: data-driven passes take the
+     * magnitude and OR the sign tag into `neg` */
+    __device__ __forceinline__ void exact_prep(float (&v)[8], const bool (&in)[8], uint32_t &neg) const
+    {
+        if (MODE == AG_MODE_DD) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (in[k])
+                    neg |= dd_neg(v[k]);
+                v[k] = fabsf(v[k]);
             }
-            __syncwarp();
+        }
+    }
+
+    /* one round of a hub row's chain: positions cb .. cb+255 of src */
+    __device__ __forceinline__ float chain_round(float s, float (&v)[8], uint32_t cb, uint32_t n, uint32_t lane,
+                                                 uint32_t &neg) const
+    {
+        bool in[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            in[k] = cb + 8u * lane + k < n;
+        exact_prep(v, in, neg);
+        if (cb == 0)
+            s = exact_start(v, in, min(n, AG_XSTART), lane);
+        return exact_round(s, v, in, lane);
+    }
+
+    /* EXACT-order hub row: the stream-order sum of its n staged values
+     * src[0, n) (16-byte aligned; the row's staging slots hold a multiple of
+     * 32 values, so a 16-byte group that starts below n ends inside them).
+     * Three rounds are loading (from L2, 16-byte loads) at any time: a
+     * buffer is refilled right after its round is added, and the rotation
+     * over the three is unrolled, so no register waits on a load to be
+     * copied. */
+    __device__ __noinline__ float ordered_chain(const float *src, uint32_t n, uint32_t lane, uint32_t &neg) const
+    {
+        float a[8], b[8], c[8];
+        auto load = [&](float (&r)[8], uint32_t cb) {
+            const uint32_t pa = cb + 8u * lane, pb = pa + 4u;
+            const float4 x = pa < n ? __ldcg(reinterpret_cast<const float4 *>(src + pa)) : make_float4(0, 0, 0, 0);
+            const float4 y = pb < n ? __ldcg(reinterpret_cast<const float4 *>(src + pb)) : make_float4(0, 0, 0, 0);
+            r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+            r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
+        };
+        load(a, 0);
+        load(b, 256u);
+        load(c, 512u);
+        float s = 0.0f;
+        for (uint32_t cb = 0;; cb += 768u) {
+            s = chain_round(s, a, cb, n, lane, neg);
+            if (cb + 768u < n)
+                load(a, cb + 768u);
+            if (cb + 256u >= n)
+                break;
+            s = chain_round(s, b, cb + 256u, n, lane, neg);
+            if (cb + 1024u < n)
+                load(b, cb + 1024u);
+            if (cb + 512u >= n)
+                break;
+            s = chain_round(s, c, cb + 512u, n, lane, neg);
+            if (cb + 1280u < n)
+                load(c, cb + 1280u);
+            if (cb + 768u >= n)
+                break;
         }
         return s;
+    }
+
+    /* the stream-order sum of vals[a, b) (the warp's shared-memory slice)
+     * by the calling lane alone, continuing s, or starting with vals[a] when
+     * `first`: four values per 16-byte shared load once the index is
+     * aligned, one binary32 add after another.  Data-driven passes add the
+     * magnitudes and OR the sign tags into `neg`. */
+    __device__ __forceinline__ float seq_sum(const float *vals, uint32_t a, uint32_t b, float s, bool first,
+                                             uint32_t &neg) const
+    {
+        auto val = [&](float v) {
+            if (MODE == AG_MODE_DD) {
+                neg |= dd_neg(v);
+                v = fabsf(v);
+            }
+            return v;
+        };
+        uint32_t j = a;
+        if (first && j < b) {
+            s = val(vals[j]);
+            ++j;
+        }
+        for (; j < b && (j & 3u); ++j)
+            s = __fadd_rn(s, val(vals[j]));
+        for (; j + 8u <= b; j += 8u) {
+            const float4 q0 = reinterpret_cast<const float4 *>(vals)[j >> 2];
+            const float4 q1 = reinterpret_cast<const float4 *>(vals)[(j >> 2) + 1];
+            s = __fadd_rn(s, val(q0.x));
+            s = __fadd_rn(s, val(q0.y));
+            s = __fadd_rn(s, val(q0.z));
+            s = __fadd_rn(s, val(q0.w));
+            s = __fadd_rn(s, val(q1.x));
+            s = __fadd_rn(s, val(q1.y));
+            s = __fadd_rn(s, val(q1.z));
+            s = __fadd_rn(s, val(q1.w));
+        }
+        for (; j < b; ++j)
+            s = __fadd_rn(s, val(vals[j]));
+        return s;
+    }
+
+    /* EXACT-order long row: the stream-order sum of in-edges [eb, ee) on one
+     * warp.  Rounds of 256 in-edges (after the first, each starting on a
+     * 16-byte group) are staged in the warp's shared-memory slice by the row
+     * items' stage (16-byte id loads, eight gathers in flight per lane);
+     * lane 0 adds a round one value after another while the next round's
+     * gathers travel.  Rows this short cross a binade in most rounds, where
+     * the integer way of the hub rows falls back to its slower forms; the
+     * lane's chain costs about 1.25 instructions per value.  `first` is the
+     * range's first id pair; the sum is lane 0's. */
+    __device__ __forceinline__ float ordered_sum(float *vals, uint32_t eb, uint32_t ee, uint32_t lane,
+                                                 const Pair &first, uint32_t &neg) const
+    {
+        uint32_t cb = eb, ce = min(ee, (eb & ~3u) + (uint32_t)AG_WCAP);
+        stage(vals, cb, ce, lane, first);
+        float s = 0.0f;
+        for (;;) {
+            __syncwarp();
+            const uint32_t nb = ce, ne = min(ee, ce + (uint32_t)AG_WCAP);
+            if (nb >= ee) {
+                if (lane == 0)
+                    s = seq_sum(vals, 0, ce - cb, s, cb == eb, neg);
+                return s;
+            }
+            /* the next round's gathers travel while this one is added */
+            float w[8];
+            stage_issue(prefetch(nb, ne, lane), nb, ne, lane, w);
+            if (lane == 0)
+                s = seq_sum(vals, 0, ce - cb, s, cb == eb, neg);
+            __syncwarp();
+            stage_commit(vals, nb, ne, lane, w);
+            cb = nb;
+            ce = ne;
+        }
     }
 };
 
@@ -702,7 +1140,9 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             float s = 0.0f;
             uint32_t neg = 0;
             bool is_long = false;
-            if (EXACT || o1 - o0 <= AG_TSEQ) {
+            if (EXACT) {
+                s = ps.seq_sum(vals, o0, o1, 0.0f, true, neg);
+            } else if (o1 - o0 <= AG_TSEQ) {
                 if (o1 > o0) {
                     float v = vals[o0];
                     neg = ps.dd_neg(v);
@@ -764,7 +1204,11 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             o1 -= eb;
             float s = 0.0f;
             bool is_long = false;
-            if (EXACT || o1 - o0 <= AG_TSEQ) {
+            if (EXACT) {
+                /* stream order, rows of any length: 16-byte shared loads */
+                uint32_t nn = 0;
+                s = ps.seq_sum(vals, o0, o1, 0.0f, true, nn);
+            } else if (o1 - o0 <= AG_TSEQ) {
                 /* stream order: the accumulator restarts with the first value
                  * and adds the rest one by one */
                 if (o1 > o0) {
@@ -807,7 +1251,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             float s;
             uint32_t neg = 0;
             if (EXACT) {
-                s = ps.ordered_sum(vals, eb, ee, lane, neg);
+                s = ps.ordered_sum(vals, eb, ee, lane, pf, neg);
             } else {
                 s = ps.strided_partial(eb, ee, lane, pf, neg);
                 s = ag_warp_sum_f(s);
@@ -854,6 +1298,8 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 }
                 uint32_t neg = 0;
                 const float tot = ps.ordered_chain(row_vals, deg, lane, neg);
+                /* each lane saw the sign tags of its own values */
+                neg = __any_sync(0xffffffffu, neg) ? 1u : 0u;
                 if (lane == 0) {
                     p.hub_cnt[pbase] = 0;
                     float rp = 0.0f;

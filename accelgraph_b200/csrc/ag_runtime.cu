@@ -1975,10 +1975,12 @@ extern "C" ag_status_t ag_graph_set_tiles(ag_graph_t g, const ag_tile_config *cf
     ag_clear_error();
     if (!g || !cfg)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_set_tiles: NULL argument");
+    /* hub_chunk is a multiple of 32: an EXACT-order hub row's staging slots
+     * then start on 16-byte boundaries and hold whole 16-byte groups */
     if (cfg->task_edges < 32 || cfg->task_edges > AG_WCAP || cfg->hub_chunk < cfg->task_edges ||
-        cfg->hub_chunk > (1u << 20))
-        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_set_tiles: task_edges in [32, %u], hub_chunk in "
-                            "[task_edges, 2^20]", AG_WCAP);
+        cfg->hub_chunk > (1u << 20) || cfg->hub_chunk % 32u != 0)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_graph_set_tiles: task_edges in [32, %u], hub_chunk a multiple "
+                            "of 32 in [task_edges, 2^20]", AG_WCAP);
     cudaStream_t s = g_ctx.stream;
     ag_status_t st = stream_wait(s, 0);
     if (st != AG_OK)
