@@ -15,6 +15,8 @@
  *   hub_cnt[H]     uint32  arrival counters of split rows, then 4 spare words
  *                          and the EXACT order's donor table (AG_STEAL_WORDS)
  *   hub_vals[H*C]  float   EXACT order: hub rows' gathered values (C = chunk)
+ *   hub_pred[H]    uint32  EXACT order: each chunk's starting binade, last pass
+ *   hub_t[H*64]    uint32  EXACT order: per-round integer step totals
  *   ctl            AgControl  iteration state read and written on the device
  */
 #ifndef AG_DEVICE_H
@@ -54,6 +56,13 @@
                               work list away to warps that run out of work */
 #endif
 #define AG_STEAL_CAP 256  /* donors per pass                                 */
+#define AG_XWORDS 64      /* EXACT order: words per hub chunk of integer step
+                             totals (two per 256-value round, the last word
+                             the chunk's data-driven sign tag)              */
+#define AG_XROUNDS 31     /* rounds of a chunk with step totals              */
+#define AG_XNOT 0x80000000u /* a round's total that does not apply          */
+#define AG_XFELL 0x100u   /* hub_pred: the chunk had a round summed one value
+                             after another in the pass before              */
 #define AG_STEAL_PROBES 8 /* donor entries a warp out of work tries          */
 #define AG_STEAL_WORDS (2 + 2 * AG_STEAL_CAP)
 #define AG_STAGE_BYTES (AG_WARPS * AG_WCAP * 4)
@@ -170,6 +179,14 @@ typedef struct AgPullParams
     uint32_t *hub_cnt;
     float *hub_vals;       /* EXACT order: hub rows' gathered values, at chunk
                               slot x whub + offset in the row                  */
+    uint32_t *hub_pred;    /* EXACT order, per hub chunk: the biased exponent
+                              of the row's stream-order sum where the chunk
+                              began in the pass before (0: unknown), and
+                              AG_XFELL                                         */
+    uint32_t *hub_t;       /* EXACT order, AG_XWORDS per hub chunk: for each
+                              round of 256 in-edges, the sum of its integer
+                              steps at that exponent and at the next one
+                              (AG_XNOT: does not apply)                        */
     uint32_t *steal;       /* EXACT order, AG_STEAL_WORDS words: [0] donors
                               of this pass, [1] warps done with their items,
                               then per donor its first given item + 1 (0: not

@@ -137,9 +137,6 @@ __device__ __forceinline__ uint32_t ag_warp_sum_u(uint32_t v)
     return v;
 }
 
-/* EXACT order: the first values of a long sum added one by one */
-#define AG_XSTART 32u
-
 /* ------------------------------------------------------------- kernel */
 template <int MODE, int PREC, bool EXACT>
 struct AgPass
@@ -469,443 +466,206 @@ struct AgPass
     }
 
     /* ---------------------------------------------------------------
-     * EXACT order on one warp: the stream-order binary32 sum
-     * ((v0 + v1) + v2) + ... of a long sequence, bit for bit, without a
-     * serial chain of adds.
+     * EXACT order of a hub row: the stream-order binary32 sum
+     * ((v0 + v1) + v2) + ... of up to millions of values, bit for bit,
+     * without a chain of that many adds on one warp.
      *
      * While the running sum s is a positive normal number of biased exponent
      * e, it is M * 2^(e-150) with an integer M in [2^23, 2^24).  The binary32
-     * add s + v rounds to M' = M + round(x), x = v / 2^(e-150), as long as the
-     * exact sum stays in the binade.  round() is to nearest, and on a tie
-     * (x = k + 1/2) to the even M', so the step is k + ((M + k) & 1): it
-     * depends on M only through M's parity.  Within a binade the adds are
-     * therefore integer adds, which associate, and a tie is a two-state map
-     * of the parity, which composes associatively too.
+     * add s + v rounds to M' = M + rint(x), x = v / 2^(e-150), as long as the
+     * exact sum stays in the binade and x is not a tie (x = k + 1/2, where
+     * the result is the even neighbour, which depends on M).  So within a
+     * binade a run of adds is one integer add of its steps, and the steps of
+     * a run can be summed in any order, by any warp.
      *
-     * A round is 256 consecutive values; lane L holds positions 8L .. 8L+7
-     * (`in` marks the ones that belong to the sum).  Three ways, tried in
-     * order, each exact:
-     *  - exact_fast: every value non-negative and finite, no tie, and M plus
-     *    the round's total still in the binade.  The steps are >= 0, so every
-     *    partial M is too: s moves by one warp-reduced integer total.
-     *  - exact_seg: a warp scan of binary32 prefix sums predicts where the
-     *    sum enters a new binade (and which values are at least half the sum
-     *    before them).  Those values are added with binary32 adds, one by
-     *    one; the runs between them are integer sums at their binade's unit,
-     *    ties included.  The prediction is only a guess: each run must keep
-     *    M in its binade, and each binary32 add must land in the binade the
-     *    next run was computed for, or the round falls through.
-     *  - exact_slow: a warp scan of the integer steps gives every partial M;
-     *    the first value that breaks a condition (leaves the binade either
-     *    way, is a tie, is huge or not finite, or s is zero, subnormal or not
-     *    finite) takes a binary32 add and the scan resumes after it.
-     * Values are the caller's: magnitudes with their sign tags taken off in
-     * data-driven passes. */
+     * A hub row is split into chunks on separate warps, and a chunk into
+     * rounds of 256 in-edges (round k of in-edges [eb, ee): those at or past
+     * eb in [(eb & ~3) + 256 k, + 256)).
+     *  - The first chunk sums its own in-edges in stream order (ordered_sum)
+     *    and stores the sum.
+     *  - Every other chunk stages its values and, for each round, sums the
+     *    integer steps at the binade e where the chunk began in the pass
+     *    before and at e + 1 (hub_steps).  A total does not apply when a
+     *    step is a tie, 2^22 or more, or not from a finite non-negative
+     *    value.
+     *  - The last chunk to arrive walks the rounds in order (hub_compose).
+     *    When s is in binade e or e + 1, the matching total applies and
+     *    M plus the total stays below 2^24, the round is one integer add
+     *    (no partial sum can leave the binade: the steps are >= 0).
+     *    Otherwise the round's staged values are added one by one.  It then
+     *    records where each chunk began, for the next pass.
+     * Data-driven passes stage the values with their sign tags and sum the
+     * magnitudes. */
 
-    /* s rebuilt from its sign and exponent bits and M (M in [2^23, 2^24)) */
-    static __device__ __forceinline__ float exact_make(uint32_t sgn_ex, uint32_t m)
+    /* s rebuilt from its exponent bits and M (M in [2^23, 2^24)) */
+    static __device__ __forceinline__ float exact_make(uint32_t ex, uint32_t m)
     {
-        return __uint_as_float(sgn_ex | (m & 0x7fffffu));
+        return __uint_as_float((ex << 23) | (m & 0x7fffffu));
     }
 
     /* 2^(150-e) for a biased exponent e in [24, 254] */
     static __device__ __forceinline__ float exact_scale(uint32_t e) { return __uint_as_float((277u - e) << 23); }
 
-    static __device__ __forceinline__ bool exact_fast(float &s, const float (&v)[8], const bool (&in)[8])
+    /* the step of x (a value in units of s's last place) and whether it
+     * breaks the integer form: a tie, too large, negative or not finite */
+    static __device__ __forceinline__ uint32_t exact_step(float x, bool &bad)
     {
-        const uint32_t sb = __float_as_uint(s);
-        const uint32_t ex = sb >> 23; /* sign bit included: positive s only */
-        if (ex < 24u || ex >= 255u)
-            return false;
-        const float scale = exact_scale(ex);
-        uint32_t t = 0;
-        bool bad = false;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            /* negative values (sign bit set) are left to the other ways */
-            const float x = in[k] ? __fmul_rn(v[k], scale) : 0.0f;
-            /* bitwise ors: no short-circuit branches per value */
-            bad |= !(x < 4194304.0f) | (in[k] & ((__float_as_uint(v[k]) >> 31) != 0u)) |
-                   (__fsub_rn(x, floorf(x)) == 0.5f);
-            t += (uint32_t)__float2int_rn(x);
-        }
-        /* not bad: every step is below 2^22, the total below 2^30 */
-        t = __reduce_add_sync(0xffffffffu, t);
-        const uint32_t m = ((sb & 0x7fffffu) | 0x800000u) + t;
-        if (__any_sync(0xffffffffu, bad) || m >= (1u << 24))
-            return false;
-        s = exact_make(ex << 23, m);
-        return true;
+        bad |= !((x >= 0.0f) & (x < 4194304.0f)) | (__fsub_rn(x, floorf(x)) == 0.5f);
+        return (uint32_t)__float2int_rn(x);
     }
 
-    /* the parity map of a run: a[p] = its total step when M starts with
-     * parity p; (0, 0) is the empty run */
-    struct XMap
+    /* EXACT-order hub chunk after the first: stages the gathered values of
+     * in-edges [eb, ee) of the row starting at o0 at dst[j - o0], and writes
+     * per round the totals of its integer steps at binade e and e + 1
+     * (words[2k], words[2k+1]; AG_XNOT when they do not apply or e is
+     * unknown) and the chunk's sign tag (words[AG_XWORDS - 1]).  The next
+     * round's gathers are in flight while a round's steps are summed. */
+    __device__ __forceinline__ void hub_steps(float *dst, uint32_t o0, uint32_t eb, uint32_t ee, uint32_t lane,
+                                              const Pair &first, uint32_t e, uint32_t *words) const
     {
-        uint32_t a0, a1;
+        const uint32_t q1 = (ee + 3u) >> 2;
+        const bool known = (e >= 24u) & (e <= 253u);
+        const float sc = known ? exact_scale(e) : 0.0f;
+        uint32_t neg = 0;
+        Pair cur = first;
+        /* the loop runs on the round's first quad, the same in every lane:
+         * the warp reductions below need all 32 lanes (lanes past the range
+         * load and gather nothing) */
+        for (uint32_t k = 0, q0 = eb >> 2; q0 < q1; ++k, q0 += 64) {
+            const uint32_t qa = q0 + lane;
+            const Pair nx = load_pair(qa + 64, q1);
+            float v[8];
+            bool in[8];
+            gather8(cur, qa, eb, ee, v, in);
+            const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (in[i])
+                    dst[ja + i - o0] = v[i];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (in[4 + i])
+                    dst[jb + i - o0] = v[4 + i];
+            if (known && k < AG_XROUNDS) {
+                uint32_t t0 = 0, t1 = 0;
+                bool b0 = false, b1 = false;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    float x = v[i];
+                    if (MODE == AG_MODE_DD) {
+                        neg |= in[i] ? dd_neg(x) : 0u;
+                        x = fabsf(x);
+                    }
+                    const float x0 = in[i] ? __fmul_rn(x, sc) : 0.0f;
+                    /* one binade up: half the units (exact, or a value far
+                     * below one unit either way) */
+                    const float x1 = __fmul_rn(x0, 0.5f);
+                    t0 += exact_step(x0, b0);
+                    t1 += exact_step(x1, b1);
+                }
+                /* a total of 2^24 or more cannot stay in a binade */
+                t0 = __reduce_add_sync(0xffffffffu, min(t0, 1u << 24));
+                t1 = __reduce_add_sync(0xffffffffu, min(t1, 1u << 24));
+                b0 = __any_sync(0xffffffffu, b0 | (t0 >= (1u << 24)));
+                b1 = __any_sync(0xffffffffu, b1 | (t1 >= (1u << 24)));
+                if (lane == 0) {
+                    words[2 * k] = b0 ? AG_XNOT : t0;
+                    words[2 * k + 1] = b1 ? AG_XNOT : t1;
+                }
+            } else if (MODE == AG_MODE_DD) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    neg |= in[i] ? dd_neg(v[i]) : 0u;
+            }
+            cur = nx;
+        }
+        if (!known && lane < AG_XROUNDS)
+            words[2 * lane] = words[2 * lane + 1] = AG_XNOT;
+        if (MODE == AG_MODE_DD) {
+            neg = __any_sync(0xffffffffu, neg) ? 1u : 0u;
+            if (lane == 0)
+                words[AG_XWORDS - 1] = neg;
+        }
+    }
+
+    /* EXACT-order hub row, on the warp of its last chunk to arrive: the
+     * stream-order sum of its deg in-edges (row start o0, chunks of
+     * p.whub at slots pbase + c) from the first chunk's sum, the other
+     * chunks' round totals and, where a total does not apply, the staged
+     * values (row_vals[j - o0]) added one by one through the warp's
+     * shared-memory slice.  Records each chunk's starting binade for the
+     * next pass.  Data-driven passes OR the sign tags into `neg`. */
+    struct XSum
+    {
+        float s;
+        uint32_t neg;
     };
 
-    /* run x then run y */
-    static __device__ __forceinline__ XMap exact_compose(XMap x, XMap y)
+    /* static, with plain arguments: a call of a member would need the
+     * kernel's parameter block in local memory */
+    static __device__ __noinline__ XSum hub_compose(const uint32_t *hub_part, const uint32_t *hub_t,
+                                                    uint32_t *hub_pred, const float *row_vals, float *vals,
+                                                    uint32_t whub, uint32_t o0, uint32_t deg, uint32_t pbase,
+                                                    uint32_t nch, uint32_t lane)
     {
-        XMap r;
-        r.a0 = x.a0 + ((x.a0 & 1u) ? y.a1 : y.a0);
-        r.a1 = x.a1 + ((x.a1 & 1u) ? y.a0 : y.a1);
-        return r;
-    }
-
-    /* the parity map of the whole warp's run of group g, in lane order */
-    static __device__ __forceinline__ XMap exact_warp_map(XMap m, uint32_t lane)
-    {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            XMap y;
-            y.a0 = __shfl_down_sync(0xffffffffu, m.a0, o);
-            y.a1 = __shfl_down_sync(0xffffffffu, m.a1, o);
-            if ((lane & (2u * o - 1u)) == 0)
-                m = exact_compose(m, y);
-        }
-        m.a0 = __shfl_sync(0xffffffffu, m.a0, 0);
-        m.a1 = __shfl_sync(0xffffffffu, m.a1, 0);
-        return m;
-    }
-
-    /* returned by exact_seg when it does not apply */
-    static __device__ __forceinline__ float exact_none() { return __uint_as_float(0x7fffffffu); }
-    static __device__ __forceinline__ bool exact_is_none(float s) { return __float_as_uint(s) == 0x7fffffffu; }
-
-    /* values and the `in` mask (bit k) by value: nothing goes through local
-     * memory at the call */
-    static __device__ __noinline__ float exact_seg(float s, float v0, float v1, float v2, float v3, float v4,
-                                                   float v5, float v6, float v7, uint32_t inm, uint32_t lane)
-    {
-        const float v[8] = {v0, v1, v2, v3, v4, v5, v6, v7};
-        bool in[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            in[k] = (inm >> k) & 1u;
-        if ((__float_as_uint(s) >> 23) < 24u || (__float_as_uint(s) >> 23) >= 255u)
-            return exact_none();
-        /* binary32 prefix sums: inclusive within the lane, then across lanes */
-        float loc[8];
-        float acc = 0.0f;
-        bool bad = false;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            /* values must be non-negative and finite (+0 and -0 included) */
-            bad |= in[k] & !((v[k] >= 0.0f) & (v[k] < __int_as_float(0x7f800000)));
-            acc = __fadd_rn(acc, in[k] ? v[k] : 0.0f);
-            loc[k] = acc;
-        }
-        if (__any_sync(0xffffffffu, bad))
-            return exact_none();
-        float inc = acc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const float y = __shfl_up_sync(0xffffffffu, inc, o);
-            if ((int)lane >= o)
-                inc = __fadd_rn(inc, y);
-        }
-        float excl = __shfl_up_sync(0xffffffffu, inc, 1);
-        if (lane == 0)
-            excl = 0.0f;
-        /* per value: the binade of the sum before and after it (predicted),
-         * whether it is added one by one, and its step */
-        uint32_t cnt = 0, ebin[8], eaft[8];
-        bool cross[8], tie[8];
-        uint32_t r[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const float before = __fadd_rn(s, __fadd_rn(excl, k ? loc[k - 1] : 0.0f));
-            const float after = __fadd_rn(s, __fadd_rn(excl, loc[k]));
-            ebin[k] = __float_as_uint(before) >> 23;
-            eaft[k] = __float_as_uint(after) >> 23;
-            bad |= in[k] & (eaft[k] >= 255u);
-            const float x = __fmul_rn(v[k], exact_scale(min(ebin[k], 254u)));
-            const float fl = floorf(x);
-            const float fr = __fsub_rn(x, fl);
-            cross[k] = in[k] & ((eaft[k] != ebin[k]) | !(x < 4194304.0f));
-            tie[k] = in[k] & !cross[k] & (fr == 0.5f);
-            r[k] = (in[k] & !cross[k]) ? (uint32_t)__float2int_rz(fl) + (fr > 0.5f ? 1u : 0u) : 0u;
-            cnt += cross[k] ? 1u : 0u;
-        }
-        if (__any_sync(0xffffffffu, bad))
-            return exact_none();
-        /* group of each value: the one-by-one values before it (all lanes) */
-        uint32_t cinc = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, cinc, o);
-            if ((int)lane >= o)
-                cinc += y;
-        }
-        const uint32_t ncross = __shfl_sync(0xffffffffu, cinc, 31);
-        const uint32_t cbase = cinc - cnt;
-        const bool anytie = __any_sync(0xffffffffu, tie[0] | tie[1] | tie[2] | tie[3] | tie[4] | tie[5] | tie[6] |
-                                                        tie[7]);
-        uint32_t sb = __float_as_uint(s);
-        uint32_t ex = sb >> 23;
-        uint32_t m = (sb & 0x7fffffu) | 0x800000u;
-        for (uint32_t g = 0;; ++g) {
-            /* the run of group g, at binade ex */
-            uint32_t grp = cbase;
-            XMap mp = {0u, 0u};
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                /* selects, not branches: the lane's values of this run */
-                const bool take = (grp == g) & in[k] & !cross[k];
-                XMap e;
-                /* a tie's step is k + ((M + k) & 1), with r[k] = k */
-                e.a0 = take ? (tie[k] ? r[k] + (r[k] & 1u) : r[k]) : 0u;
-                e.a1 = take ? (tie[k] ? r[k] + ((r[k] + 1u) & 1u) : r[k]) : 0u;
-                bad |= take & (ebin[k] != ex);
-                if (anytie)
-                    mp = exact_compose(mp, e);
-                else
-                    mp.a0 += e.a0;
-                grp += cross[k] ? 1u : 0u;
-            }
-            if (anytie)
-                mp = exact_warp_map(mp, lane);
-            else
-                mp.a0 = __reduce_add_sync(0xffffffffu, mp.a0);
-            if (__any_sync(0xffffffffu, bad))
-                return exact_none();
-            m += (anytie & ((m & 1u) != 0u)) ? mp.a1 : mp.a0;
-            if (m >= (1u << 24))
-                return exact_none();
-            s = exact_make(ex << 23, m);
-            if (g == ncross)
-                break;
-            /* the one-by-one value that ends group g */
-            grp = cbase;
-            float xv = 0.0f;
-            uint32_t xe = 0;
-            bool mine = false;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const bool here = cross[k] & (grp == g);
-                xv = here ? v[k] : xv;
-                xe = here ? eaft[k] : xe;
-                mine |= here;
-                grp += cross[k] ? 1u : 0u;
-            }
-            const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
-            xv = __shfl_sync(0xffffffffu, xv, src);
-            xe = __shfl_sync(0xffffffffu, xe, src);
-            s = __fadd_rn(s, xv);
-            sb = __float_as_uint(s);
-            ex = sb >> 23;
-            if (ex != xe)
-                return exact_none();
-            m = (sb & 0x7fffffu) | 0x800000u;
-        }
-        return s;
-    }
-
-    /* general way: adds, in position order, the lane's values v[k]
-     * (position 8 * lane + k) that have in[k] set */
-    static __device__ __noinline__ float exact_slow(float s, float v0, float v1, float v2, float v3, float v4,
-                                                    float v5, float v6, float v7, uint32_t inm, uint32_t lane)
-    {
-        const float v[8] = {v0, v1, v2, v3, v4, v5, v6, v7};
-        bool in[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            in[k] = (inm >> k) & 1u;
-        uint32_t cur = 0;
-        for (;;) {
-            bool ok[8], rem = false;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                ok[k] = in[k] & (8u * lane + k >= cur);
-                rem |= ok[k];
-            }
-            const unsigned rm = __ballot_sync(0xffffffffu, rem);
-            if (!rm)
-                return s;
-            const uint32_t sb = __float_as_uint(s);
-            const uint32_t ex = (sb >> 23) & 0xffu;
-            if (ex < 24u || ex == 255u) {
-                /* zero, tiny or not finite: one binary32 add of the first
-                 * remaining value */
-                const int src = __ffs(rm) - 1;
-                float x = 0.0f;
-                uint32_t fk = 8;
-#pragma unroll
-                for (int k = 7; k >= 0; --k)
-                    if (ok[k]) {
-                        x = v[k];
-                        fk = k;
-                    }
-                x = __shfl_sync(0xffffffffu, x, src);
-                fk = __shfl_sync(0xffffffffu, fk, src);
-                s = __fadd_rn(s, x);
-                cur = 8u * src + fk + 1u;
-                continue;
-            }
-            const uint32_t sgn = sb & 0x80000000u;
-            /* +-2^(150-e): values in units of s's last place, s's sign folded in */
-            const float scale = __uint_as_float(sgn | ((277u - ex) << 23));
-            const int m0 = (int)((sb & 0x7fffffu) | 0x800000u);
-            int r[8];
-            bool up[8], bad[8];
-            int t = 0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float x = ok[k] ? __fmul_rn(v[k], scale) : 0.0f;
-                const float fl = floorf(x);
-                const float fr = __fsub_rn(x, fl);
-                bad[k] = !(fabsf(x) < 4194304.0f) | (fr == 0.5f);
-                up[k] = fr > 0.5f;
-                r[k] = bad[k] ? 0 : __float2int_rz(fl) + (up[k] ? 1 : 0);
-                t += r[k];
-            }
-            int inc = t;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, inc, o);
-                if ((int)lane >= o)
-                    inc += y;
-            }
-            /* M before each value; a value is out when it is bad, when the sum
-             * before it plus its floor falls below the binade, or when its
-             * rounded sum reaches the next binade */
-            int mj = m0 + inc - t, mb = mj;
-            uint32_t fk = 8;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int mn = mj + r[k];
-                const bool out = ok[k] & (bad[k] | (mn - (up[k] ? 1 : 0) < (1 << 23)) | (mn >= (1 << 24)));
-                if (out && fk == 8) {
-                    fk = k;
-                    mb = mj;
-                }
-                mj = mn;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, fk != 8);
-            if (!bal) {
-                const int mend = __shfl_sync(0xffffffffu, m0 + inc, 31);
-                return exact_make(sgn | (ex << 23), (uint32_t)mend);
-            }
-            const int src = __ffs(bal) - 1;
-            float x = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                if ((uint32_t)k == fk)
-                    x = v[k];
-            x = __shfl_sync(0xffffffffu, x, src);
-            fk = __shfl_sync(0xffffffffu, fk, src);
-            mb = __shfl_sync(0xffffffffu, mb, src);
-            s = __fadd_rn(exact_make(sgn | (ex << 23), (uint32_t)mb), x);
-            cur = 8u * src + fk + 1u;
-        }
-    }
-
-    /* one round added to s (see above) */
-    static __device__ __forceinline__ float exact_round(float s, const float (&v)[8], const bool (&in)[8],
-                                                        uint32_t lane)
-    {
-        if (exact_fast(s, v, in))
-            return s;
-        uint32_t inm = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-            inm |= in[k] ? 1u << k : 0u;
-        const float r = exact_seg(s, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], inm, lane);
-        if (!exact_is_none(r))
-            return r;
-        return exact_slow(s, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], inm, lane);
-    }
-
-    /* the start of a sequence: s = its first value plus the next ones, one by
-     * one, up to `cnt` (<= AG_XSTART) values (positions 0 .. cnt-1, held by
-     * lanes 0 .. 3), which then leave the round.  There the values are as
-     * large as the sum and the binade changes at almost every add. */
-    static __device__ __forceinline__ float exact_start(const float (&v)[8], bool (&in)[8], uint32_t cnt,
-                                                        uint32_t lane)
-    {
-        float s = 0.0f;
-#pragma unroll
-        for (uint32_t q = 0; q < AG_XSTART; ++q) {
-            const float x = __shfl_sync(0xffffffffu, v[q & 7u], (int)(q >> 3));
-            if (q < cnt)
-                s = q == 0 ? x : __fadd_rn(s, x);
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < 8; ++k)
-            if (8u * lane + k < cnt)
-                in[k] = false;
-        return s;
-    }
-
-    /* the caller's value of a gathered element: data-driven passes take the
-     * magnitude and OR the sign tag into `neg` */
-    __device__ __forceinline__ void exact_prep(float (&v)[8], const bool (&in)[8], uint32_t &neg) const
-    {
+        uint32_t neg = 0;
+        float s = __uint_as_float(__ldcg(hub_part + pbase));
         if (MODE == AG_MODE_DD) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                if (in[k])
-                    neg |= dd_neg(v[k]);
-                v[k] = fabsf(v[k]);
+            neg |= dd_neg(s);
+            s = fabsf(s);
+        }
+        const uint32_t *wp = hub_t + (size_t)(pbase + 1) * AG_XWORDS;
+        uint32_t wa = __ldcg(wp + lane), wb = __ldcg(wp + 32 + lane);
+        uint32_t pr = __ldcg(hub_pred + pbase + 1);
+        for (uint32_t c = 1; c < nch; ++c) {
+            /* the next chunk's words travel while this one is composed */
+            uint32_t na = 0, nb = 0, npr = 0;
+            if (c + 1 < nch) {
+                const uint32_t *wn = hub_t + (size_t)(pbase + c + 1) * AG_XWORDS;
+                na = __ldcg(wn + lane);
+                nb = __ldcg(wn + 32 + lane);
+                npr = __ldcg(hub_pred + pbase + c + 1);
             }
-        }
-    }
-
-    /* one round of a hub row's chain: positions cb .. cb+255 of src */
-    __device__ __forceinline__ float chain_round(float s, float (&v)[8], uint32_t cb, uint32_t n, uint32_t lane,
-                                                 uint32_t &neg) const
-    {
-        bool in[8];
+            if (MODE == AG_MODE_DD)
+                neg |= __shfl_sync(0xffffffffu, wb, 31) & 1u;
+            const uint32_t e = pr & 0xffu;
+            const uint32_t e_start = __float_as_uint(s) >> 23;
+            bool fell = false;
+            const uint32_t cb = o0 + c * whub, ce = min(o0 + deg, cb + whub), base = cb & ~3u;
+            const uint32_t nr = (ce - base + 255u) >> 8;
+            for (uint32_t k = 0; k < nr; ++k) {
+                const uint32_t lo = max(cb, base + 256u * k), hi = min(ce, base + 256u * (k + 1u));
+                const uint32_t w0 = __shfl_sync(0xffffffffu, k < 16u ? wa : wb, (int)((2u * k) & 31u));
+                const uint32_t w1 = __shfl_sync(0xffffffffu, k < 16u ? wa : wb, (int)((2u * k + 1u) & 31u));
+                const uint32_t sb = __float_as_uint(s), ex = sb >> 23;
+                uint32_t w = AG_XNOT;
+                if (k < AG_XROUNDS && e != 0u)
+                    w = ex == e ? w0 : (ex == e + 1u ? w1 : AG_XNOT);
+                const uint32_t m = ((sb & 0x7fffffu) | 0x800000u) + (w & 0x1ffffffu);
+                if (!(w & AG_XNOT) && (ex >= 24u) & (ex <= 254u) && m < (1u << 24)) {
+                    s = exact_make(ex, m);
+                } else {
+                    /* this round's values, one by one */
+                    __syncwarp();
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-            in[k] = cb + 8u * lane + k < n;
-        exact_prep(v, in, neg);
-        if (cb == 0)
-            s = exact_start(v, in, min(n, AG_XSTART), lane);
-        return exact_round(s, v, in, lane);
-    }
-
-    /* EXACT-order hub row: the stream-order sum of its n staged values
-     * src[0, n) (16-byte aligned; the row's staging slots hold a multiple of
-     * 32 values, so a 16-byte group that starts below n ends inside them).
-     * Three rounds are loading (from L2, 16-byte loads) at any time: a
-     * buffer is refilled right after its round is added, and the rotation
-     * over the three is unrolled, so no register waits on a load to be
-     * copied. */
-    __device__ __noinline__ float ordered_chain(const float *src, uint32_t n, uint32_t lane, uint32_t &neg) const
-    {
-        float a[8], b[8], c[8];
-        auto load = [&](float (&r)[8], uint32_t cb) {
-            const uint32_t pa = cb + 8u * lane, pb = pa + 4u;
-            const float4 x = pa < n ? __ldcg(reinterpret_cast<const float4 *>(src + pa)) : make_float4(0, 0, 0, 0);
-            const float4 y = pb < n ? __ldcg(reinterpret_cast<const float4 *>(src + pb)) : make_float4(0, 0, 0, 0);
-            r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
-            r[4] = y.x; r[5] = y.y; r[6] = y.z; r[7] = y.w;
-        };
-        load(a, 0);
-        load(b, 256u);
-        load(c, 512u);
-        float s = 0.0f;
-        for (uint32_t cb = 0;; cb += 768u) {
-            s = chain_round(s, a, cb, n, lane, neg);
-            if (cb + 768u < n)
-                load(a, cb + 768u);
-            if (cb + 256u >= n)
-                break;
-            s = chain_round(s, b, cb + 256u, n, lane, neg);
-            if (cb + 1024u < n)
-                load(b, cb + 1024u);
-            if (cb + 512u >= n)
-                break;
-            s = chain_round(s, c, cb + 512u, n, lane, neg);
-            if (cb + 1280u < n)
-                load(c, cb + 1280u);
-            if (cb + 768u >= n)
-                break;
+                    for (int i = 0; i < 8; ++i) {
+                        const uint32_t j = lo + lane + 32u * i;
+                        vals[lane + 32u * i] = j < hi ? __ldcg(row_vals + (j - o0)) : 0.0f;
+                    }
+                    __syncwarp();
+                    if (lane == 0)
+                        s = seq_sum(vals, 0, hi - lo, s, false, neg);
+                    s = __shfl_sync(0xffffffffu, s, 0);
+                    fell = true;
+                }
+            }
+            if (lane == 0)
+                hub_pred[pbase + c] = e_start | (fell ? AG_XFELL : 0u);
+            wa = na;
+            wb = nb;
+            pr = npr;
         }
-        return s;
+        return XSum{s, neg};
     }
 
     /* the stream-order sum of vals[a, b) (the warp's shared-memory slice)
@@ -913,8 +673,8 @@ struct AgPass
      * `first`: four values per 16-byte shared load once the index is
      * aligned, one binary32 add after another.  Data-driven passes add the
      * magnitudes and OR the sign tags into `neg`. */
-    __device__ __forceinline__ float seq_sum(const float *vals, uint32_t a, uint32_t b, float s, bool first,
-                                             uint32_t &neg) const
+    static __device__ __forceinline__ float seq_sum(const float *vals, uint32_t a, uint32_t b, float s, bool first,
+                                                    uint32_t &neg)
     {
         auto val = [&](float v) {
             if (MODE == AG_MODE_DD) {
@@ -1266,22 +1026,33 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             __syncwarp();
             pf = pn;
         } else if (EXACT) {
-            /* hub chunk, EXACT order: the chunk's values go to the staging
-             * array at their place in the row; the row's last chunk to arrive
-             * sums the whole row in stream order */
+            /* hub chunk, EXACT order: the first chunk sums its in-edges in
+             * stream order, the others stage their values and sum their
+             * integer steps per round; the row's last chunk to arrive
+             * composes the row (hub_compose) */
             const uint32_t pbase = task.y & AG_SLOT_MASK, chunk = task.y >> AG_SLOT_BITS;
             const uint32_t o0 = eb - chunk * p.whub;
             float *row_vals = p.hub_vals + (size_t)pbase * p.whub;
             const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
-            ps.stage_global(row_vals, o0, eb, ee, lane, pf);
+            if (chunk == 0) {
+                uint32_t neg0 = 0;
+                const float s0 = ps.ordered_sum(vals, eb, ee, lane, pf, neg0);
+                if (lane == 0) {
+                    /* data-driven: the sign bit carries the chunk's tag */
+                    const uint32_t bits = __float_as_uint(s0) | (MODE == AG_MODE_DD && neg0 ? 0x80000000u : 0u);
+                    reinterpret_cast<uint32_t *>(p.hub_part)[pbase] = bits;
+                }
+            } else {
+                const uint32_t pred = __ldcg(p.hub_pred + pbase + chunk);
+                ps.hub_steps(row_vals, o0, eb, ee, lane, pf, pred & 0xffu, p.hub_t + (size_t)(pbase + chunk) * AG_XWORDS);
+            }
             __threadfence();
             __syncwarp();
             uint32_t last = 0;
             const uint32_t deg = p.row_off[r0 + 1] - o0;
-            if (lane == 0) {
-                const uint32_t nch = (deg + p.whub - 1) / p.whub;
+            const uint32_t nch = (deg + p.whub - 1) / p.whub;
+            if (lane == 0)
                 last = atomicAdd(&p.hub_cnt[pbase], 1u) == nch - 1 ? 1u : 0u;
-            }
             last = __shfl_sync(0xffffffffu, last, 0);
             if (last) {
                 __threadfence();
@@ -1296,10 +1067,11 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                         steal.donor = (int)d;
                     }
                 }
-                uint32_t neg = 0;
-                const float tot = ps.ordered_chain(row_vals, deg, lane, neg);
-                /* each lane saw the sign tags of its own values */
-                neg = __any_sync(0xffffffffu, neg) ? 1u : 0u;
+                const typename AgPass<MODE, PREC, EXACT>::XSum xs = AgPass<MODE, PREC, EXACT>::hub_compose(
+                    reinterpret_cast<const uint32_t *>(p.hub_part), p.hub_t, p.hub_pred, row_vals, vals, p.whub, o0,
+                    deg, pbase, nch, lane);
+                const float tot = xs.s;
+                const uint32_t neg = xs.neg;
                 if (lane == 0) {
                     p.hub_cnt[pbase] = 0;
                     float rp = 0.0f;

@@ -359,6 +359,8 @@ struct ag_graph_s
     float *hub_part;
     uint32_t *hub_cnt;
     float *hub_vals; /* EXACT order: staged values of hub rows */
+    uint32_t *hub_pred; /* EXACT order: chunk starting binades of the last pass */
+    uint32_t *hub_t;    /* EXACT order: per-round integer step totals */
     AgControl *ctl;
     float *init_buf;
     uint32_t *flag;
@@ -492,6 +494,8 @@ extern "C" ag_status_t ag_graph_release(ag_graph_t g)
     dev_free(g->hub_part);
     dev_free(g->hub_cnt);
     dev_free(g->hub_vals);
+    dev_free(g->hub_pred);
+    dev_free(g->hub_t);
     dev_free(g->ctl);
     dev_free(g->init_buf);
     dev_free(g->flag);
@@ -550,10 +554,16 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
     /* EXACT order stages a hub row's gathered values here (chunk slot x
      * chunk size + offset in the row) before summing them in stream order */
     float *hv = (float *)dev_alloc(g, (size_t)tot[0] * whub * 4 + 16, &st);
+    /* and keeps each chunk's starting binade and per-round integer step
+     * totals (the predictions start unknown) */
+    uint32_t *hpr = (uint32_t *)dev_alloc(g, (size_t)tot[0] * 4 + 16, &st);
+    uint32_t *ht = (uint32_t *)dev_alloc(g, (size_t)tot[0] * AG_XWORDS * 4 + 16, &st);
     if (st == AG_OK) {
         e = ag_plan_write(&ps, tot, tdf, tde, s);
         if (e == cudaSuccess)
             e = cudaMemsetAsync(hc, 0, hc_bytes, s);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(hpr, 0, (size_t)tot[0] * 4 + 16, s);
         if (e != cudaSuccess) {
             cudaGetLastError();
             st = ag_set_error(AG_ERR_CUDA, "work-list planning failed: %s", cudaGetErrorString(e));
@@ -566,6 +576,8 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
         dev_free(hp);
         dev_free(hc);
         dev_free(hv);
+        dev_free(hpr);
+        dev_free(ht);
         return st;
     }
     dev_free(g->tasks_fast);
@@ -573,11 +585,15 @@ static ag_status_t plan_device(ag_graph_s *g, uint32_t cap, uint32_t whub)
     dev_free(g->hub_part);
     dev_free(g->hub_cnt);
     dev_free(g->hub_vals);
+    dev_free(g->hub_pred);
+    dev_free(g->hub_t);
     g->tasks_fast = tdf;
     g->tasks_exact = tde;
     g->hub_part = hp;
     g->hub_cnt = hc;
     g->hub_vals = hv;
+    g->hub_pred = hpr;
+    g->hub_t = ht;
     g->ntasks_fast = nf;
     g->ntasks_exact = ne;
     g->nparts = tot[0];
@@ -1004,6 +1020,8 @@ static AgPullParams base_params(ag_graph_s *g, int exact)
     p.hub_part = g->hub_part;
     p.hub_cnt = g->hub_cnt;
     p.hub_vals = g->hub_vals;
+    p.hub_pred = g->hub_pred;
+    p.hub_t = g->hub_t;
     p.steal = g->hub_cnt + g->nparts + 4;
     p.ctl = g->ctl;
     p.init_ranks = g->init_buf;
