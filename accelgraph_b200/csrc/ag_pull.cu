@@ -720,6 +720,8 @@ struct AgPass
                                                  const Pair &first, uint32_t &neg) const
     {
         uint32_t cb = eb, ce = min(ee, (eb & ~3u) + (uint32_t)AG_WCAP);
+        /* the ids of a round are requested one round before its gathers */
+        Pair ids = prefetch(ce, min(ee, ce + (uint32_t)AG_WCAP), lane);
         stage(vals, cb, ce, lane, first);
         float s = 0.0f;
         for (;;) {
@@ -732,7 +734,8 @@ struct AgPass
             }
             /* the next round's gathers travel while this one is added */
             float w[8];
-            stage_issue(prefetch(nb, ne, lane), nb, ne, lane, w);
+            stage_issue(ids, nb, ne, lane, w);
+            ids = prefetch(ne, min(ee, ne + (uint32_t)AG_WCAP), lane);
             if (lane == 0)
                 s = seq_sum(vals, 0, ce - cb, s, cb == eb, neg);
             __syncwarp();
