@@ -61,6 +61,9 @@ def _load() -> C.CDLL:
                                u32p, C.c_int]
     lib.oracle_ppr.restype = C.c_uint32
     lib.oracle_max_threads.restype = C.c_int
+    lib.oracle_rmat_inverse.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                        u32p, u32p, u32p, u32p]
+    lib.oracle_rmat_inverse.restype = C.c_uint64
     return lib
 
 
@@ -74,6 +77,22 @@ def _p(a, t):
 def _csr(in_idx, in_deg, in_nb):
     return (np.ascontiguousarray(in_idx, np.uint32), np.ascontiguousarray(in_deg, np.uint32),
             np.ascontiguousarray(in_nb, np.uint32))
+
+
+def rmat_inverse(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19):
+    """Seeded R-MAT graph (self loops and duplicates dropped) as the arrays
+    the pull oracle reads: dict(in_idx, in_deg, in_nb, out_deg, num_edges)."""
+    n = 1 << scale
+    m = edge_factor * n
+    in_idx = np.zeros(n + 1, np.uint32)
+    in_deg = np.zeros(n, np.uint32)
+    in_nb = np.zeros(max(m, 1), np.uint32)
+    out_deg = np.zeros(n, np.uint32)
+    e = lib.oracle_rmat_inverse(scale, edge_factor, a, b, c, seed, _p(in_idx, u32p), _p(in_deg, u32p),
+                                _p(in_nb, u32p), _p(out_deg, u32p))
+    if e == 2 ** 64 - 1:
+        raise MemoryError("oracle_rmat_inverse: allocation failed")
+    return {"in_idx": in_idx, "in_deg": in_deg, "in_nb": in_nb[:e], "out_deg": out_deg, "num_edges": int(e)}
 
 
 def gather(in_idx, in_deg, in_nb, x, threads=0):

@@ -793,3 +793,116 @@ uint32_t oracle_ppr(uint32_t n, const uint32_t *in_idx, const uint32_t *in_deg, 
 }
 
 int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+/* ----------------------------------------------------------------------
+ * Seeded R-MAT graph as an inverse CSR, for the CPU legs that must not load
+ * the product library.  Graph500-style quadrant recursion: edge e draws one
+ * 32-bit uniform per level, 64-bit draw k of stream e covering levels 2k and
+ * 2k+1 (low half first), where draw k of stream e under `seed` is the
+ * SplitMix64 finaliser (Steele, Lea, Flood, OOPSLA 2014) of
+ * mix(seed + G) + (64 e + k + 1) G, G = 0x9E3779B97F4A7C15, mix(z) the two
+ * xor-shift-multiply rounds of that finaliser.  A level's draw u picks the
+ * quadrant: u < a 2^32 top-left, < (a+b) 2^32 top-right (destination bit),
+ * < (a+b+c) 2^32 bottom-left (source bit), else bottom-right.
+ * Self loops and duplicate edges are dropped (the reference's -k), and each
+ * inverse row lists its sources in ascending order.  Returns the edge count;
+ * in_nb must hold edge_factor * 2^scale entries. */
+static inline uint64_t oracle_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* parallel LSD radix sort of 64-bit keys, 8 bits per pass, `bits` low bits
+ * significant; tmp holds n keys */
+static void oracle_radix64(uint64_t *a, uint64_t *tmp, uint64_t n, int bits)
+{
+    const int T = omp_get_max_threads();
+    uint64_t *cnt = (uint64_t *)malloc((size_t)T * 256 * sizeof(uint64_t));
+    for (int shift = 0; shift < bits; shift += 8) {
+        memset(cnt, 0, (size_t)T * 256 * sizeof(uint64_t));
+#pragma omp parallel num_threads(T)
+        {
+            const int t = omp_get_thread_num();
+            const uint64_t lo = n * t / T, hi = n * (t + 1) / T;
+            uint64_t *c = cnt + (size_t)t * 256;
+            for (uint64_t i = lo; i < hi; ++i)
+                c[(a[i] >> shift) & 255u]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                uint64_t base = 0;
+                for (int d = 0; d < 256; ++d)
+                    for (int u = 0; u < T; ++u) {
+                        const uint64_t x = cnt[(size_t)u * 256 + d];
+                        cnt[(size_t)u * 256 + d] = base;
+                        base += x;
+                    }
+            }
+            for (uint64_t i = lo; i < hi; ++i)
+                tmp[c[(a[i] >> shift) & 255u]++] = a[i];
+        }
+        uint64_t *s = a;
+        a = tmp;
+        tmp = s;
+    }
+    /* an odd number of passes leaves the result in the scratch array */
+    if (((bits + 7) / 8) & 1)
+        memcpy(tmp, a, n * sizeof(uint64_t));
+    free(cnt);
+}
+
+uint64_t oracle_rmat_inverse(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                             uint32_t *in_idx, uint32_t *in_deg, uint32_t *in_nb, uint32_t *out_deg)
+{
+    const uint64_t G = 0x9E3779B97F4A7C15ull;
+    const uint64_t N = 1ull << scale, m = (uint64_t)edge_factor * N;
+    const uint32_t ta = (uint32_t)fmin(4294967295.0, floor(a * 4294967296.0));
+    const uint32_t tb = (uint32_t)fmin(4294967295.0, floor((a + b) * 4294967296.0));
+    const uint32_t tc = (uint32_t)fmin(4294967295.0, floor((a + b + c) * 4294967296.0));
+    const uint64_t base = oracle_mix64(seed + G);
+    uint64_t *key = (uint64_t *)malloc((m ? m : 1) * sizeof(uint64_t));
+    uint64_t *tmp = (uint64_t *)malloc((m ? m : 1) * sizeof(uint64_t));
+    if (!key || !tmp) {
+        free(key);
+        free(tmp);
+        return ~0ull;
+    }
+    /* key = destination * N + source: sorting it orders the inverse rows */
+#pragma omp parallel for schedule(static)
+    for (uint64_t e = 0; e < m; ++e) {
+        uint64_t s = 0, d = 0, r = 0;
+        for (uint32_t l = 0; l < scale; ++l) {
+            if ((l & 1u) == 0)
+                r = oracle_mix64(base + (e * 64ull + (l >> 1) + 1ull) * G);
+            const uint32_t u = (l & 1u) ? (uint32_t)(r >> 32) : (uint32_t)r;
+            const uint64_t sb = u >= tb, db = (u >= ta && u < tb) || u >= tc;
+            s = (s << 1) | sb;
+            d = (d << 1) | db;
+        }
+        key[e] = (d << scale) | s;
+    }
+    oracle_radix64(key, tmp, m, 2 * (int)scale);
+    free(tmp);
+    memset(in_deg, 0, N * sizeof(uint32_t));
+    memset(out_deg, 0, N * sizeof(uint32_t));
+    uint64_t E = 0;
+    for (uint64_t i = 0; i < m; ++i) {
+        const uint64_t k = key[i];
+        const uint32_t d = (uint32_t)(k >> scale), s = (uint32_t)(k & (N - 1));
+        if (s == d || (i > 0 && key[i - 1] == k))
+            continue;
+        in_nb[E++] = s;
+        in_deg[d]++;
+        out_deg[s]++;
+    }
+    free(key);
+    uint64_t off = 0;
+    for (uint64_t v = 0; v < N; ++v) {
+        in_idx[v] = (uint32_t)off;
+        off += in_deg[v];
+    }
+    in_idx[N] = (uint32_t)off;
+    return E;
+}

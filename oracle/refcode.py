@@ -18,11 +18,14 @@ from __future__ import annotations
 
 import ctypes as C
 import subprocess
+import os
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_ref" / "libref_pagerank.so"
-REF_SOURCE = Path("/root/reference/02_capi_graph/src/algorithms/capi/pageRank.c")
+# the reference checkout: $AG_REFERENCE, else `reference` beside this checkout
+REF_ROOT = Path(os.environ.get("AG_REFERENCE") or Path(__file__).resolve().parent.parent.parent / "reference")
+REF_SOURCE = REF_ROOT / "02_capi_graph/src/algorithms/capi/pageRank.c"
 
 
 class _PageRankStats(C.Structure):

@@ -28,12 +28,16 @@ from __future__ import annotations
 
 import json
 import re
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+# the reference checkout: the first argument, else $AG_REFERENCE, else
+# `reference` beside this checkout
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else
+           (os.environ.get("AG_REFERENCE") or Path(__file__).resolve().parents[3] / "reference"))
 TB = REF / "03_capi_integration/accelerator_verification/rtl/unit/algorithms/tb"
 OUT = Path(__file__).resolve().parent / "rtl_fixtures.json"
 
