@@ -1,27 +1,38 @@
 """Benchmark of the pull PageRank hot path (one JSON line on rank 0).
 
-Workload (default): plain FP32 PageRank pull on a seeded R-MAT graph of
-scale 22, edge factor 16 (a,b,c = 0.57,0.19,0.19; self loops and duplicates
-removed; uint32 ids), damping 0.85, run to epsilon 1e-6 (iteration cap 300).
-A step is one complete solve: init, pull passes until no vertex changes by
->= epsilon, normalisation.  The metric is GTEPS = edges x passes / time.
+Workload (default): PageRank pull on a seeded R-MAT graph of scale 24, edge
+factor 16 (a,b,c = 0.57,0.19,0.19; self loops and duplicates removed; uint32
+ids; 16,777,216 vertices, about 2.6e8 in-edges), damping 0.85, run to epsilon
+1e-6 (iteration cap 300), in EXACT order: every row is summed in the reference
+loop's stream order, so ranks, per-pass active counts and the iteration count
+are the reference's bit for bit.  A step is one complete solve: init, pull
+passes until no vertex changes by >= epsilon, normalisation.  The metric is
+GTEPS = edges x passes / time.
 
   value  device time of K solves, graph resident in HBM (CUDA events on the
          library stream); inputs (ids: 4 bytes x E > 126 MB L2) exceed L2.
   e2e    the same metric through the C ABI entry ag_pagerank_pull_ex with the
          graph in page-locked host memory: upload (H2D), plan, solve, ranks
          back (D2H) inside the timed region, host clock.
-  roofline  algorithmic bytes of one pull pass (4E + 24N) / average pass time.
-  cpu_baseline  the CPU oracle (restatement of the reference OpenMP pull) on a
-         bounded number of passes of the same graph, all host threads.
+  roofline  algorithmic bytes of one pull pass (4E + 24N) / average pass
+         time; traffic from the committed ncu summary of the same kernel and
+         graph, named in traffic_source.
+  parity  the CPU oracle solved on the same graph: iteration counts, per-pass
+         active counts, bit-exactness and relative L1 of the ranks; relative L1
+         against the FP64 fixpoint (GPU FP64 kernels).
+  cpu_baseline  that oracle solve (restatement of the reference OpenMP pull,
+         all host threads), timed.
 
---impl reference times that CPU restatement alone, as the reference arm.
+--order fast sums rows of more than 32 in-edges in a fixed tree order (ranks
+within 1e-5 relative L1, iteration count not guaranteed equal).
+--impl reference times the CPU restatement alone, as the reference arm, on a
+graph built by the oracle's own generator (the product library is not loaded).
 --gpus N (torchrun): by default every rank solves its own graph (seed + rank),
 no data exchange, value = all ranks' edges x passes / max-over-ranks time
 (weak scaling); --mode rows splits one graph by rows across the ranks with
 an all-gather of contributions per pass (strong scaling).
 --workload selects the other forms (SpMV, precision, PPR, many graphs, warm
-start, gather-rate probe); each prints its own JSON line.
+start); each prints its own JSON line.
 """
 from __future__ import annotations
 
@@ -48,15 +59,14 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--scale", type=int, default=24)
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--epsilon", type=float, default=1e-6)
     p.add_argument("--iterations", type=int, default=300)
     p.add_argument("--precision", type=int, default=0)
-    p.add_argument("--order", default="fast", choices=["fast", "exact"],
+    p.add_argument("--order", default="exact", choices=["fast", "exact"],
                    help="pagerank: summation order (exact = the reference loop's, bit for bit)")
     p.add_argument("--e2e-steps", type=int, default=3)
-    p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--workload", default="pagerank",
                    choices=["pagerank", "spmv", "precision", "ppr", "multigraph", "warmstart", "gather-probe",
@@ -77,16 +87,20 @@ def dist_env():
     return rank, world, local
 
 
-def profiled_traffic(scale: int, edge_factor: int):
-    """DRAM bytes (read + write) of one pull pass from the committed ncu
-    summary of this workload (profiles/ag_pull_kernel_rmat<scale>.md, row
-    `dram__bytes_read.sum + write | R + W MB`), or None without one."""
+def profiled_traffic(scale: int, edge_factor: int, order: str):
+    """DRAM bytes (read + write) of one pull pass of this kernel and graph from
+    the committed ncu summary profiles/ag_pull_kernel_<order>_rmat<scale>.md
+    (row `dram__bytes_read.sum + write | R + W MB`), with the file it came
+    from; (None, None) without one."""
     import re
-    f = ROOT / "profiles" / f"ag_pull_kernel_rmat{scale}.md"
+    name = f"profiles/ag_pull_kernel_{order}_rmat{scale}.md"
+    f = ROOT / name
     if edge_factor != 16 or not f.exists():
-        return None
+        return None, None
     m = re.search(r"\|\s*dram__bytes_read\.sum \+ write\s*\|\s*([0-9.]+) \+ ([0-9.]+) MB", f.read_text())
-    return None if not m else (float(m.group(1)) + float(m.group(2))) * 1e6
+    if not m:
+        return None, None
+    return (float(m.group(1)) + float(m.group(2))) * 1e6, name
 
 
 def reduce_time_work(seconds_or_ms: float, work: float, device=None):
@@ -105,8 +119,10 @@ def reduce_time_work(seconds_or_ms: float, work: float, device=None):
 
 
 def workload_config(a, world):
+    order = ("EXACT order (stream-order row sums, bit-identical to the reference loop)" if a.order == "exact"
+             else "FAST order (rows over 32 in-edges summed in a fixed tree)")
     return {
-        "workload": f"PageRank pull FP32, RMAT scale {a.scale} edge factor {a.edge_factor} "
+        "workload": f"PageRank pull FP32, {order}, RMAT scale {a.scale} edge factor {a.edge_factor} "
                     f"(a,b,c=0.57,0.19,0.19, dedup, no self loops), d=0.85, eps={a.epsilon:g}, cap {a.iterations}",
         "graph": f"rmat{a.scale}_ef{a.edge_factor}",
         "epsilon": a.epsilon,
@@ -176,35 +192,42 @@ def peak_hbm():
     return 6650.0, "fallback"
 
 
-def cpu_sample(oracle, g, a, seconds):
-    """Time the CPU oracle (all host threads) on whole passes of the same
-    graph, about `seconds` of work."""
-    args = (g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree())
-    one = oracle.pagerank_pull(*args, iterations=1, epsilon=a.epsilon)
-    t1 = float(one["seconds"][0])
-    k = int(max(1, min(a.iterations, seconds / max(t1, 1e-6))))
-    res = oracle.pagerank_pull(*args, iterations=k, epsilon=a.epsilon)
-    t = float(res["seconds"].sum())
-    passes = int(res["passes"])
+def oracle_solve(oracle, arrays, a):
+    """The CPU oracle's complete solve of the same graph (all host threads),
+    timed: the reported CPU baseline and the parity reference."""
+    in_idx, in_deg, in_nb, out_deg = arrays
+    t0 = time.perf_counter()
+    ref = oracle.pagerank_pull(in_idx, in_deg, in_nb, out_deg, iterations=a.iterations, epsilon=a.epsilon)
+    ref["wall_s"] = time.perf_counter() - t0
+    return ref
+
+
+def cpu_baseline(ref, num_edges, a, oracle):
+    t = float(ref["seconds"].sum())
+    passes = int(ref["passes"])
     return {
-        "value": g.num_edges * passes / t / 1e9,
+        "value": num_edges * passes / t / 1e9,
         "unit": UNIT,
         "cores": oracle.max_threads(),
         "kind": "port",
-        "sample": f"{passes} PageRank-pull passes of the same RMAT s{a.scale} graph "
-                  f"({t:.1f} s), per-pass timers as in pageRank.c:1025,1071",
+        "sample": f"one complete solve ({passes} passes to eps {a.epsilon:g}, {t:.1f} s) of the same RMAT "
+                  f"s{a.scale} graph by the C/OpenMP restatement of pageRankPullGraphCSR, per-pass timers "
+                  f"as in pageRank.c:1025,1071",
         "seconds_per_pass": t / passes,
     }
 
 
 def run_reference(a):
+    """The reference arm: the oracle (C/OpenMP restatement of the reference's
+    pull) on all host threads, on a graph built by the oracle's own
+    generator; the product library is not loaded."""
     rank, world, local = dist_env()
     if rank != 0:
         return
-    import accelgraph_b200 as ag
     import oracle
-    g = ag.Graph.rmat(a.scale, a.edge_factor, seed=SEED)
-    args = (g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree())
+    gr = oracle.rmat_inverse(a.scale, a.edge_factor, SEED)
+    args = (gr["in_idx"], gr["in_deg"], gr["in_nb"], gr["out_deg"])
+    E = gr["num_edges"]
     one = oracle.pagerank_pull(*args, iterations=1, epsilon=a.epsilon)
     t1 = float(one["seconds"][0])
     budget = min(10.0, 150.0 / max(1, a.steps + a.warmup))
@@ -217,7 +240,7 @@ def run_reference(a):
         r = oracle.pagerank_pull(*args, iterations=per_step, epsilon=a.epsilon)
         tot_t += time.perf_counter() - t0
         tot_p += int(r["passes"])
-    value = g.num_edges * tot_p / tot_t / 1e9
+    value = E * tot_p / tot_t / 1e9
     cores = oracle.max_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
@@ -228,7 +251,7 @@ def run_reference(a):
                          "sample": f"{per_step} passes per step of the C/OpenMP restatement of "
                                    f"pageRankPullGraphCSR on RMAT s{a.scale} ef{a.edge_factor}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "num_vertices": g.num_vertices, "num_edges": g.num_edges,
+        "num_vertices": 1 << a.scale, "num_edges": E,
     }
     print(json.dumps(line), flush=True)
 
@@ -294,7 +317,8 @@ def run_b200(a):
             "traffic": None, "peak_kind": peak_kind, "kernel": "ag_pull_kernel<PR,fp32,%s>" % a.order,
             "bytes_per_pass": alg_bytes, "pass_us": pass_s * 1e6,
             "pass_us_device_timer_median": float(np.median(dev_pass[1:]) * 1e6) if len(dev_pass) > 1 else None}
-    roof["traffic"] = profiled_traffic(a.scale, a.edge_factor) if a.order == "fast" else None
+    if a.precision == 0:
+        roof["traffic"], roof["traffic_source"] = profiled_traffic(a.scale, a.edge_factor, a.order)
 
     # -------- end to end through the C ABI (host buffers, pinned)
     args = ag.default_arguments(a.iterations, a.epsilon)
@@ -313,22 +337,45 @@ def run_b200(a):
     e2e_t = time.perf_counter() - t0
     e2e_t, e2e_edges = reduce_time_work(e2e_t, float(E * e2e_passes), device="cuda")
     e4 = ((E + 3) & ~3) + 4
-    h2d = 4 * e4 + 4 * (N + 1) + 4 * N + 16 * info.num_tasks
+    # copied per step: in-neighbour ids (E rounded to 4, plus 4), row starts,
+    # out-degrees; the work lists are planned on the device
+    h2d = 4 * e4 + 4 * (N + 1) + 4 * N
     d2h = 4 * N
     e2e = {"value": e2e_edges / e2e_t / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "ms_per_step": 1e3 * e2e_t / a.e2e_steps, "api": "ag_pagerank_pull_ex (pageRankPullGraphCSR semantics)"}
 
-    cpu = None
+    # -------- CPU oracle on the same graph: baseline and parity
+    cpu = parity = None
     if rank == 0 and world == 1 and not a.no_cpu:
         import oracle
-        cpu = cpu_sample(oracle, g, a, a.cpu_seconds)
+        ref = oracle_solve(oracle, (g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree()), a)
+        cpu = cpu_baseline(ref, E, a, oracle)
+        r64, p64 = dg.pagerank_f64(5000, 1e-13)
+        ra = ranks.astype(np.float64)
+        dref = np.abs(ra - ref["ranks"])
+        n_hist = min(len(hist["active"]), len(ref["active"]))
+        parity = {
+            "iterations": int(res.iterations), "iterations_oracle": int(ref["iterations"]),
+            "passes": passes, "passes_oracle": int(ref["passes"]),
+            "active_per_pass_equal": bool(passes == int(ref["passes"]) and
+                                          np.array_equal(hist["active"][:n_hist], ref["active"][:n_hist])),
+            "ranks_bit_exact": bool(np.array_equal(ranks.view(np.uint32), ref["ranks"].view(np.uint32))),
+            "rel_l1_vs_oracle": float(dref.sum() / np.abs(ref["ranks"]).sum()),
+            "max_abs_vs_oracle": float(dref.max()),
+            "rel_l1_vs_fp64": float(np.abs(ra - r64).sum() / np.abs(r64).sum()),
+            "max_abs_vs_fp64": float(np.abs(ra - r64).max()),
+            "oracle_rel_l1_vs_fp64": float(np.abs(ref["ranks"] - r64).sum() / np.abs(r64).sum()),
+            "fp64_passes": int(p64),
+            "oracle": "C/OpenMP restatement of pageRankPullGraphCSR (pageRank.c:942-1109), same graph",
+        }
 
     launches = a.steps * (passes + 2)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": workload_config(a, world),
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "parity": parity, "clocks": clk,
+        "gpu_launches": launches,
         "passes_per_solve": passes, "iterations": int(res.iterations), "converged": int(res.converged),
         "num_vertices": N, "num_edges": E, "tasks": info.num_tasks, "grid": info.grid,
         "hub_rows": info.num_hub_rows,
