@@ -10,6 +10,7 @@ Reference interface mirrored (AccelGraph, 02_capi_graph):
   struct PageRankStats        include/algorithms/capi/pageRank.h:19-30
   struct SPMVStats            include/algorithms/capi/SPMV.h:19-28
   pageRankGraphCSR / pageRankPullGraphCSR   pageRank.h:69-70
+  pageRank<form>GraphCSR (13 forms)         pageRank.h:71-86
   SPMVGraphCSR / SPMVPullGraphCSR           SPMV.h:51-52
 """
 from __future__ import annotations
@@ -126,7 +127,7 @@ class GraphInfo(C.Structure):
 # constants of include/accelgraph_b200.h
 AG_OK = 0
 AG_ERR_INVALID_ARG, AG_ERR_INVALID_GRAPH, AG_ERR_CUDA, AG_ERR_OOM = -1, -2, -3, -4
-AG_ERR_TIMEOUT, AG_ERR_NO_DEVICE, AG_ERR_UNSUPPORTED = -5, -6, -7
+AG_ERR_TIMEOUT, AG_ERR_NO_DEVICE, AG_ERR_UNSUPPORTED, AG_ERR_DEVICE_WAIT = -5, -6, -7, -8
 AG_BUILD_DEDUPE, AG_BUILD_SORT, AG_BUILD_PINNED, AG_BUILD_WEIGHTS, AG_BUILD_SYMMETRIC = 1, 2, 4, 8, 16
 AG_FILE_TEXT, AG_FILE_BINARY, AG_FILE_CSR = 0, 1, 2
 AG_UPLOAD_WEIGHTS, AG_UPLOAD_VALIDATE, AG_UPLOAD_TRUSTED = 1, 2, 4
@@ -155,6 +156,19 @@ SIGNATURES = [
     ("freePageRankStats", None, [C.POINTER(PageRankStats)]),
     ("pageRankGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
     ("pageRankPullGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPushGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullFixedPoint64BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullFixedPoint32BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullFixedPoint16BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullFixedPoint8BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPushFixedPointGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullQuant32BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullQuant16BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPullQuant8BitGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankPushQuantGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankDataDrivenPullGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankDataDrivenPushGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
+    ("pageRankDataDrivenPullPushGraphCSR", C.POINTER(PageRankStats), [C.POINTER(Arguments), GraphP]),
     ("newSPMVStatsGraphCSR", C.POINTER(SPMVStats), [GraphP]),
     ("freeSPMVStats", None, [C.POINTER(SPMVStats)]),
     ("SPMVGraphCSR", C.POINTER(SPMVStats), [C.POINTER(Arguments), GraphP]),

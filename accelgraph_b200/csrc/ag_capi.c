@@ -197,6 +197,92 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
     return stats;
 }
 
+/* one form of the reference's dispatcher on the GPU: the pull entry with the
+ * form's precision, direction and worklist options; on failure the
+ * reference's failure line and exit, with the form's phase name */
+static struct PageRankStats *run_form(struct Arguments *arguments, struct GraphCSR *graph, int32_t precision,
+                                      int32_t direction, int32_t data_driven, const char *phase)
+{
+    struct PageRankStats *stats = NULL;
+    ag_pr_opts o;
+    ag_status_t st;
+    ag_pr_opts_init(&o);
+    o.precision = precision;
+    o.direction = direction;
+    o.data_driven = data_driven;
+    st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
+    if (st != AG_OK)
+        fail_exit(phase, st);
+    return stats;
+}
+
+/* the reference's per-form entry points (pageRank.h:71-86); each runs the
+ * form that pageRankGraphCSR selects for its pushpull code */
+struct PageRankStats *pageRankPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FP32, AG_DIR_PUSH, 0, "pagerank-push");
+}
+
+struct PageRankStats *pageRankPullFixedPoint64BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FIXED64, AG_DIR_PULL, 0, "pagerank-pull-fp64");
+}
+
+struct PageRankStats *pageRankPullFixedPoint32BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FIXED32, AG_DIR_PULL, 0, "pagerank-pull-fp32");
+}
+
+struct PageRankStats *pageRankPullFixedPoint16BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FIXED16, AG_DIR_PULL, 0, "pagerank-pull-fp16");
+}
+
+struct PageRankStats *pageRankPullFixedPoint8BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FIXED8, AG_DIR_PULL, 0, "pagerank-pull-fp8");
+}
+
+struct PageRankStats *pageRankPushFixedPointGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FIXED64, AG_DIR_PUSH, 0, "pagerank-push-fp64");
+}
+
+struct PageRankStats *pageRankPullQuant32BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_QUANT32, AG_DIR_PULL, 0, "pagerank-pull-quant32");
+}
+
+struct PageRankStats *pageRankPullQuant16BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_QUANT16, AG_DIR_PULL, 0, "pagerank-pull-quant16");
+}
+
+struct PageRankStats *pageRankPullQuant8BitGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_QUANT8, AG_DIR_PULL, 0, "pagerank-pull-quant8");
+}
+
+struct PageRankStats *pageRankPushQuantGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_QUANT32, AG_DIR_PUSH, 0, "pagerank-push-quant32");
+}
+
+struct PageRankStats *pageRankDataDrivenPullGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FP32, AG_DIR_PULL, 1, "pagerank-pull-dd");
+}
+
+struct PageRankStats *pageRankDataDrivenPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FP32, AG_DIR_PUSH, 1, "pagerank-push-dd");
+}
+
+struct PageRankStats *pageRankDataDrivenPullPushGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
+{
+    return run_form(arguments, graph, AG_PREC_FP32, AG_DIR_PULL_PUSH, 1, "pagerank-pull-push-dd");
+}
+
 /* dispatch on arguments->pushpull as pageRank.c:874-939 does: 0 the pull,
  * 1 the push, 2, 9, 10, 11 the 64/32/16/8-bit fixed-point pulls, 3 the
  * fixed-point push, 4, 12, 13 the 32/16/8-bit quantised pulls, 5 the
@@ -205,44 +291,25 @@ struct PageRankStats *pageRankPullGraphCSR(struct Arguments *arguments, struct G
  * case does, with a note on stderr */
 struct PageRankStats *pageRankGraphCSR(struct Arguments *arguments, struct GraphCSR *graph)
 {
-    /* pull variants on the GPU: pushpull code, precision form, phase name of
-     * the failure line */
-    static const struct
-    {
-        uint32_t pushpull;
-        int32_t precision, direction, data_driven;
-        const char *phase;
-    } forms[] = {
-        {1, AG_PREC_FP32, AG_DIR_PUSH, 0, "pagerank-push"},
-        {2, AG_PREC_FIXED64, AG_DIR_PULL, 0, "pagerank-pull-fp64"},
-        {3, AG_PREC_FIXED64, AG_DIR_PUSH, 0, "pagerank-push-fp64"},
-        {4, AG_PREC_QUANT32, AG_DIR_PULL, 0, "pagerank-pull-quant32"},
-        {5, AG_PREC_QUANT32, AG_DIR_PUSH, 0, "pagerank-push-quant32"},
-        {6, AG_PREC_FP32, AG_DIR_PULL, 1, "pagerank-pull-dd"},
-        {7, AG_PREC_FP32, AG_DIR_PUSH, 1, "pagerank-push-dd"},
-        {8, AG_PREC_FP32, AG_DIR_PULL_PUSH, 1, "pagerank-pull-push-dd"},
-        {9, AG_PREC_FIXED32, AG_DIR_PULL, 0, "pagerank-pull-fp32"},
-        {10, AG_PREC_FIXED16, AG_DIR_PULL, 0, "pagerank-pull-fp16"},
-        {11, AG_PREC_FIXED8, AG_DIR_PULL, 0, "pagerank-pull-fp8"},
-        {12, AG_PREC_QUANT16, AG_DIR_PULL, 0, "pagerank-pull-quant16"},
-        {13, AG_PREC_QUANT8, AG_DIR_PULL, 0, "pagerank-pull-quant8"},
+    static struct PageRankStats *(*const forms[14])(struct Arguments *, struct GraphCSR *) = {
+        pageRankPullGraphCSR,
+        pageRankPushGraphCSR,
+        pageRankPullFixedPoint64BitGraphCSR,
+        pageRankPushFixedPointGraphCSR,
+        pageRankPullQuant32BitGraphCSR,
+        pageRankPushQuantGraphCSR,
+        pageRankDataDrivenPullGraphCSR,
+        pageRankDataDrivenPushGraphCSR,
+        pageRankDataDrivenPullPushGraphCSR,
+        pageRankPullFixedPoint32BitGraphCSR,
+        pageRankPullFixedPoint16BitGraphCSR,
+        pageRankPullFixedPoint8BitGraphCSR,
+        pageRankPullQuant16BitGraphCSR,
+        pageRankPullQuant8BitGraphCSR,
     };
-    for (size_t i = 0; arguments && i < sizeof(forms) / sizeof(forms[0]); ++i) {
-        if (arguments->pushpull != forms[i].pushpull)
-            continue;
-        struct PageRankStats *stats = NULL;
-        ag_pr_opts o;
-        ag_status_t st;
-        ag_pr_opts_init(&o);
-        o.precision = forms[i].precision;
-        o.direction = forms[i].direction;
-        o.data_driven = forms[i].data_driven;
-        st = ag_pagerank_pull_ex(arguments, graph, &o, &stats);
-        if (st != AG_OK)
-            fail_exit(forms[i].phase, st);
-        return stats;
-    }
-    if (arguments && arguments->pushpull != 0)
+    if (arguments && arguments->pushpull < 14)
+        return forms[arguments->pushpull](arguments, graph);
+    if (arguments)
         fprintf(stderr, "pageRankGraphCSR: pushpull=%u runs the FP32 pull on the GPU\n", arguments->pushpull);
     return pageRankPullGraphCSR(arguments, graph);
 }

@@ -198,6 +198,8 @@ typedef struct AgPullParams
     float base, damp;
     int wmode;             /* AG_SPMV_W_* */
     uint32_t use_cond;     /* 1: launched by the CUDA graph's WHILE node      */
+    uint32_t mbar_spins;   /* polls of the hot-table copy's mbarrier before the
+                              wait counts as run out (ctl->fault)              */
     uint32_t hot_n;        /* contributions (ids < hot_n) served from shared
                               memory; a multiple of 64                         */
     uint32_t hot_n16;      /* entries of the same table in 16-bit passes       */

@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 ag_bulk_g2s(hot + off, src + off, min(AG_BULK_CHUNK, bytes - off), &s_bar);
         }
         __syncthreads();
-        if (!ag_mbar_wait(&s_bar, 0, 1u << 20)) {
+        if (!ag_mbar_wait(&s_bar, 0, p.mbar_spins)) {
             if (p.ctl)
                 atomicOr(&p.ctl->fault, 1u);
             /* the copies may still be in flight: give them a long, bounded
@@ -1331,6 +1331,7 @@ __global__ void __launch_bounds__(AG_SBLK) ag_pr_init_kernel2(const AgPullParams
         c->low_passes = 0;
         c->t0 = ag_globaltimer();
         c->stop = (run.max_iter > 0 && p.N > 0) ? 0u : 1u;
+        c->fault = 0;
         if (p.use_cond)
             cudaGraphSetConditional(p.cond, (run.max_iter > 0 && p.N > 0) ? 1u : 0u);
     }

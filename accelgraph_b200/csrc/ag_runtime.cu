@@ -1001,10 +1001,26 @@ static ag_status_t ensure_buffers(ag_graph_s *g, int prec)
     return st;
 }
 
+/* polls of the hot-table copy's mbarrier before a pull kernel reports the wait
+ * as run out: AG_MBAR_SPINS (0 allowed: the first wait runs out at once, the
+ * kernel flags it and then waits, bounded, for the copies) or 2^20 */
+static uint32_t mbar_spins(void)
+{
+    const char *env = getenv("AG_MBAR_SPINS");
+    if (env && *env) {
+        char *end = nullptr;
+        const unsigned long v = strtoul(env, &end, 10);
+        if (end && *end == 0 && v <= 0xFFFFFFFFul)
+            return (uint32_t)v;
+    }
+    return 1u << 20;
+}
+
 static AgPullParams base_params(ag_graph_s *g, int exact)
 {
     AgPullParams p;
     memset(&p, 0, sizeof(p));
+    p.mbar_spins = mbar_spins();
     p.row_off = g->row_off;
     p.ids = g->ids;
     p.w = g->w;
@@ -1554,7 +1570,8 @@ extern "C" void ag_pr_opts_init(ag_pr_opts *o)
     memset(o, 0, sizeof(*o));
     o->struct_size = sizeof(*o);
     o->precision = AG_PREC_FP32;
-    o->order = AG_ORDER_FAST;
+    /* the reference's stream-order sums unless the caller asks for FAST */
+    o->order = AG_ORDER_EXACT;
     o->switch_residual = 1e-4;
 }
 
@@ -1700,7 +1717,11 @@ extern "C" ag_status_t ag_pagerank_fetch(ag_graph_t g, float *ranks, ag_pr_resul
             hist_seconds[i] = (double)(hc->hist_t[i] - prev) * 1e-9;
         }
     }
+    const uint32_t fault = hc->fault;
     free(hc);
+    if (fault)
+        return ag_set_error(AG_ERR_DEVICE_WAIT, "a pull kernel's bounded wait for its hot-table copy ran out "
+                            "(the copies completed before the kernel went on; results are filled in)");
     return AG_OK;
 }
 

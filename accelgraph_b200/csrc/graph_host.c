@@ -56,6 +56,7 @@ const char *ag_status_string(ag_status_t s)
     case AG_ERR_TIMEOUT: return "timeout";
     case AG_ERR_NO_DEVICE: return "no CUDA device";
     case AG_ERR_UNSUPPORTED: return "unsupported";
+    case AG_ERR_DEVICE_WAIT: return "device wait ran out";
     default: return "unknown status";
     }
 }

@@ -43,6 +43,10 @@ typedef int32_t ag_status_t;
 #define AG_ERR_TIMEOUT        -5  /* a bounded host wait ran out                  */
 #define AG_ERR_NO_DEVICE      -6  /* no usable CUDA device                        */
 #define AG_ERR_UNSUPPORTED    -7  /* option not available for this input          */
+#define AG_ERR_DEVICE_WAIT    -8  /* a bounded wait inside a kernel ran out (the
+                                     solve still finished; its results are
+                                     returned, but the device was not answering
+                                     in time)                                     */
 
 const char *ag_status_string(ag_status_t status);
 /* Detail of the most recent failure of this thread's last call ("" if none). */
@@ -237,9 +241,14 @@ ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config *best, dou
 #define AG_DIR_PULL_PUSH 2
 
 #define AG_ORDER_FAST  0 /* rows of <= 32 in-edges summed in stream order,
-                            longer rows by a fixed lane-strided tree         */
+                            longer rows by a fixed lane-strided tree: ranks
+                            within 1e-5 relative L1 of the reference's, the
+                            stopping pass not guaranteed equal               */
 #define AG_ORDER_EXACT 1 /* every row summed in stream order: bit-identical
-                            to a sequential binary32 loop                    */
+                            to a sequential binary32 loop, so ranks, active
+                            counts and iterations are the reference's.  The
+                            default of ag_pr_opts_init and of the reference
+                            entry points (pageRank.h)                         */
 
 typedef struct ag_pr_opts
 {
@@ -281,6 +290,8 @@ typedef struct ag_pr_result
     double device_ms;          /* device time of the solve                    */
 } ag_pr_result;
 
+/* Defaults: FP32, EXACT order (the reference's results bit for bit), no warm
+ * start, pull, topology-driven, tables printed, switch_residual 1e-4. */
 void ag_pr_opts_init(ag_pr_opts *opts);
 
 /* Fixed-point gather on a device graph: y[v] = sum of x[u] over v's in-edges,

@@ -23,11 +23,28 @@ def declared_functions():
     return sorted(names)
 
 
+# every CSR entry point of the reference's pageRank.h:32-86 and SPMV.h:30-52
+REFERENCE_CSR_SYMBOLS = (
+    "newPageRankStatsGraphCSR", "freePageRankStats", "pageRankGraphCSR", "pageRankPullGraphCSR",
+    "pageRankPushGraphCSR", "pageRankPullFixedPoint64BitGraphCSR", "pageRankPullFixedPoint32BitGraphCSR",
+    "pageRankPullFixedPoint16BitGraphCSR", "pageRankPullFixedPoint8BitGraphCSR", "pageRankPushFixedPointGraphCSR",
+    "pageRankPullQuant32BitGraphCSR", "pageRankPullQuant16BitGraphCSR", "pageRankPullQuant8BitGraphCSR",
+    "pageRankPushQuantGraphCSR", "pageRankDataDrivenPullGraphCSR", "pageRankDataDrivenPushGraphCSR",
+    "pageRankDataDrivenPullPushGraphCSR",
+    "newSPMVStatsGraphCSR", "freeSPMVStats", "SPMVGraphCSR", "SPMVPullGraphCSR",
+)
+
+
 def test_headers_declare_reference_entry_points():
     names = declared_functions()
-    for ref in ("pageRankGraphCSR", "pageRankPullGraphCSR", "newPageRankStatsGraphCSR", "freePageRankStats",
-                "SPMVGraphCSR", "SPMVPullGraphCSR", "newSPMVStatsGraphCSR", "freeSPMVStats"):
-        assert ref in names
+    missing = [ref for ref in REFERENCE_CSR_SYMBOLS if ref not in names]
+    assert not missing, missing
+
+
+def test_library_exports_every_reference_csr_symbol(ag):
+    lib = C.CDLL(str(ag.LIB_PATH))
+    missing = [n for n in REFERENCE_CSR_SYMBOLS if not hasattr(lib, n)]
+    assert not missing, missing
 
 
 def test_library_exports_every_declared_symbol(ag):
