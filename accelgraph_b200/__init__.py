@@ -181,7 +181,6 @@ SIGNATURES = [
     ("ag_set_stream", C.c_int32, [C.c_void_p]),
     ("ag_synchronize", C.c_int32, [C.c_double]),
     ("ag_num_sms", C.c_int, []),
-    ("ag_probe_gather_rates", C.c_int32, [f64p]),
     ("ag_graph_from_edges", GraphP, [C.c_uint32, C.c_uint64, u32p, u32p, f32p, C.c_uint32]),
     ("ag_graph_rmat", GraphP, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                C.c_uint32]),

@@ -24,7 +24,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libaccelgraph_b200.so"
 
 C_SOURCES = ["graph_host.c", "ag_capi.c"]
-CU_SOURCES = ["ag_pull.cu", "ag_layout.cu", "ag_runtime.cu", "ag_noalloc.cu", "ag_ppr.cu", "ag_mlp.cu", "ag_probe.cu", "ag_plan.cu", "ag_build.cu", "ag_fixed.cu", "ag_push.cu"]
+CU_SOURCES = ["ag_pull.cu", "ag_layout.cu", "ag_runtime.cu", "ag_noalloc.cu", "ag_ppr.cu", "ag_mlp.cu", "ag_plan.cu", "ag_build.cu", "ag_fixed.cu", "ag_push.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

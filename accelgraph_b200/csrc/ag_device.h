@@ -25,6 +25,16 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+/* SMs of the library's device (ag_runtime.cu) */
+extern "C" int ag_num_sms(void);
+
+/* grid cap of a grid-stride kernel: `per_sm` CTAs on every SM of the device */
+static inline unsigned ag_sm_grid(unsigned per_sm)
+{
+    const int n = ag_num_sms();
+    return (unsigned)(n > 0 ? n : 1) * per_sm;
+}
+
 /* ---------------------------------------------------------- tiling */
 #ifndef AG_BLK
 #define AG_BLK 1024       /* threads per CTA of the pull kernel              */

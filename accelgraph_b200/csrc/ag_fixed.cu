@@ -483,7 +483,7 @@ extern "C" const void *ag_quant_kernel_ptr(int bytes)
 static unsigned ag_elem_blocks(uint32_t n)
 {
     unsigned blocks = (n + 255) / 256;
-    return blocks > 148 * 16 ? 148 * 16 : blocks;
+    return blocks > ag_sm_grid(16) ? ag_sm_grid(16) : blocks;
 }
 
 extern "C" cudaError_t ag_permute_uint_in(const uint32_t *perm, const void *x, void *y, uint32_t n, int bytes,

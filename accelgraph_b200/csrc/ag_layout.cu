@@ -128,8 +128,8 @@ __global__ void ag_permute_out_kernel(const uint32_t *inv, const float *y_new, f
 static unsigned grid_for(uint64_t n, unsigned per_block)
 {
     uint64_t g = (n + per_block - 1) / per_block;
-    if (g > 148 * 16)
-        g = 148 * 16;
+    if (g > ag_sm_grid(16))
+        g = ag_sm_grid(16);
     return g ? (unsigned)g : 1u;
 }
 

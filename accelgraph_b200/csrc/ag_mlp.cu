@@ -464,11 +464,11 @@ extern "C" ag_status_t ag_features(ag_graph_t g, float *features)
     uint2 *deg2 = nullptr;
     MCHK(cudaMallocAsync((void **)&deg2, (size_t)gv.N * sizeof(uint2), gv.stream));
     uint64_t blocks = ((uint64_t)gv.N + 255) / 256;
-    if (blocks > 148 * 16)
-        blocks = 148 * 16;
+    if (blocks > ag_sm_grid(16))
+        blocks = ag_sm_grid(16);
     ag_deg2_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2);
     ag_features_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2, features);
-    ag_features_long_kernel<<<148 * 16, 256, 0, gv.stream>>>(gv, deg2, features);
+    ag_features_long_kernel<<<ag_sm_grid(16), 256, 0, gv.stream>>>(gv, deg2, features);
     const cudaError_t e = cudaGetLastError();
     cudaFreeAsync(deg2, gv.stream);
     MCHK(e);
@@ -510,8 +510,8 @@ static ag_status_t mlp_grad(ag_mlp_t m, const float *X, const float *T, uint32_t
     MCHK(cudaMemsetAsync(m->g, 0, AG_MLP_NPARAM * sizeof(float), s));
     MCHK(cudaMemsetAsync(m->loss, 0, sizeof(float), s));
     uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK;
-    if (blocks > 148 * 16)
-        blocks = 148 * 16;
+    if (blocks > ag_sm_grid(16))
+        blocks = ag_sm_grid(16);
     ag_mlp_k1<<<(unsigned)blocks, AG_MLP_BLK, 0, s>>>(m->wb, X, T, n, 1.0f / (float)n, m->buf, m->loss);
     MCHK(cudaGetLastError());
     const size_t smem = AG_MLP_CHUNK * AG_MLP_REC * sizeof(float);
@@ -597,7 +597,7 @@ extern "C" ag_status_t ag_mlp_warm_start_device(ag_graph_t g, ag_mlp_t m, float 
     if (st == AG_OK)
         st = ag_mlp_forward(m, X, gv.N, init_dev);
     if (st == AG_OK) {
-        ag_mlp_to_ranks_kernel<<<148 * 8, 256, 0, s>>>(init_dev, gv.N, 1.0f - Damp, init_dev);
+        ag_mlp_to_ranks_kernel<<<ag_sm_grid(8), 256, 0, s>>>(init_dev, gv.N, 1.0f - Damp, init_dev);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             st = ag_set_error(AG_ERR_CUDA, "ag_mlp_warm_start_device: %s", cudaGetErrorString(e));
@@ -626,7 +626,7 @@ extern "C" ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_r
     if (st == AG_OK)
         st = ag_mlp_forward(m, X, gv.N, Y);
     if (st == AG_OK) {
-        ag_mlp_to_ranks_kernel<<<148 * 8, 256, 0, s>>>(Y, gv.N, 1.0f - Damp, Y);
+        ag_mlp_to_ranks_kernel<<<ag_sm_grid(8), 256, 0, s>>>(Y, gv.N, 1.0f - Damp, Y);
         cudaError_t e = cudaMemcpyAsync(init_ranks, Y, (size_t)gv.N * sizeof(float), cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess)
             st = ag_set_error(AG_ERR_CUDA, "ag_mlp_warm_start: %s", cudaGetErrorString(e));

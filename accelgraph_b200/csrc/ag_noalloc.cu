@@ -16,20 +16,26 @@
  * AG_NOALLOC_HEADER on list them.  In host code the array's name only stands
  * for the symbol; the device address is obtained once per device with
  * cudaGetSymbolAddress on the first call made with that device current, so
- * that first call should come before any stream capture.  Every call shares
- * the array and keeps the previous call's contents: the count is cleared at
- * the start of each call, and two calls whose work overlaps on the GPU race
- * on the list (issue them on one stream, or serialise them).
+ * that first call should come before any stream capture.  The address is kept
+ * for the life of the process: a call after cudaDeviceReset (which unloads
+ * the module) is not supported.  Every call shares the array and keeps the
+ * previous call's contents: the count is cleared at the start of each call,
+ * and two calls whose work overlaps on the GPU race on the list (issue them
+ * on one stream, or serialise them).
  *
  * Work split: kernel 1 gives each row of <= AG_NOALLOC_SPLIT in-edges to one
  * warp (lane-strided partial sums, fixed xor tree) and appends every longer
  * row to the list; kernel 2 gives each listed row to one CTA (thread-strided
  * partials, fixed-order CTA reduction).  Results do not depend on the list
- * order.  Arithmetic per edge matches the pull kernel: one binary32 multiply
- * w * x[u] (no multiply in unit mode), then binary32 adds.
+ * order.  A long row that finds the list full (only when the caller's
+ * num_edges understates the graph) is summed by its warp in kernel 1 instead:
+ * slower, never dropped.  Arithmetic per edge matches the pull kernel: one
+ * binary32 multiply w * x[u] (no multiply in unit mode), then binary32 adds.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
 
 #include "ag_internal.h"
 
@@ -68,12 +74,15 @@ __global__ void __launch_bounds__(AG_NOALLOC_BLK) ag_na_rows_kernel(uint32_t n, 
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
         const uint32_t b = __ldg(row_off + r), e = __ldg(row_off + r + 1);
         if (e - b > AG_NOALLOC_SPLIT) {
+            uint32_t k = 0;
             if (lane == 0) {
-                const uint32_t k = atomicAdd(scratch, 1u);
+                k = atomicAdd(scratch, 1u);
                 if (k < AG_NOALLOC_MAX_LONG)
                     scratch[AG_NOALLOC_HEADER + k] = r;
             }
-            continue;
+            /* listed: kernel 2 sums it; the list is full: this warp does */
+            if (__shfl_sync(0xffffffffu, k, 0) < AG_NOALLOC_MAX_LONG)
+                continue;
         }
         float s = 0.0f;
         for (uint32_t j = b + lane; j < e; j += 32)
@@ -110,11 +119,14 @@ __global__ void __launch_bounds__(AG_NOALLOC_BLK) ag_na_long_kernel(const uint32
     }
 }
 
-/* device address of the scratch array, looked up once per device */
+/* device address of the scratch array and the SM count, looked up once per
+ * device (atomic: concurrent first calls from several host threads store the
+ * same values) */
 #define AG_NOALLOC_MAX_DEVICES 64
-static uint32_t *g_na_scratch[AG_NOALLOC_MAX_DEVICES];
+static std::atomic<uint32_t *> g_na_scratch[AG_NOALLOC_MAX_DEVICES];
+static std::atomic<int> g_na_sms[AG_NOALLOC_MAX_DEVICES];
 
-static ag_status_t na_scratch(uint32_t **out)
+static ag_status_t na_scratch(uint32_t **out, int *sms)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -125,17 +137,24 @@ static ag_status_t na_scratch(uint32_t **out)
     if (dev < 0 || dev >= AG_NOALLOC_MAX_DEVICES)
         return ag_set_error(AG_ERR_UNSUPPORTED, "ag_spmv_pull_noalloc: device %d beyond %d", dev,
                             AG_NOALLOC_MAX_DEVICES);
-    if (!g_na_scratch[dev]) {
+    uint32_t *cached = g_na_scratch[dev].load(std::memory_order_acquire);
+    if (!cached) {
         void *p = nullptr;
+        int n = 0;
         e = cudaGetSymbolAddress(&p, ag_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess || !p || n <= 0) {
             cudaGetLastError();
-            return ag_set_error(AG_ERR_CUDA, "ag_spmv_pull_noalloc: cudaGetSymbolAddress failed: %s",
+            return ag_set_error(AG_ERR_CUDA, "ag_spmv_pull_noalloc: device set-up failed: %s",
                                 cudaGetErrorString(e));
         }
-        g_na_scratch[dev] = (uint32_t *)p;
+        g_na_sms[dev].store(n, std::memory_order_relaxed);
+        cached = (uint32_t *)p;
+        g_na_scratch[dev].store(cached, std::memory_order_release);
     }
-    *out = g_na_scratch[dev];
+    *out = cached;
+    *sms = g_na_sms[dev].load(std::memory_order_relaxed);
     return AG_OK;
 }
 
@@ -148,6 +167,9 @@ extern "C" ag_status_t ag_spmv_pull_noalloc(uint32_t num_vertices, uint32_t num_
         return AG_OK;
     if (!row_off || !x || !y || (num_edges && !ids))
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_noalloc: NULL argument");
+    if (mode & ~AG_SPMV_UNIT)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_noalloc: mode %u: only AG_SPMV_GRAPH_WEIGHTS (0) and "
+                            "AG_SPMV_UNIT (1); the stream-order form (AG_SPMV_EXACT) needs ag_spmv_pull", mode);
     if ((uint64_t)num_edges > (uint64_t)AG_NOALLOC_MAX_LONG * AG_NOALLOC_SPLIT)
         return ag_set_error(AG_ERR_UNSUPPORTED,
                             "ag_spmv_pull_noalloc: %u in-edges exceed the fixed scratch (at most %llu edges: "
@@ -155,18 +177,19 @@ extern "C" ag_status_t ag_spmv_pull_noalloc(uint32_t num_vertices, uint32_t num_
                             num_edges, (unsigned long long)AG_NOALLOC_MAX_LONG * AG_NOALLOC_SPLIT,
                             AG_NOALLOC_MAX_LONG, AG_NOALLOC_SPLIT);
     uint32_t *scratch = nullptr;
-    ag_status_t st = na_scratch(&scratch);
+    int sms = 0;
+    ag_status_t st = na_scratch(&scratch, &sms);
     if (st != AG_OK)
         return st;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t), s);
     if (e == cudaSuccess) {
         uint64_t blocks = ((uint64_t)num_vertices * 32 + AG_NOALLOC_BLK - 1) / AG_NOALLOC_BLK;
-        if (blocks > 148ull * 16)
-            blocks = 148ull * 16;
+        if (blocks > (uint64_t)sms * 16)
+            blocks = (uint64_t)sms * 16;
         ag_na_rows_kernel<<<(unsigned)blocks, AG_NOALLOC_BLK, 0, s>>>(num_vertices, row_off, ids, w, x, y, mode,
                                                                        scratch);
-        ag_na_long_kernel<<<148 * 4, AG_NOALLOC_BLK, 0, s>>>(row_off, ids, w, x, y, mode, scratch);
+        ag_na_long_kernel<<<(unsigned)sms * 4, AG_NOALLOC_BLK, 0, s>>>(row_off, ids, w, x, y, mode, scratch);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

@@ -202,7 +202,7 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     AgPprParams p;
     memset(&p, 0, sizeof(p));
     const unsigned grid_rows = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>(((uint64_t)gv.N * 32 + AG_PPR_BLK - 1) / AG_PPR_BLK, 148ull * 8));
+        1, std::min<uint64_t>(((uint64_t)gv.N * 32 + AG_PPR_BLK - 1) / AG_PPR_BLK, (uint64_t)ag_sm_grid(8)));
 #define PCHK(call)                                                                                       \
     do {                                                                                                 \
         err = (call);                                                                                    \
@@ -264,7 +264,7 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     PCHK(cudaEventRecord(e1, s));
     if (ranks) {
         PCHK(cudaMallocAsync((void **)&out, (size_t)gv.N * k * sizeof(float), s));
-        ag_ppr_output_kernel<<<148 * 8, 256, 0, s>>>(p, gv.perm, out);
+        ag_ppr_output_kernel<<<ag_sm_grid(8), 256, 0, s>>>(p, gv.perm, out);
         PCHK(cudaGetLastError());
         PCHK(cudaMemcpyAsync(ranks, out, (size_t)gv.N * k * sizeof(float), cudaMemcpyDeviceToHost, s));
     }

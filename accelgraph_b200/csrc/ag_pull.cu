@@ -1461,8 +1461,8 @@ extern "C" cudaError_t ag_validate_ids(const uint32_t *ids, uint64_t E, uint32_t
     if (E == 0)
         return cudaSuccess;
     uint64_t blocks = (E + 255) / 256;
-    if (blocks > 148 * 32)
-        blocks = 148 * 32;
+    if (blocks > ag_sm_grid(32))
+        blocks = ag_sm_grid(32);
     ag_validate_ids_kernel<<<(unsigned)blocks, 256, 0, s>>>(ids, E, N, flag);
     return cudaGetLastError();
 }
@@ -1471,7 +1471,7 @@ extern "C" cudaError_t ag_pr_f64_run(const uint32_t *row_off, const uint32_t *id
                                      uint32_t max_iter, double tol, double *r, double *r2, double *c,
                                      double *maxdiff_dev, uint32_t *passes_out, cudaStream_t s)
 {
-    const unsigned gb = 148 * 8;
+    const unsigned gb = ag_sm_grid(8);
     double *const r_final = r;
     uint32_t it = 0;
     cudaError_t e;

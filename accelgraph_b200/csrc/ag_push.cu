@@ -381,8 +381,8 @@ extern "C" cudaError_t ag_forward_build(const uint32_t *row_off, const uint32_t 
     if (err != cudaSuccess)
         return err;
     unsigned blocks = (e + 255) / 256;
-    if (blocks > 148 * 32)
-        blocks = 148 * 32;
+    if (blocks > ag_sm_grid(32))
+        blocks = ag_sm_grid(32);
     ag_edge_rows_kernel<<<blocks, 256, 0, s>>>(row_off, n, e, rows);
     err = cudaGetLastError();
     /* stable by source: each source's destinations stay in row order */

@@ -743,14 +743,26 @@ def run_rows(a):
 
 
 def run_gather_probe(a):
-    """Random 4-byte gather rates of this device (ag_probe_gather_rates)."""
+    """Random 4-byte gather rates of this device: tests/probe/gather_probe.cu,
+    a measuring aid outside the library, built here into its own
+    libgather_probe.so (sm_100a) when missing or older than its source."""
     import numpy as np
-    ag = _gpu_setup()
+    import torch
+    torch.cuda.set_device(0)
+    src = ROOT / "tests" / "probe" / "gather_probe.cu"
+    lib = src.with_name("libgather_probe.so")
+    if not lib.exists() or lib.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-shared",
+                        "-Xcompiler", "-fPIC", "-o", str(lib), str(src)], check=True)
+    probe = C.CDLL(str(lib))
+    probe.gather_probe_rates.argtypes = [C.POINTER(C.c_double)]
     r = np.zeros(6)
-    ag.check(ag.lib.ag_probe_gather_rates(r.ctypes.data_as(ag.f64p)), "ag_probe_gather_rates")
+    rc = probe.gather_probe_rates(r.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"gather_probe_rates: CUDA error {rc}")
     names = ["shared_64KB", "global_L1_256KB", "global_L2_64MB", "global_HBM_256MB", "texture_L2_64MB",
              "cluster_shared_8x160KB"]
-    sms = ag.lib.ag_num_sms()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
     print(json.dumps({"workload": "random 4-byte gathers, 1024 threads/SM, 8 in flight per thread",
                       "gathers_per_s": dict(zip(names, r.tolist())),
                       "per_clock_per_sm_at_1.9GHz": dict(zip(names, (r / sms / 1.9e9).round(3).tolist()))}),

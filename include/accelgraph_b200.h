@@ -69,11 +69,6 @@ ag_status_t ag_set_stream(void *stream);
 ag_status_t ag_synchronize(double timeout_s);
 /* Number of streaming multiprocessors of the library's device (0 if none). */
 int ag_num_sms(void);
-/* Device probe of random 4-byte gather rates (gathers per second), the
- * quantity that bounds a pull pass: rates[0..5] = shared memory, L1-resident,
- * L2-resident, HBM-resident, L2-resident through textures, distributed shared
- * memory of an 8-CTA cluster.  Allocates and frees 256 MB. */
-ag_status_t ag_probe_gather_rates(double *rates);
 
 /* ------------------------------------------------- host graph substrate */
 #define AG_BUILD_DEDUPE   1u  /* drop self loops and duplicate edges; implies SORT */
@@ -437,16 +432,18 @@ ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint32_t mode);
  * Inputs and outputs are caller-owned DEVICE pointers: row_off[num_vertices+1]
  * (inverse-CSR row starts), ids[num_edges] (in-neighbours), w[num_edges] (or
  * NULL: the reference's unweighted 0.0001f), x and y[num_vertices]; mode is
- * AG_SPMV_GRAPH_WEIGHTS or AG_SPMV_UNIT; stream is a cudaStream_t (NULL: the
- * legacy default stream).  The work is enqueued on that stream and the call
- * returns without waiting.
+ * AG_SPMV_GRAPH_WEIGHTS or AG_SPMV_UNIT (any other bit, AG_SPMV_EXACT
+ * included, is rejected with AG_ERR_INVALID_ARG); stream is a cudaStream_t
+ * (NULL: the legacy default stream).  The work is enqueued on that stream and
+ * the call returns without waiting.
  * Limit: its only scratch is a fixed 256 KB device array listing the rows of
  * more than 4096 in-edges (at most 65536 of them), so num_edges must be at
  * most 2^28; larger inputs are rejected with AG_ERR_UNSUPPORTED.  Every GPU
  * that loads the library holds that array until the process exits.  The
  * first call on a device looks up the array's device address, so make it
- * before any stream capture.  All calls share the array: calls whose work
- * overlaps on the GPU race, so issue them on one stream. */
+ * before any stream capture; the address is kept for the process, so a call
+ * after cudaDeviceReset is not supported.  All calls share the array: calls
+ * whose work overlaps on the GPU race, so issue them on one stream. */
 ag_status_t ag_spmv_pull_noalloc(uint32_t num_vertices, uint32_t num_edges, const uint32_t *row_off,
                                  const uint32_t *ids, const float *w, const float *x, float *y,
                                  uint32_t mode, void *stream);

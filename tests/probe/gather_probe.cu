@@ -1,6 +1,8 @@
 /*
- * ag_probe.cu -- device probe of random 4-byte gather rates, the quantity
- * that bounds a pull pass (every in-edge is one random gather).
+ * gather_probe.cu -- device probe of random 4-byte gather rates, the quantity
+ * that bounds a pull pass (every in-edge is one random gather).  A measuring
+ * aid, not part of the library: bench.py --workload gather-probe builds it into
+ * its own libgather_probe.so (tests/probe/) and calls gather_probe_rates.
  *
  * Each probe kernel runs one 1024-thread CTA per SM (clusters of 8 for the
  * distributed case); every thread issues 256 x 8 gathers with indexes from an
@@ -13,8 +15,6 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
-
-#include "ag_internal.h"
 
 namespace cg = cooperative_groups;
 
@@ -94,21 +94,26 @@ __global__ void __cluster_dims__(AG_PB_CL, 1, 1) __launch_bounds__(AG_PB_BLK, 1)
 }
 
 /* rates[0..5] = gathers/s from: shared memory, L1-resident, L2-resident,
- * HBM-resident, L2-resident through textures, cluster shared memory */
-extern "C" ag_status_t ag_probe_gather_rates(double *rates)
+ * HBM-resident, L2-resident through textures, cluster shared memory, on the
+ * current device.  Returns 0 or the failing call's cudaError_t. */
+extern "C" int gather_probe_rates(double *rates)
 {
-    ag_clear_error();
     if (!rates)
-        return ag_set_error(AG_ERR_INVALID_ARG, "ag_probe_gather_rates: NULL output");
-    cudaStream_t s = (cudaStream_t)ag_stream();
-    if (!s)
-        return ag_set_error(AG_ERR_NO_DEVICE, "ag_probe_gather_rates: no device");
-    const int nsm = ag_num_sms();
+        return (int)cudaErrorInvalidValue;
+    int dev = 0, nsm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess)
+        return (int)e;
+    cudaStream_t s = nullptr;
+    if ((e = cudaStreamCreate(&s)) != cudaSuccess)
+        return (int)e;
     const uint32_t n = 1u << 26; /* 256 MB */
     float *src = nullptr, *out = nullptr;
     cudaTextureObject_t tex = 0;
     cudaEvent_t a = nullptr, b = nullptr;
-    cudaError_t e = cudaMalloc((void **)&src, (size_t)n * 4);
+    e = cudaMalloc((void **)&src, (size_t)n * 4);
     if (e == cudaSuccess)
         e = cudaMalloc((void **)&out, (size_t)nsm * AG_PB_BLK * 4);
     if (e == cudaSuccess)
@@ -169,9 +174,8 @@ extern "C" ag_status_t ag_probe_gather_rates(double *rates)
         cudaEventDestroy(b);
     cudaFree(src);
     cudaFree(out);
-    if (e != cudaSuccess) {
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess)
         cudaGetLastError();
-        return ag_set_error(AG_ERR_CUDA, "ag_probe_gather_rates: %s", cudaGetErrorString(e));
-    }
-    return AG_OK;
+    return (int)e;
 }
