@@ -229,6 +229,9 @@ SIGNATURES = [
     ("ag_graph_upload_rows", C.c_int32, [GraphP, u32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.POINTER(C.c_void_p)]),
     ("ag_partition_init", C.c_int32, [C.c_void_p, C.c_void_p]),
+    ("ag_partition_step", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_void_p,
+                                      C.c_void_p]),
+    ("ag_partition_close", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ag_partition_pass", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     ("ag_partition_fetch", C.c_int32, [C.c_void_p, f32p]),
     ("ag_ppr_spmm", C.c_int32, [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_double, f32p, C.POINTER(PRResult)]),

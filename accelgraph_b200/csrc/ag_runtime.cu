@@ -2273,6 +2273,75 @@ extern "C" ag_status_t ag_partition_pass(ag_graph_t g, const float *c_in_full, f
     return AG_OK;
 }
 
+/* the pass of a solve driven by a device stop flag: state[0] != 0 makes the
+ * pull kernel return at once and the statistics zero */
+__global__ void ag_partition_step_setup_kernel(AgControl *c, double eps, const uint32_t *state)
+{
+    c->iter = 0;
+    c->max_iter = AG_MAX_HISTORY;
+    c->active_acc = 0;
+    c->done_ctas = 0;
+    c->err_acc = 0.0;
+    c->eps = eps;
+    c->stop = state[0] ? 1u : 0u;
+    c->mode_read = 0;
+    c->mode_write = 0;
+    c->hist_active[0] = 0;
+    c->last_err_sum = 0.0;
+}
+
+__global__ void ag_partition_close_kernel(const double *stats, uint32_t *state, double *err)
+{
+    if (state[0])
+        return;
+    state[1] += 1;
+    *err = stats[1];
+    if (stats[0] == 0.0) {
+        state[0] = 1;
+        state[2] = 1;
+    }
+}
+
+extern "C" ag_status_t ag_partition_step(ag_graph_t g, const float *c_in_full, float *c_out_full, double epsilon,
+                                         int32_t order, double *stats_dev, const uint32_t *state_dev)
+{
+    ag_clear_error();
+    if (!g || !c_in_full || !c_out_full || !stats_dev || !state_dev || !g->norm_n)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_step: not a row partition / NULL argument");
+    if (order != AG_ORDER_FAST && order != AG_ORDER_EXACT)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_step: order %d", order);
+    cudaStream_t s = g_ctx.stream;
+    ag_partition_step_setup_kernel<<<1, 1, 0, s>>>(g->ctl, epsilon, state_dev);
+    AG_CUDA(cudaGetLastError());
+    if (g->N) {
+        const int exact = order == AG_ORDER_EXACT;
+        AgPullParams p = base_params(g, exact);
+        p.c32_0 = const_cast<float *>(c_in_full);
+        p.c32_1 = c_out_full;
+        p.use_cond = 0;
+        const void *k = ag_pull_kernel_ptr(AG_MODE_PR, 0, exact);
+        const unsigned grid = pull_grid(k, p.ntasks, pull_smem(g));
+        void *args[1] = {&p};
+        AG_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(AG_BLK), args, pull_smem(g), s));
+    }
+    ag_partition_stats_kernel<<<1, 1, 0, s>>>(g->ctl, stats_dev);
+    AG_CUDA(cudaGetLastError());
+    return AG_OK;
+}
+
+extern "C" ag_status_t ag_partition_close(const double *stats_dev, uint32_t *state_dev, double *err_dev)
+{
+    ag_clear_error();
+    if (!stats_dev || !state_dev || !err_dev)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_partition_close: NULL argument");
+    ag_status_t st = ctx_ensure(-1);
+    if (st != AG_OK)
+        return st;
+    ag_partition_close_kernel<<<1, 1, 0, g_ctx.stream>>>(stats_dev, state_dev, err_dev);
+    AG_CUDA(cudaGetLastError());
+    return AG_OK;
+}
+
 /* this rank's ranks divided by the global vertex count (host array) */
 extern "C" ag_status_t ag_partition_fetch(ag_graph_t g, float *ranks_local)
 {

@@ -359,10 +359,24 @@ ag_status_t ag_graph_upload_rows(const struct GraphCSR *graph, const uint32_t *b
 /* ranks start at base_pr; writes this rank's first contributions into its
  * slice of c_full (device) */
 ag_status_t ag_partition_init(ag_graph_t g, float *c_full);
-/* one pass; stats_dev (device, 2 doubles) receives this rank's active count
- * and sum of |r' - r| */
+/* one pass (FAST order); stats_dev (device, 2 doubles) receives this rank's
+ * active count and sum of |r' - r| */
 ag_status_t ag_partition_pass(ag_graph_t g, const float *c_in_full, float *c_out_full, double epsilon,
                               double *stats_dev);
+/* A solve whose loop needs no host round trip per pass.  state_dev (device,
+ * 3 uint32: stop, passes, converged; zeroed by the caller before the solve)
+ * is shared by the two calls:
+ *  - ag_partition_step: one pass in `order` (AG_ORDER_*), the same as
+ *    ag_partition_pass, except that once state_dev[0] is set the pass does
+ *    nothing and stats_dev is {0, 0};
+ *  - ag_partition_close, after the caller's all-reduce of stats_dev: counts
+ *    the pass, keeps its error sum in err_dev (device double) and sets the stop
+ *    flag when no vertex of any rank was active.
+ * All ranks issue the same calls and collectives every pass; the host reads
+ * state_dev when it wants to know whether to stop (every few passes). */
+ag_status_t ag_partition_step(ag_graph_t g, const float *c_in_full, float *c_out_full, double epsilon,
+                              int32_t order, double *stats_dev, const uint32_t *state_dev);
+ag_status_t ag_partition_close(const double *stats_dev, uint32_t *state_dev, double *err_dev);
 /* this rank's ranks / num_vertices (host array of bounds[r+1] - bounds[r]) */
 ag_status_t ag_partition_fetch(ag_graph_t g, float *ranks_local);
 

@@ -64,6 +64,8 @@ def _load() -> C.CDLL:
     lib.oracle_rmat_inverse.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                         u32p, u32p, u32p, u32p]
     lib.oracle_rmat_inverse.restype = C.c_uint64
+    lib.oracle_partition_pass.argtypes = [C.c_uint32, C.c_uint32, u32p, u32p, u32p, u32p, u32p, f32p, f32p, f32p,
+                                          C.c_double, f64p]
     return lib
 
 
@@ -93,6 +95,22 @@ def rmat_inverse(scale, edge_factor, seed, a=0.57, b=0.19, c=0.19):
     if e == 2 ** 64 - 1:
         raise MemoryError("oracle_rmat_inverse: allocation failed")
     return {"in_idx": in_idx, "in_deg": in_deg, "in_nb": in_nb[:e], "out_deg": out_deg, "num_edges": int(e)}
+
+
+def partition_pass(rb, re, in_idx, in_deg, in_nb, out_deg, pos, c_in_full, c_out_full, rank_local, eps):
+    """One pull pass over rows [rb, re) of a row partition (contribution of u
+    at pos[u]); updates rank_local and the rows' entries of c_out_full in
+    place; returns [active rows, sum of |r' - r|]."""
+    in_idx, in_deg, in_nb = _csr(in_idx, in_deg, in_nb)
+    out_deg = np.ascontiguousarray(out_deg, np.uint32)
+    pos = np.ascontiguousarray(pos, np.uint32)
+    for a in (c_in_full, c_out_full, rank_local):
+        assert a.dtype == np.float32 and a.flags.c_contiguous
+    stats = np.zeros(2, np.float64)
+    lib.oracle_partition_pass(rb, re, _p(in_idx, u32p), _p(in_deg, u32p), _p(in_nb, u32p), _p(out_deg, u32p),
+                              _p(pos, u32p), _p(c_in_full, f32p), _p(c_out_full, f32p), _p(rank_local, f32p), eps,
+                              _p(stats, f64p))
+    return stats
 
 
 def gather(in_idx, in_deg, in_nb, x, threads=0):

@@ -906,3 +906,35 @@ uint64_t oracle_rmat_inverse(uint32_t scale, uint32_t edge_factor, double a, dou
     in_idx[N] = (uint32_t)off;
     return E;
 }
+
+/* One pull pass of a row partition (the multi-GPU solve's per-rank step):
+ * rows [rb, re) of the inverse CSR, with the contribution of vertex u at
+ * pos[u] of the rank-padded vectors c_in_full / c_out_full.  Each row is summed
+ * in stream order as in oracle_pagerank_pull (binary32 from 0.0f), then the
+ * update of pageRank.c:1055-1069 (binary32 multiply and add, |r' - r| in
+ * binary32 compared in binary64) and the next contribution written at pos[v].
+ * rank_local[v - rb] holds the rows' un-normalised ranks.  stats[0] = rows
+ * that moved by at least eps, stats[1] = sum of |r' - r|. */
+void oracle_partition_pass(uint32_t rb, uint32_t re, const uint32_t *in_idx, const uint32_t *in_deg,
+                           const uint32_t *in_nb, const uint32_t *out_deg, const uint32_t *pos,
+                           const float *c_in_full, float *c_out_full, float *rank_local, double eps, double *stats)
+{
+    const float damp = ORACLE_DAMP;
+    const float base_pr = (1.0f - damp);
+    double err_sum = 0.0;
+    uint32_t active = 0;
+    for (uint32_t v = rb; v < re; ++v) {
+        float s = 0.0f;
+        for (uint32_t j = in_idx[v]; j < in_idx[v] + in_deg[v]; ++j)
+            s += c_in_full[pos[in_nb[j]]];
+        const float next = base_pr + (damp * s);
+        const double err = fabs(next - rank_local[v - rb]);
+        err_sum += err;
+        if (err >= eps)
+            active++;
+        rank_local[v - rb] = next;
+        c_out_full[pos[v]] = out_deg[v] ? next / (float)out_deg[v] : 0.0f;
+    }
+    stats[0] = (double)active;
+    stats[1] = err_sum;
+}

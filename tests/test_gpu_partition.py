@@ -25,10 +25,15 @@ def test_rows_partition_single_rank_matches_oracle(gpu, oracle):
                             timeout=datetime.timedelta(seconds=120))
     try:
         g = ag.Graph.rmat(13, 16)
-        ranks, (rb, re), info = agd.pagerank_rows_gpu(g, iterations=60, epsilon=1e-4)
         ref = oracle.pagerank_pull(g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree(), 60, 1e-4)
+        # EXACT order (the default): the oracle's ranks bit for bit; the loop
+        # stops on the device flag, read every 8 passes
+        ranks, (rb, re), info = agd.pagerank_rows_gpu(g, iterations=60, epsilon=1e-4)
         assert (rb, re) == (0, g.num_vertices)
-        assert info["iterations"] == ref["iterations"]
+        assert info["iterations"] == ref["iterations"] and info["passes"] == ref["passes"]
+        assert info["converged"] == (ref["iterations"] < 60)
+        assert np.array_equal(ranks.view(np.uint32), ref["ranks"].view(np.uint32))
+        ranks, _, info = agd.pagerank_rows_gpu(g, iterations=60, epsilon=1e-4, exact=False)
         assert np.abs(ranks.astype(np.float64) - ref["ranks"]).sum() / ref["ranks"].sum() <= 1e-5
     finally:
         dist.destroy_process_group()

@@ -51,9 +51,12 @@ def test_reduce_time_work_single_process():
 
 
 def _partition_worker(rank, world, port, out):
-    """The partitioned loop of accelgraph_b200.distributed on two gloo ranks,
-    with a CPU pass that sums every row in stream order (binary32) over the
-    padded global ids: the result must equal the single-process oracle."""
+    """The partitioned loop of accelgraph_b200.distributed on two gloo ranks:
+    the product's loop (solve), in-place all-gather of the contribution
+    slices, all-reduce of the pass statistics and the stop rule of
+    ag_partition_close, with the oracle's row-range pass
+    (oracle_partition_pass, C) in place of the GPU kernel.  The result must
+    equal the single-process oracle."""
     import datetime
 
     import numpy as np
@@ -61,6 +64,7 @@ def _partition_worker(rank, world, port, out):
     import torch.distributed as dist
 
     import accelgraph_b200 as ag
+    import oracle
     from accelgraph_b200 import distributed as agd
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -69,50 +73,46 @@ def _partition_worker(rank, world, port, out):
     n = g.num_vertices
     bounds, slice_ = agd.partition_bounds(g.in_degree(), world)
     rb, re = int(bounds[rank]), int(bounds[rank + 1])
-    owner = np.zeros(n, np.int64)
+    pos = np.zeros(n, np.uint32)
     for r in range(world):
-        owner[bounds[r]:bounds[r + 1]] = r * slice_ + np.arange(bounds[r + 1] - bounds[r])
+        pos[bounds[r]:bounds[r + 1]] = r * slice_ + np.arange(bounds[r + 1] - bounds[r])
     idx, deg, nb, od = g.in_edges_idx(), g.in_degree(), g.in_neighbours(), g.out_degree()
     f = np.float32
-    base, damp = f(f(1.0) - f(0.85)), f(0.85)
+    base = f(f(1.0) - f(0.85))
     r_local = np.full(re - rb, base, np.float32)
+    state = {"stop": False, "passes": 0, "converged": False, "err": 0.0}
 
-    def contrib(v_local):
-        o = od[rb + v_local]
-        return f(r_local[v_local] / f(o)) if o else f(0.0)
-
-    def init_fn(_):
+    def init_fn():
         bufs = [torch.zeros(world * slice_, dtype=torch.float32) for _ in range(2)]
-        for i in range(re - rb):
-            bufs[0][rank * slice_ + i] = float(contrib(i))
+        o = od[rb:re]
+        c0 = np.where(o > 0, r_local / np.maximum(o, 1).astype(np.float32), f(0.0)).astype(np.float32)
+        bufs[0][rank * slice_:rank * slice_ + (re - rb)] = torch.from_numpy(c0)
         return bufs
 
     def pass_fn(c_in, c_out, eps):
-        cin = c_in.numpy()
-        active, err = 0, 0.0
-        for i in range(re - rb):
-            v = rb + i
-            s = f(0.0)
-            for j in range(idx[v], idx[v] + deg[v]):
-                s = f(s + cin[owner[nb[j]]])
-            new = f(base + f(damp * s))
-            e = abs(float(f(new - r_local[i])))
-            err += e
-            active += e >= eps
-            r_local[i] = new
-            c_out[rank * slice_ + i] = float(contrib(i))
-        return torch.tensor([float(active), err], dtype=torch.float64)
+        if state["stop"]:
+            return torch.zeros(2, dtype=torch.float64)
+        st = oracle.partition_pass(rb, re, idx, deg, nb, od, pos, c_in.numpy(), c_out.numpy(), r_local, eps)
+        return torch.from_numpy(st)
 
     def allgather_fn(c):
-        parts = [torch.zeros(slice_, dtype=torch.float32) for _ in range(world)]
-        dist.all_gather(parts, c[rank * slice_:(rank + 1) * slice_].clone())
-        c.copy_(torch.cat(parts))
+        dist.all_gather_into_tensor(c, c[rank * slice_:(rank + 1) * slice_])
 
     def allreduce_fn(st):
         dist.all_reduce(st)
-        return int(st[0].item()), float(st[1].item())
 
-    its, passes, conv, err = agd.solve(rank, world, slice_, init_fn, pass_fn, allgather_fn, allreduce_fn, 30, 1e-4)
+    def close_fn(st):
+        # the rule of ag_partition_close_kernel
+        if state["stop"]:
+            return
+        state["passes"] += 1
+        state["err"] = float(st[1])
+        if float(st[0]) == 0.0:
+            state["stop"] = state["converged"] = True
+
+    its, passes, conv, err = agd.solve(init_fn, pass_fn, allgather_fn, allreduce_fn, close_fn,
+                                       lambda: state["stop"],
+                                       lambda: (state["passes"], state["converged"], state["err"]), 30, 1e-4)
     out[rank] = (its, passes, rb, re, (r_local / f(n)).astype(np.float32).tobytes())
     dist.barrier()
     dist.destroy_process_group()
