@@ -514,14 +514,26 @@ struct AgPass
         return (uint32_t)__float2int_rn(x);
     }
 
-    /* EXACT-order hub chunk after the first: stages the gathered values of
-     * in-edges [eb, ee) of the row starting at o0 at dst[j - o0], and writes
+    /* whether a hub chunk after the first stages its gathered values, from
+     * its record of the pass before (hub_pred): when its starting binade is
+     * unknown or it had a round added value by value.  The composing warp
+     * re-gathers an unstaged round if it needs one after all.  SpMV and
+     * 16-bit passes always stage. */
+    static __device__ __forceinline__ bool hub_staged(uint32_t pr)
+    {
+        const uint32_t e = pr & 0xffu;
+        return MODE == AG_MODE_SPMV || PREC != 0 || e < 24u || e > 253u || (pr & AG_XFELL) != 0u;
+    }
+
+    /* EXACT-order hub chunk after the first: stages (when `stage`) the
+     * gathered values of in-edges [eb, ee) of the row starting at o0 at
+     * dst[j - o0], and writes
      * per round the totals of its integer steps at binade e and e + 1
      * (words[2k], words[2k+1]; AG_XNOT when they do not apply or e is
      * unknown) and the chunk's sign tag (words[AG_XWORDS - 1]).  The next
      * round's gathers are in flight while a round's steps are summed. */
     __device__ __forceinline__ void hub_steps(float *dst, uint32_t o0, uint32_t eb, uint32_t ee, uint32_t lane,
-                                              const Pair &first, uint32_t e, uint32_t *words) const
+                                              const Pair &first, uint32_t e, bool stage, uint32_t *words) const
     {
         const uint32_t q1 = (ee + 3u) >> 2;
         const bool known = (e >= 24u) & (e <= 253u);
@@ -537,15 +549,17 @@ struct AgPass
             float v[8];
             bool in[8];
             gather8(cur, qa, eb, ee, v, in);
-            const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
+            if (stage) {
+                const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (in[i])
-                    dst[ja + i - o0] = v[i];
+                for (int i = 0; i < 4; ++i)
+                    if (in[i])
+                        dst[ja + i - o0] = v[i];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (in[4 + i])
-                    dst[jb + i - o0] = v[4 + i];
+                for (int i = 0; i < 4; ++i)
+                    if (in[4 + i])
+                        dst[jb + i - o0] = v[4 + i];
+            }
             if (known && k < AG_XROUNDS) {
                 uint32_t t0 = 0, t1 = 0;
                 bool b0 = false, b1 = false;
@@ -604,9 +618,9 @@ struct AgPass
     /* static, with plain arguments: a call of a member would need the
      * kernel's parameter block in local memory */
     static __device__ __noinline__ XSum hub_compose(const uint32_t *hub_part, const uint32_t *hub_t,
-                                                    uint32_t *hub_pred, const float *row_vals, float *vals,
-                                                    uint32_t whub, uint32_t o0, uint32_t deg, uint32_t pbase,
-                                                    uint32_t nch, uint32_t lane)
+                                                    uint32_t *hub_pred, const float *row_vals, const uint32_t *ids,
+                                                    const float *c_in, float *vals, uint32_t whub, uint32_t o0,
+                                                    uint32_t deg, uint32_t pbase, uint32_t nch, uint32_t lane)
     {
         uint32_t neg = 0;
         float s = __uint_as_float(__ldcg(hub_part + pbase));
@@ -645,12 +659,28 @@ struct AgPass
                 if (!(w & AG_XNOT) && (ex >= 24u) & (ex <= 254u) && m < (1u << 24)) {
                     s = exact_make(ex, m);
                 } else {
-                    /* this round's values, one by one */
+                    /* this round's values, one by one: staged by the chunk,
+                     * or gathered again (contribution of each in-edge's
+                     * source; the hot table holds copies of the same values) */
                     __syncwarp();
+                    if (hub_staged(pr)) {
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const uint32_t j = lo + lane + 32u * i;
-                        vals[lane + 32u * i] = j < hi ? __ldcg(row_vals + (j - o0)) : 0.0f;
+                        for (int i = 0; i < 8; ++i) {
+                            const uint32_t j = lo + lane + 32u * i;
+                            vals[lane + 32u * i] = j < hi ? __ldcg(row_vals + (j - o0)) : 0.0f;
+                        }
+                    } else {
+                        uint32_t u[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const uint32_t j = lo + lane + 32u * i;
+                            u[i] = j < hi ? __ldg(ids + j) : 0u;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const uint32_t j = lo + lane + 32u * i;
+                            vals[lane + 32u * i] = j < hi ? __ldcg(c_in + u[i]) : 0.0f;
+                        }
                     }
                     __syncwarp();
                     if (lane == 0)
@@ -1047,7 +1077,8 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 }
             } else {
                 const uint32_t pred = __ldcg(p.hub_pred + pbase + chunk);
-                ps.hub_steps(row_vals, o0, eb, ee, lane, pf, pred & 0xffu, p.hub_t + (size_t)(pbase + chunk) * AG_XWORDS);
+                ps.hub_steps(row_vals, o0, eb, ee, lane, pf, pred & 0xffu, ps.hub_staged(pred),
+                             p.hub_t + (size_t)(pbase + chunk) * AG_XWORDS);
             }
             __threadfence();
             __syncwarp();
@@ -1071,8 +1102,8 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                     }
                 }
                 const typename AgPass<MODE, PREC, EXACT>::XSum xs = AgPass<MODE, PREC, EXACT>::hub_compose(
-                    reinterpret_cast<const uint32_t *>(p.hub_part), p.hub_t, p.hub_pred, row_vals, vals, p.whub, o0,
-                    deg, pbase, nch, lane);
+                    reinterpret_cast<const uint32_t *>(p.hub_part), p.hub_t, p.hub_pred, row_vals, p.ids, ps.c_in32,
+                    vals, p.whub, o0, deg, pbase, nch, lane);
                 const float tot = xs.s;
                 const uint32_t neg = xs.neg;
                 if (lane == 0) {
