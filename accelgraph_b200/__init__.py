@@ -221,6 +221,7 @@ SIGNATURES = [
     ("ag_mlp_get_params", C.c_int32, [C.c_void_p, f32p]),
     ("ag_features", C.c_int32, [C.c_void_p, C.c_void_p]),
     ("ag_mlp_forward", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("ag_mlp_predict", C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("ag_mlp_gradients", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, f32p, f32p]),
     ("ag_mlp_train", C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                  f32p]),

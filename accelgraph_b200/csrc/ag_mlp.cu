@@ -225,6 +225,132 @@ __global__ void __launch_bounds__(AG_MLP_BLK) ag_mlp_infer_kernel(const __nv_bfl
     Y[s] = y;
 }
 
+/* ------------------------------------------------ tensor-core inference */
+/* The warm start's prediction on the tensor cores: one warp per tile of 16
+ * vertices, mma.sync m16n8k16 with bfloat16 operands and binary32
+ * accumulation.  A binary32 activation a is split into a bfloat16 head
+ * hi = bf16(a) and tail lo = bf16(a - hi), and hi * w + lo * w is formed
+ * exactly in the accumulator, so the products see about 16 significant bits
+ * of a instead of 8 (the weights are bfloat16 in both forward passes).
+ *  layer 1: K = 16 holds the 8 features' heads and their 8 tails, B = W1^T
+ *           twice; 8 MMAs give the 16 x 64 pre-activations, bias and ReLU in
+ *           binary32.
+ *  layer 2: the layer-1 accumulator fragments are exactly the A fragments of
+ *           the next product (columns 16 ks .. 16 ks + 15 are n-tiles 2 ks and
+ *           2 ks + 1); heads and tails, B = W2^T: 2 x 4 k-steps x 8 n-tiles =
+ *           64 MMAs.
+ *  output:  bias, ReLU and the 64-weight dot product on the accumulators, a
+ *           sum over the 4 lanes that share a row.
+ * The sums run in another order than ag_mlp_forward's, and the tails lose
+ * the last bits: the prediction agrees with the binary32 forward pass to
+ * about 1e-4 in log-rank.  Fragment layouts: PTX ISA, mma.m16n8k16 for
+ * .bf16. */
+__device__ __forceinline__ uint32_t ag_bf16x2(float lo, float hi)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+/* the bfloat16 tails of a pair: a - bf16(a) */
+__device__ __forceinline__ uint32_t ag_bf16x2_tail(float a, float b)
+{
+    return ag_bf16x2(a - __bfloat162float(__float2bfloat16_rn(a)), b - __bfloat162float(__float2bfloat16_rn(b)));
+}
+
+__device__ __forceinline__ void ag_mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                            uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+#define AG_MLP_TC_BLK 256
+__global__ void __launch_bounds__(AG_MLP_TC_BLK) ag_mlp_infer_tc_kernel(const __nv_bfloat16 *wb, const float *X,
+                                                                        uint32_t n, float *Y)
+{
+    /* W1 and W2 as bfloat16 pairs along the input index: pair p of output o
+     * holds inputs 2p, 2p+1 (the B fragment's element order) */
+    __shared__ uint32_t sw1[AG_MLP_H * AG_MLP_IN / 2];
+    __shared__ uint32_t sw2[AG_MLP_H * AG_MLP_H / 2];
+    __shared__ float sb1[AG_MLP_H], sb2[AG_MLP_H], sw3[AG_MLP_H];
+    __shared__ float sb3;
+    const uint32_t *wp = reinterpret_cast<const uint32_t *>(wb);
+    for (uint32_t i = threadIdx.x; i < AG_MLP_H * AG_MLP_IN / 2; i += blockDim.x)
+        sw1[i] = wp[AG_MLP_OFF_W1 / 2 + i];
+    for (uint32_t i = threadIdx.x; i < AG_MLP_H * AG_MLP_H / 2; i += blockDim.x)
+        sw2[i] = wp[AG_MLP_OFF_W2 / 2 + i];
+    for (uint32_t i = threadIdx.x; i < AG_MLP_H; i += blockDim.x) {
+        sb1[i] = __bfloat162float(wb[AG_MLP_OFF_B1 + i]);
+        sb2[i] = __bfloat162float(wb[AG_MLP_OFF_B2 + i]);
+        sw3[i] = __bfloat162float(wb[AG_MLP_OFF_W3 + i]);
+    }
+    if (threadIdx.x == 0)
+        sb3 = __bfloat162float(wb[AG_MLP_OFF_B3]);
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const uint32_t nwarps = gridDim.x * (AG_MLP_TC_BLK / 32);
+    for (uint32_t tile = blockIdx.x * (AG_MLP_TC_BLK / 32) + (threadIdx.x >> 5); (uint64_t)tile * 16 < n;
+         tile += nwarps) {
+        const uint32_t r0 = tile * 16 + gid, r1 = r0 + 8;
+        /* features of rows r0 and r1, columns 2 tig and 2 tig + 1 */
+        float2 x0 = make_float2(0.f, 0.f), x1 = x0;
+        if (r0 < n)
+            x0 = *reinterpret_cast<const float2 *>(X + (size_t)r0 * AG_MLP_IN + 2 * tig);
+        if (r1 < n)
+            x1 = *reinterpret_cast<const float2 *>(X + (size_t)r1 * AG_MLP_IN + 2 * tig);
+        const uint32_t xa0 = ag_bf16x2(x0.x, x0.y), xa1 = ag_bf16x2(x1.x, x1.y);
+        const uint32_t xt0 = ag_bf16x2_tail(x0.x, x0.y), xt1 = ag_bf16x2_tail(x1.x, x1.y);
+        /* layer 1: n-tile t gives units 8 t .. 8 t + 7; K 0-7 heads, 8-15 tails */
+        float h[8][4];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            h[t][0] = h[t][1] = h[t][2] = h[t][3] = 0.0f;
+            const uint32_t w1 = sw1[(8 * t + gid) * (AG_MLP_IN / 2) + tig];
+            ag_mma_bf16(h[t], xa0, xa1, xt0, xt1, w1, w1);
+            const uint32_t c = 8 * t + 2 * tig;
+            h[t][0] = fmaxf(h[t][0] + sb1[c], 0.0f);
+            h[t][1] = fmaxf(h[t][1] + sb1[c + 1], 0.0f);
+            h[t][2] = fmaxf(h[t][2] + sb1[c], 0.0f);
+            h[t][3] = fmaxf(h[t][3] + sb1[c + 1], 0.0f);
+        }
+        /* layer 2 and the output layer, one n-tile of 8 units at a time */
+        float y0 = 0.0f, y1 = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            const uint32_t *w2 = sw2 + (8 * t + gid) * (AG_MLP_H / 2);
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                const uint32_t b0 = w2[8 * ks + tig], b1 = w2[8 * ks + 4 + tig];
+                ag_mma_bf16(acc, ag_bf16x2(h[2 * ks][0], h[2 * ks][1]), ag_bf16x2(h[2 * ks][2], h[2 * ks][3]),
+                            ag_bf16x2(h[2 * ks + 1][0], h[2 * ks + 1][1]),
+                            ag_bf16x2(h[2 * ks + 1][2], h[2 * ks + 1][3]), b0, b1);
+                ag_mma_bf16(acc, ag_bf16x2_tail(h[2 * ks][0], h[2 * ks][1]),
+                            ag_bf16x2_tail(h[2 * ks][2], h[2 * ks][3]),
+                            ag_bf16x2_tail(h[2 * ks + 1][0], h[2 * ks + 1][1]),
+                            ag_bf16x2_tail(h[2 * ks + 1][2], h[2 * ks + 1][3]), b0, b1);
+            }
+            const uint32_t c = 8 * t + 2 * tig;
+            y0 = fmaf(sw3[c], fmaxf(acc[0] + sb2[c], 0.0f), y0);
+            y0 = fmaf(sw3[c + 1], fmaxf(acc[1] + sb2[c + 1], 0.0f), y0);
+            y1 = fmaf(sw3[c], fmaxf(acc[2] + sb2[c], 0.0f), y1);
+            y1 = fmaf(sw3[c + 1], fmaxf(acc[3] + sb2[c + 1], 0.0f), y1);
+        }
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if (tig == 0) {
+            if (r0 < n)
+                Y[r0] = y0 + sb3;
+            if (r1 < n)
+                Y[r1] = y1 + sb3;
+        }
+    }
+}
+
 /* per-sample training signals; buf layout per sample (stride 2 + 4*64 + 8):
  * [x(8) h1(64) h2(64) dh1(64) dh2(64) d3 pad] */
 #define AG_MLP_REC (AG_MLP_IN + 4 * AG_MLP_H + 2)
@@ -488,6 +614,21 @@ extern "C" ag_status_t ag_mlp_forward(ag_mlp_t m, const float *X, uint32_t n, fl
     return AG_OK;
 }
 
+extern "C" ag_status_t ag_mlp_predict(ag_mlp_t m, const float *X, uint32_t n, float *Y)
+{
+    ag_clear_error();
+    if (!m || (n && (!X || !Y)))
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_mlp_predict: NULL argument");
+    if (n == 0)
+        return AG_OK;
+    uint64_t blocks = ((uint64_t)n + 16 * (AG_MLP_TC_BLK / 32) - 1) / (16 * (AG_MLP_TC_BLK / 32));
+    if (blocks > ag_sm_grid(8))
+        blocks = ag_sm_grid(8);
+    ag_mlp_infer_tc_kernel<<<(unsigned)blocks, AG_MLP_TC_BLK, 0, mlp_stream()>>>(m->wb, X, n, Y);
+    MCHK(cudaGetLastError());
+    return AG_OK;
+}
+
 static ag_status_t mlp_ensure_buf(ag_mlp_t m, uint32_t n)
 {
     if (m->buf_cap >= n)
@@ -595,7 +736,7 @@ extern "C" ag_status_t ag_mlp_warm_start_device(ag_graph_t g, ag_mlp_t m, float 
     MCHK(cudaMallocAsync((void **)&X, (size_t)gv.N * AG_MLP_IN * sizeof(float), s));
     st = ag_features(g, X);
     if (st == AG_OK)
-        st = ag_mlp_forward(m, X, gv.N, init_dev);
+        st = ag_mlp_predict(m, X, gv.N, init_dev);
     if (st == AG_OK) {
         ag_mlp_to_ranks_kernel<<<ag_sm_grid(8), 256, 0, s>>>(init_dev, gv.N, 1.0f - Damp, init_dev);
         cudaError_t e = cudaGetLastError();
@@ -624,7 +765,7 @@ extern "C" ag_status_t ag_mlp_warm_start(ag_graph_t g, ag_mlp_t m, float *init_r
     MCHK(cudaMallocAsync((void **)&Y, (size_t)gv.N * sizeof(float), s));
     st = ag_features(g, X);
     if (st == AG_OK)
-        st = ag_mlp_forward(m, X, gv.N, Y);
+        st = ag_mlp_predict(m, X, gv.N, Y);
     if (st == AG_OK) {
         ag_mlp_to_ranks_kernel<<<ag_sm_grid(8), 256, 0, s>>>(Y, gv.N, 1.0f - Damp, Y);
         cudaError_t e = cudaMemcpyAsync(init_ranks, Y, (size_t)gv.N * sizeof(float), cudaMemcpyDeviceToHost, s);

@@ -80,6 +80,18 @@ class MLP:
         _sync()
         return Y
 
+    def predict(self, X):
+        """The warm start's prediction on the tensor cores (ag_mlp_predict):
+        bfloat16 head and tail of every feature and activation, binary32
+        accumulation."""
+        torch = _torch()
+        n = X.shape[0]
+        Y = torch.empty(n, dtype=torch.float32, device=X.device)
+        _sync()
+        check(lib.ag_mlp_predict(self.h, X.data_ptr(), n, Y.data_ptr()), "ag_mlp_predict")
+        _sync()
+        return Y
+
     def gradients(self, X, T):
         g = np.empty(self.num_params, np.float32)
         loss = C.c_float()

@@ -532,9 +532,14 @@ def run_multigraph(a):
 
 def run_warmstart(a):
     """Train the warm-start MLP on this GPU's PageRank results of seeded
-    graphs (scales 14-18), evaluate on a held-out RMAT graph."""
+    graphs (scales 14-18), evaluate on a held-out RMAT graph: passes and time
+    to epsilon from the prediction against the uniform start, the prediction's
+    cost split into features and MLP (SIMT and tensor-core), the pass saving
+    its accuracy allows at most, and the warm start combined with the
+    data-driven pull and with BF16 contributions."""
     import time
     import numpy as np
+    import torch
     ag = _gpu_setup()
     from accelgraph_b200 import warmstart as ws
     t0 = time.perf_counter()
@@ -554,6 +559,51 @@ def run_warmstart(a):
     eu = _rel(c["ranks_uniform"], r64)
     ew = _rel(c["ranks_warm"], r64)
     ei = _rel(c["init"] / g.num_vertices, r64)
+    e0 = _rel(np.full(g.num_vertices, (1.0 - 0.85) / g.num_vertices, np.float32), r64)
+
+    # the prediction's parts, timed on the library stream
+    stream = torch.cuda.ExternalStream(ag.lib.ag_stream(), device=torch.device("cuda", 0))
+
+    def timed(fn, reps=5):
+        fn()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    n = g.num_vertices
+    Xf = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    Yf = torch.empty(n, dtype=torch.float32, device="cuda")
+    t_feat = timed(lambda: ag.check(ag.lib.ag_features(dg.h, Xf.data_ptr()), "ag_features"))
+    t_simt = timed(lambda: ag.check(ag.lib.ag_mlp_forward(m.h, Xf.data_ptr(), n, Yf.data_ptr()), "forward"))
+    t_tc = timed(lambda: ag.check(ag.lib.ag_mlp_predict(m.h, Xf.data_ptr(), n, Yf.data_ptr()), "predict"))
+    mlp_flops = 2.0 * (8 * 64 + 64 * 64 + 64) * n
+
+    # what a warm start can give: each pass costs the same whatever the start,
+    # so halving the time to eps means skipping half the passes, and the pull
+    # contracts the error by about the damping factor per pass: the start
+    # must already be about 0.85^(passes / 2) times closer to the fixpoint
+    # than the uniform start is
+    t_u = c["uniform"]["device_ms"]
+    half = c["uniform"]["passes"] / 2.0
+    need = e0[0] * 0.85 ** half
+    free = t_u / c["warm"]["device_ms"]
+
+    # combined forms from the same prediction
+    init = torch.from_numpy(c["init"]).cuda()
+    comb = {}
+    for name, kw in (("warm_dd", {"data_driven": True}), ("warm_bf16", {"precision": ag.AG_PREC_BF16}),
+                     ("dd", {"data_driven": True, "init": False}), ("bf16", {"precision": ag.AG_PREC_BF16,
+                                                                            "init": False})):
+        use_init = kw.pop("init", True)
+        r, res, _ = dg.pagerank(a.iterations, a.epsilon, init_ranks=init if use_init else None, **kw)
+        r, res, _ = dg.pagerank(a.iterations, a.epsilon, init_ranks=init if use_init else None, **kw)
+        ms = res.device_ms + (c["warm"]["predict_ms"] if use_init else 0.0)
+        comb[name] = {"passes": res.passes, "ms_to_eps": ms, "speedup_vs_uniform_fp32": t_u / ms,
+                      "rel_l1_vs_fp64": _rel(r, r64)[0]}
     print(json.dumps({"workload": f"learned warm start, eval RMAT s{a.scale} ef{a.edge_factor} (seed 9999), "
                                   f"trained on {a.train_graphs} graphs s14-18", "N": g.num_vertices,
                       "E": g.num_edges, "train_samples": int(X.shape[0]), "loss_initial": loss0,
@@ -561,6 +611,16 @@ def run_warmstart(a):
                       "uniform": c["uniform"], "warm": c["warm"],
                       "speedup_time_to_eps": c["uniform"]["device_ms"] / (c["warm"]["device_ms"] +
                                                                           c["warm"]["predict_ms"]),
+                      "predict_breakdown_ms": {"features": t_feat, "mlp_simt_fp32": t_simt,
+                                               "mlp_tensor_core": t_tc,
+                                               "mlp_tensor_core_tflops": mlp_flops / (t_tc * 1e-3) / 1e12,
+                                               "mlp_simt_tflops": mlp_flops / (t_simt * 1e-3) / 1e12},
+                      "bound": {"rel_l1_uniform_start": e0[0], "rel_l1_prediction": ei[0],
+                                "passes_saved_measured": c["uniform"]["passes"] - c["warm"]["passes"],
+                                "passes_to_skip_for_2x": half,
+                                "start_rel_l1_needed_for_2x": need,
+                                "speedup_with_a_free_prediction": free},
+                      "combined": comb,
                       "rel_l1_vs_fp64": {"uniform": eu[0], "warm": ew[0], "prediction_alone": ei[0]}}),
           flush=True)
 

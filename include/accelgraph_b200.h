@@ -410,8 +410,14 @@ ag_status_t ag_mlp_get_params(ag_mlp_t m, float *params);          /* host array
  * their out-degrees, min and max of their out-degrees, sum of their
  * 1/out-degree, max of their in-degrees. */
 ag_status_t ag_features(ag_graph_t g, float *features);
-/* Y[i] = MLP(X[i]) for n samples; X (n x 8) and Y (n) are device arrays. */
+/* Y[i] = MLP(X[i]) for n samples; X (n x 8) and Y (n) are device arrays.
+ * The training forward pass: binary32 activations with the bfloat16 weights. */
 ag_status_t ag_mlp_forward(ag_mlp_t m, const float *X, uint32_t n, float *Y);
+/* The same prediction on the tensor cores (mma.sync bfloat16 operands,
+ * binary32 accumulation; each feature and activation split into a bfloat16
+ * head and tail): what the warm start uses.  Within about 1e-4 of
+ * ag_mlp_forward in log-rank. */
+ag_status_t ag_mlp_predict(ag_mlp_t m, const float *X, uint32_t n, float *Y);
 /* Gradient of the mean squared error of MLP(X) against T (device arrays)
  * with respect to the parameters (host array of ag_mlp_num_params()
  * values, may be NULL) and the loss (may be NULL). */

@@ -64,6 +64,25 @@ def test_mlp_forward_and_gradients_match_oracle(gpu):
         assert np.linalg.norm(g[a:b] - g_ref[a:b]) <= 1e-3 * np.linalg.norm(g_ref[a:b]) + 1e-7
 
 
+def test_tensor_core_prediction_matches_forward(gpu):
+    """The warm start's prediction (mma.sync with bfloat16 head and tail of
+    every feature and activation, binary32 accumulation) agrees with the
+    binary32-activation forward pass that training and the oracle use to 1e-3
+    relative, for sample counts that are not multiples of the 16-row tile."""
+    ag = gpu
+    import torch
+
+    from accelgraph_b200 import warmstart as ws
+    m = ws.MLP(seed=7)
+    rng = np.random.default_rng(2)
+    for n in (1, 15, 16, 17, 1000, 40_003):
+        X = torch.from_numpy((rng.random((n, 8)) * 6.0).astype(np.float32)).cuda()
+        y = m.forward(X).cpu().numpy()
+        yp = m.predict(X).cpu().numpy()
+        assert np.all(np.isfinite(yp))
+        assert np.max(np.abs(yp - y) / np.maximum(1.0, np.abs(y))) <= 1e-3, n
+
+
 def test_training_reduces_loss_and_warm_start_gains(gpu, oracle):
     """Train on GPU PageRank results of small seeded graphs; on a held-out
     graph the warm start needs fewer passes than uniform starting ranks and
