@@ -99,7 +99,7 @@ class PROpts(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("precision", C.c_int32), ("order", C.c_int32), ("quiet", C.c_int32),
         ("switch_residual", C.c_double), ("init_ranks", f32p), ("init_on_device", C.c_int32),
-        ("data_driven", C.c_int32), ("direction", C.c_int32),
+        ("data_driven", C.c_int32), ("direction", C.c_int32), ("keep_graph", C.c_int32),
     ]
 
 
@@ -195,6 +195,7 @@ SIGNATURES = [
     ("ag_fill_uniform", None, [f32p, C.c_uint64, C.c_uint64]),
     ("ag_graph_upload", C.c_int32, [GraphP, C.c_uint32, C.POINTER(C.c_void_p)]),
     ("ag_graph_release", C.c_int32, [C.c_void_p]),
+    ("ag_graph_forget", C.c_int32, [GraphP]),
     ("ag_graph_get_info", C.c_int32, [C.c_void_p, C.POINTER(GraphInfo)]),
     ("ag_graph_get_tiles", C.c_int32, [C.c_void_p, C.POINTER(TileConfig)]),
     ("ag_gather_u64", C.c_int32, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

@@ -32,6 +32,116 @@ static void fail_exit(const char *phase, ag_status_t st)
     exit(EXIT_FAILURE);
 }
 
+static int env_keep(void)
+{
+    const char *k = getenv("AG_KEEP_GRAPH");
+    return k && k[0] && k[0] != '0';
+}
+
+/* ------------------------------------------------ uploads kept between calls */
+/* A caller that solves on one unchanged GraphCSR several times pays the
+ * upload once when it asks for it.  An entry matches on the GraphCSR
+ * address, its vertex and edge counts, the addresses of every array the
+ * upload reads and the upload flags.  The library is called from one host
+ * thread at a time, so the table has no lock. */
+#define AG_KEEP_SLOTS 8
+
+typedef struct keep_slot
+{
+    const struct GraphCSR *graph;
+    uint32_t num_vertices, num_edges, flags;
+    const void *arrays[5];
+    ag_graph_t g;
+    uint64_t used;
+} keep_slot;
+
+static keep_slot g_keep[AG_KEEP_SLOTS];
+static uint64_t g_keep_tick;
+
+static void keep_key(const struct GraphCSR *graph, const void *a[5])
+{
+    const struct Vertex *iv = graph->inverse_vertices, *fv = graph->vertices;
+    const struct EdgeList *iel = graph->inverse_sorted_edges_array;
+    a[0] = iv ? (const void *)iv->edges_idx : NULL;
+    a[1] = iv ? (const void *)iv->out_degree : NULL;
+    a[2] = fv ? (const void *)fv->out_degree : NULL;
+    a[3] = iel ? (const void *)iel->edges_array_dest : NULL;
+    a[4] = iel ? (const void *)iel->edges_array_weight : NULL;
+}
+
+/* the device graph of `graph` uploaded with `flags`: with `keep`, a kept
+ * one that matches or a new upload that is then kept (*kept = 1: the caller
+ * does not release it); without, a new upload the caller releases */
+static ag_status_t upload_graph(const struct GraphCSR *graph, uint32_t flags, int keep, ag_graph_t *out, int *kept)
+{
+    const void *a[5];
+    int i, victim = -1;
+    ag_status_t st;
+    keep_slot *s;
+
+    *kept = 0;
+    if (!keep)
+        return ag_graph_upload(graph, flags, out);
+    keep_key(graph, a);
+    for (i = 0; i < AG_KEEP_SLOTS; i++) {
+        s = &g_keep[i];
+        if (s->g && s->graph == graph && s->num_vertices == graph->num_vertices &&
+            s->num_edges == graph->num_edges && s->flags == flags && !memcmp(s->arrays, a, sizeof(a))) {
+            s->used = ++g_keep_tick;
+            *out = s->g;
+            *kept = 1;
+            return AG_OK;
+        }
+    }
+    /* an empty slot, else the least recently used */
+    for (i = 0; i < AG_KEEP_SLOTS; i++)
+        if (!g_keep[i].g || victim < 0 || (g_keep[victim].g && g_keep[i].used < g_keep[victim].used))
+            victim = i;
+    st = ag_graph_upload(graph, flags, out);
+    if (st != AG_OK)
+        return st;
+    s = &g_keep[victim];
+    if (s->g)
+        ag_graph_release(s->g);
+    s->graph = graph;
+    s->num_vertices = graph->num_vertices;
+    s->num_edges = graph->num_edges;
+    s->flags = flags;
+    memcpy(s->arrays, a, sizeof(a));
+    s->g = *out;
+    s->used = ++g_keep_tick;
+    *kept = 1;
+    return AG_OK;
+}
+
+/* release a device graph after a call: a kept one stays unless the call
+ * failed, when it is forgotten (its state after a failure is not reused) */
+static void finish_graph(ag_graph_t g, int kept, int failed)
+{
+    int i;
+    if (!g)
+        return;
+    if (kept && !failed)
+        return;
+    for (i = 0; i < AG_KEEP_SLOTS; i++)
+        if (g_keep[i].g == g)
+            memset(&g_keep[i], 0, sizeof(g_keep[i]));
+    ag_graph_release(g);
+}
+
+ag_status_t ag_graph_forget(const struct GraphCSR *graph)
+{
+    int i;
+    ag_clear_error();
+    for (i = 0; i < AG_KEEP_SLOTS; i++) {
+        if (g_keep[i].g && (!graph || g_keep[i].graph == graph)) {
+            ag_graph_release(g_keep[i].g);
+            memset(&g_keep[i], 0, sizeof(g_keep[i]));
+        }
+    }
+    return AG_OK;
+}
+
 /* ------------------------------------------------------------ PageRank */
 struct PageRankStats *newPageRankStatsGraphCSR(struct GraphCSR *graph)
 {
@@ -78,6 +188,7 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
     ag_pr_opts o;
     ag_pr_result res;
     ag_graph_t g = NULL;
+    int kept = 0;
     ag_status_t st;
     struct PageRankStats *stats;
     uint32_t *h_active = NULL;
@@ -136,7 +247,7 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
             printf("| %-10s | %-8u | %-15.13lf | %-9f | \n", "Init", graph->num_vertices, 0.0, 0.0);
     }
 
-    st = ag_graph_upload(graph, 0, &g);
+    st = upload_graph(graph, 0, o.keep_graph || env_keep(), &g, &kept);
     if (st != AG_OK)
         goto fail;
     st = ag_pagerank_launch(g, arguments->iterations, arguments->epsilon, &o);
@@ -153,7 +264,7 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
     st = ag_pagerank_fetch(g, stats->pageRanks, &res, h_active, h_err, h_sec, cap);
     if (st != AG_OK)
         goto fail;
-    ag_graph_release(g);
+    finish_graph(g, kept, 0);
     g = NULL;
 
     stats->iterations = res.iterations;
@@ -179,8 +290,7 @@ ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct 
     return AG_OK;
 
 fail:
-    if (g)
-        ag_graph_release(g);
+    finish_graph(g, kept, 1);
     free(h_active);
     free(h_err);
     free(h_sec);
@@ -348,6 +458,7 @@ ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct Grap
                             struct SPMVStats **out)
 {
     ag_graph_t g = NULL;
+    int kept = 0;
     ag_status_t st;
     struct SPMVStats *stats;
     double *sec = NULL;
@@ -365,7 +476,7 @@ ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct Grap
         return ag_set_error(AG_ERR_OOM, "stats allocation failed");
     iters = arguments->iterations;
 
-    st = ag_graph_upload(graph, AG_UPLOAD_WEIGHTS, &g);
+    st = upload_graph(graph, AG_UPLOAD_WEIGHTS, env_keep(), &g, &kept);
     if (st != AG_OK)
         goto fail;
     if (!quiet) {
@@ -406,14 +517,13 @@ ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct Grap
         printf(" -----------------------------------------------------\n");
         fflush(stdout);
     }
-    ag_graph_release(g);
+    finish_graph(g, kept, 0);
     free(sec);
     *out = stats;
     return AG_OK;
 
 fail:
-    if (g)
-        ag_graph_release(g);
+    finish_graph(g, kept, 1);
     free(sec);
     freeSPMVStats(stats);
     return st;

@@ -15,14 +15,28 @@
  *
  * Layout: contributions and ranks are N x 64 binary32, row-major (256 bytes
  * per vertex).  One warp owns a destination row; lane l owns columns 2l and
- * 2l + 1.  Each in-edge becomes one fully coalesced 256-byte row gather, eight
- * rows in flight per lane, so the pass streams the gathered rows from HBM at
- * full width (the per-edge 4-byte random gather of the single-vector kernel
- * becomes a 256-byte sequential one).  Every column is summed in stream
- * order, so each column is bit-identical to a sequential binary32 loop.
+ * 2l + 1.  Each in-edge becomes one fully coalesced 256-byte row gather, so
+ * the pass streams the gathered rows from HBM at full width (the per-edge
+ * 4-byte random gather of the single-vector kernel becomes a 256-byte
+ * sequential one).  Every column is summed in stream order, so each column
+ * is bit-identical to a sequential binary32 loop.
+ *
+ * The contribution matrix of a graph of millions of vertices is far larger
+ * than L2, so the gathered rows come from HBM: 256 bytes per in-edge is the
+ * pass's real traffic.  The kernel therefore keeps as many row gathers in
+ * flight as it can: eight per warp, a grid of exactly the resident warps,
+ * and the next row's bounds and first 32 ids loading while the current row
+ * is gathered, so no warp waits on the offsets -> ids -> rows chain between
+ * rows.
+ *
+ * The loop stays on the device: after each pass a one-thread kernel counts
+ * it and sets a stop flag once no (v, i) pair moved by epsilon; passes that
+ * see the flag return at once, and the host reads the flag every
+ * AG_PPR_CHECK passes.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -33,6 +47,22 @@
 
 #define AG_PPR_K 64
 #define AG_PPR_BLK 256
+#define AG_PPR_DEPTH 8 /* row gathers in flight per warp: 62 registers, 32
+                          resident warps per SM.  AG_PPR_DEPTH=16 in the
+                          environment takes sixteen (80 registers, 24 warps):
+                          8.56 against 7.46 ms per pass on ER 2^23, k = 64 */
+#define AG_PPR_CHECK 8  /* passes between host reads of the stop flag */
+
+/* the device-side loop state, written by ag_ppr_close_kernel */
+struct AgPprState
+{
+    uint32_t stop;       /* set once a pass had no active pair */
+    uint32_t passes;     /* passes that did work               */
+    uint32_t converged;
+    uint32_t pad;
+    unsigned long long active_last;
+    double err_last;
+};
 
 struct AgPprParams
 {
@@ -50,6 +80,7 @@ struct AgPprParams
     double eps;
     unsigned long long *active; /* pairs with |r' - r| >= eps */
     double *err;      /* sum of |r' - r|                      */
+    AgPprState *state;
 };
 
 __device__ __forceinline__ float2 ag_ppr_ld_row(const float *X, uint32_t u, uint32_t lane)
@@ -80,10 +111,13 @@ __global__ void __launch_bounds__(AG_PPR_BLK) ag_ppr_init_kernel(AgPprParams p)
     }
 }
 
+template <int DEPTH>
 __global__ void __launch_bounds__(AG_PPR_BLK) ag_ppr_pass_kernel(AgPprParams p)
 {
     __shared__ unsigned long long s_act[AG_PPR_BLK / 32];
     __shared__ double s_err[AG_PPR_BLK / 32];
+    if (*(volatile const uint32_t *)&p.state->stop)
+        return;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t c0 = 2 * lane, c1 = c0 + 1;
@@ -92,29 +126,49 @@ __global__ void __launch_bounds__(AG_PPR_BLK) ag_ppr_pass_kernel(AgPprParams p)
     const uint32_t s1 = live1 ? p.src_rows[c1] : 0xFFFFFFFFu;
     unsigned long long my_act = 0;
     double my_err = 0.0;
-    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < p.N; v += nw) {
-        const uint32_t b = p.row_off[v], e = p.row_off[v + 1];
+    /* row v's bounds and first ids, and row vn's bounds, are loaded one row
+     * ahead of their use */
+    uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t b = 0, e = 0, myid = 0;
+    if (v < p.N) {
+        b = p.row_off[v];
+        e = p.row_off[v + 1];
+        myid = lane < min(32u, e - b) ? p.ids[b + lane] : 0u;
+    }
+    uint32_t vn = v + nw, bn = 0, en = 0;
+    if (vn < p.N) {
+        bn = p.row_off[vn];
+        en = p.row_off[vn + 1];
+    }
+    while (v < p.N) {
         const uint32_t od = p.outdeg[v];
         const float2 rp = reinterpret_cast<const float2 *>(p.R + (size_t)v * AG_PPR_K)[lane];
-        float ax = 0.0f, ay = 0.0f;
-        bool first = true;
+        const uint32_t myid_n = (vn < p.N && lane < min(32u, en - bn)) ? p.ids[bn + lane] : 0u;
+        const uint32_t vnn = vn + nw;
+        uint32_t bnn = 0, enn = 0;
+        if (vnn < p.N) {
+            bnn = p.row_off[vnn];
+            enn = p.row_off[vnn + 1];
+        }
+        /* stream order; -0 + x = x for every binary32 x, so the sum starts
+         * at -0 instead of at the first value, and a row without in-edges
+         * still gives +0 once the teleport term (+0 or positive) is added */
+        float ax = -0.0f, ay = -0.0f;
         for (uint32_t j0 = b; j0 < e; j0 += 32) {
             const uint32_t n = min(32u, e - j0);
-            const uint32_t myid = lane < n ? p.ids[j0 + lane] : 0u;
-            for (uint32_t t = 0; t < n; t += 8) {
-                float2 val[8];
+            const uint32_t chunk = (j0 == b) ? myid : (lane < n ? p.ids[j0 + lane] : 0u);
+            for (uint32_t t = 0; t < n; t += DEPTH) {
+                float2 val[DEPTH];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const uint32_t u = __shfl_sync(0xffffffffu, myid, (t + q) & 31);
+                for (int q = 0; q < DEPTH; ++q) {
+                    const uint32_t u = __shfl_sync(0xffffffffu, chunk, (t + q) & 31);
                     val[q] = (t + q < n) ? ag_ppr_ld_row(p.X, u, lane) : make_float2(0.f, 0.f);
                 }
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
+                for (int q = 0; q < DEPTH; ++q) {
                     if (t + q < n) {
-                        /* stream order; the first value restarts the sum */
-                        ax = first ? val[q].x : __fadd_rn(ax, val[q].x);
-                        ay = first ? val[q].y : __fadd_rn(ay, val[q].y);
-                        first = false;
+                        ax = __fadd_rn(ax, val[q].x);
+                        ay = __fadd_rn(ay, val[q].y);
                     }
                 }
             }
@@ -134,6 +188,13 @@ __global__ void __launch_bounds__(AG_PPR_BLK) ag_ppr_pass_kernel(AgPprParams p)
         cn.y = od ? __fdiv_rn(rn.y, __uint2float_rn(od)) : 0.0f;
         reinterpret_cast<float2 *>(p.R + (size_t)v * AG_PPR_K)[lane] = rn;
         reinterpret_cast<float2 *>(p.Xn + (size_t)v * AG_PPR_K)[lane] = cn;
+        v = vn;
+        b = bn;
+        e = en;
+        myid = myid_n;
+        vn = vnn;
+        bn = bnn;
+        en = enn;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -157,6 +218,24 @@ __global__ void __launch_bounds__(AG_PPR_BLK) ag_ppr_pass_kernel(AgPprParams p)
         if (er != 0.0)
             atomicAdd(p.err, er);
     }
+}
+
+/* after each pass: count it, keep its statistics, stop when nothing moved;
+ * clears the counters for the next pass */
+__global__ void ag_ppr_close_kernel(AgPprParams p)
+{
+    AgPprState *st = p.state;
+    if (!st->stop) {
+        st->passes += 1;
+        st->active_last = *p.active;
+        st->err_last = *p.err;
+        if (*p.active == 0) {
+            st->stop = 1;
+            st->converged = 1;
+        }
+    }
+    *p.active = 0;
+    *p.err = 0.0;
 }
 
 /* out[perm[v] * k + i] = R[v][i] / N (binary32), caller order */
@@ -192,6 +271,10 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     float *X = nullptr, *Xn = nullptr, *R = nullptr, *out = nullptr;
     uint32_t *src_dev = nullptr;
     unsigned long long *ctr = nullptr;
+    AgPprState *state = nullptr;
+    AgPprState hs;
+    int per_sm = 0;
+    void (*pass_kernel)(AgPprParams) = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::vector<uint32_t> src_rows(k);
     cudaError_t err = cudaSuccess;
@@ -201,8 +284,12 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     float ms = 0.0f;
     AgPprParams p;
     memset(&p, 0, sizeof(p));
+    /* init and output: a few waves; passes: exactly the resident CTAs, so
+     * that every warp's share of rows runs at once */
     const unsigned grid_rows = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>(((uint64_t)gv.N * 32 + AG_PPR_BLK - 1) / AG_PPR_BLK, (uint64_t)ag_sm_grid(8)));
+    unsigned grid_pass = grid_rows;
+    memset(&hs, 0, sizeof(hs));
 #define PCHK(call)                                                                                       \
     do {                                                                                                 \
         err = (call);                                                                                    \
@@ -224,6 +311,17 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     PCHK(cudaMallocAsync((void **)&R, mat, s));
     PCHK(cudaMallocAsync((void **)&src_dev, AG_PPR_K * 4, s));
     PCHK(cudaMallocAsync((void **)&ctr, 16, s));
+    PCHK(cudaMallocAsync((void **)&state, sizeof(AgPprState), s));
+    PCHK(cudaMemsetAsync(ctr, 0, 16, s));
+    PCHK(cudaMemsetAsync(state, 0, sizeof(AgPprState), s));
+    {
+        const char *d = getenv("AG_PPR_DEPTH");
+        pass_kernel = (d && atoi(d) == 16) ? ag_ppr_pass_kernel<16> : ag_ppr_pass_kernel<AG_PPR_DEPTH>;
+    }
+    PCHK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, AG_PPR_BLK, 0));
+    grid_pass = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)gv.N * 32 + AG_PPR_BLK - 1) / AG_PPR_BLK,
+                              (uint64_t)ag_sm_grid((unsigned)std::max(per_sm, 1))));
     PCHK(cudaMemcpyAsync(src_dev, src_rows.data(), (size_t)k * 4, cudaMemcpyHostToDevice, s));
     PCHK(cudaEventCreate(&e0));
     PCHK(cudaEventCreate(&e1));
@@ -238,6 +336,7 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     p.eps = epsilon;
     p.active = ctr;
     p.err = reinterpret_cast<double *>(ctr + 1);
+    p.state = state;
     PCHK(cudaEventRecord(e0, s));
     p.X = X;
     p.Xn = X; /* init writes the first contributions into X */
@@ -245,23 +344,23 @@ extern "C" ag_status_t ag_ppr_spmm(ag_graph_t g, const uint32_t *sources, uint32
     ag_ppr_init_kernel<<<grid_rows, AG_PPR_BLK, 0, s>>>(p);
     PCHK(cudaGetLastError());
     for (uint32_t it = 0; it < max_iterations; ++it) {
-        unsigned long long h[2] = {0, 0};
         p.X = (it & 1) ? Xn : X;
         p.Xn = (it & 1) ? X : Xn;
-        PCHK(cudaMemsetAsync(ctr, 0, 16, s));
-        ag_ppr_pass_kernel<<<grid_rows, AG_PPR_BLK, 0, s>>>(p);
+        pass_kernel<<<grid_pass, AG_PPR_BLK, 0, s>>>(p);
+        ag_ppr_close_kernel<<<1, 1, 0, s>>>(p);
         PCHK(cudaGetLastError());
-        PCHK(cudaMemcpyAsync(h, ctr, 16, cudaMemcpyDeviceToHost, s));
-        PCHK(cudaStreamSynchronize(s));
-        ++passes;
-        act_last = h[0];
-        memcpy(&err_last, &h[1], sizeof(double));
-        if (act_last == 0) {
-            converged = 1;
-            break;
+        if ((it + 1) % AG_PPR_CHECK == 0 || it + 1 == max_iterations) {
+            PCHK(cudaMemcpyAsync(&hs, state, sizeof(hs), cudaMemcpyDeviceToHost, s));
+            PCHK(cudaStreamSynchronize(s));
+            if (hs.stop)
+                break;
         }
     }
     PCHK(cudaEventRecord(e1, s));
+    passes = hs.passes;
+    converged = hs.converged;
+    act_last = hs.active_last;
+    err_last = hs.err_last;
     if (ranks) {
         PCHK(cudaMallocAsync((void **)&out, (size_t)gv.N * k * sizeof(float), s));
         ag_ppr_output_kernel<<<ag_sm_grid(8), 256, 0, s>>>(p, gv.perm, out);
@@ -292,6 +391,8 @@ done:
         cudaFreeAsync(src_dev, s);
     if (ctr)
         cudaFreeAsync(ctr, s);
+    if (state)
+        cudaFreeAsync(state, s);
     if (e0)
         cudaEventDestroy(e0);
     if (e1)

@@ -487,6 +487,9 @@ def run_ppr(a):
     _, res1, _ = dg.pagerank(a.iterations, a.epsilon)
     peak, kind = peak_hbm()
     alg = 4 * E + 8 * N + 16 * a.k * N
+    # the contribution matrix (N x 256 bytes) is far larger than L2, so every
+    # in-edge's 256-byte row gather comes from HBM
+    moved = 4 * E + 8 * N + 256 * E + 12 * 64 * N
     print(json.dumps({"workload": f"personalized PageRank, k={a.k} sources, ER n=2^{a.scale} avg degree 16",
                       "N": N, "E": E, "ppr_passes": res.passes, "ppr_device_ms": res.device_ms,
                       "ppr_ms_per_pass": res.device_ms / max(res.passes, 1),
@@ -495,7 +498,10 @@ def run_ppr(a):
                       "plain_single_ms": res1.device_ms, "plain_single_passes": res1.passes,
                       "speedup_per_source_vs_plain": res1.device_ms / (res.device_ms / a.k),
                       "roofline_model_frac": alg / (res.device_ms * 1e-3 / res.passes) / 1e9 / peak,
-                      "gathered_row_bytes_per_pass": 256 * E}), flush=True)
+                      "gathered_row_bytes_per_pass": 256 * E,
+                      "hbm_bytes_per_pass_with_row_gathers": moved,
+                      "hbm_frac_with_row_gathers": moved / (res.device_ms * 1e-3 / res.passes) / 1e9 / peak,
+                      "peak_gbs": peak, "peak_kind": kind}), flush=True)
 
 
 def run_multigraph(a):

@@ -183,6 +183,16 @@ typedef struct ag_tile_config
  * the host graph may be freed after the call returns. */
 ag_status_t ag_graph_upload(const struct GraphCSR *graph, uint32_t flags, ag_graph_t *out);
 ag_status_t ag_graph_release(ag_graph_t g);
+/* Device copies kept between calls.  With ag_pr_opts.keep_graph (or the
+ * environment variable AG_KEEP_GRAPH=1, which also covers the reference entry
+ * points of pageRank.h and SPMV.h), the CSR entry points keep the upload of
+ * a GraphCSR (copy, relabelling, work-list plan) in a table of 8 entries,
+ * least recently used first out, and a later call reuses it when the
+ * GraphCSR address, its vertex and edge counts, the addresses of the arrays
+ * the upload reads and the upload flags all match.  A caller that changes
+ * the arrays in place, or frees the GraphCSR, calls ag_graph_forget(graph)
+ * first; NULL forgets every kept graph.  A failed solve forgets its graph. */
+ag_status_t ag_graph_forget(const struct GraphCSR *graph);
 ag_status_t ag_graph_get_info(ag_graph_t g, ag_graph_info *info);
 ag_status_t ag_graph_get_tiles(ag_graph_t g, ag_tile_config *cfg);
 /* Copy a work list of the pull kernel (exact = 0: FAST order, 1: EXACT
@@ -269,6 +279,11 @@ typedef struct ag_pr_opts
                                   FIXED64, QUANT32; with data_driven the
                                   data-driven push, pushpull 7), AG_DIR_PULL_PUSH
                                   the data-driven pull-push (pushpull 8)      */
+    int32_t keep_graph;        /* nonzero: ag_pagerank_pull_ex keeps the
+                                  device copy of `graph` after the call and a
+                                  later call on the same GraphCSR reuses it
+                                  (see ag_graph_forget); 0: upload per call,
+                                  as the reference maps the arrays per call  */
 } ag_pr_opts;
 
 typedef struct ag_pr_result
