@@ -530,8 +530,7 @@ struct AgPass
      * dst[j - o0], and writes
      * per round the totals of its integer steps at binade e and e + 1
      * (words[2k], words[2k+1]; AG_XNOT when they do not apply or e is
-     * unknown) and the chunk's sign tag (words[AG_XWORDS - 1]).  The next
-     * round's gathers are in flight while a round's steps are summed. */
+     * unknown) and the chunk's sign tag (words[AG_XWORDS - 1]). */
     __device__ __forceinline__ void hub_steps(float *dst, uint32_t o0, uint32_t eb, uint32_t ee, uint32_t lane,
                                               const Pair &first, uint32_t e, bool stage, uint32_t *words) const
     {
@@ -539,25 +538,37 @@ struct AgPass
         const bool known = (e >= 24u) & (e <= 253u);
         const float sc = known ? exact_scale(e) : 0.0f;
         uint32_t neg = 0;
-        Pair cur = first;
+        /* two rounds of gathers in flight, as in strided_partial: round k's
+         * steps are summed while round k + 1's values travel and round
+         * k + 2's ids load.  Values outside [eb, ee) gather as +0, whose
+         * step is 0. */
+        uint32_t q0 = eb >> 2;
+        float v[8];
+        {
+            bool in[8];
+            gather8(first, q0 + lane, eb, ee, v, in);
+        }
+        Pair nxt = load_pair(q0 + lane + 64, q1);
         /* the loop runs on the round's first quad, the same in every lane:
          * the warp reductions below need all 32 lanes (lanes past the range
          * load and gather nothing) */
-        for (uint32_t k = 0, q0 = eb >> 2; q0 < q1; ++k, q0 += 64) {
+        for (uint32_t k = 0; q0 < q1; ++k, q0 += 64) {
             const uint32_t qa = q0 + lane;
-            const Pair nx = load_pair(qa + 64, q1);
-            float v[8];
-            bool in[8];
-            gather8(cur, qa, eb, ee, v, in);
+            const Pair nn = load_pair(qa + 128, q1);
+            float vn[8];
+            {
+                bool in[8];
+                gather8(nxt, qa + 64, eb, ee, vn, in);
+            }
             if (stage) {
                 const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    if (in[i])
+                    if (ja + i >= eb && ja + i < ee)
                         dst[ja + i - o0] = v[i];
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    if (in[4 + i])
+                    if (jb + i >= eb && jb + i < ee)
                         dst[jb + i - o0] = v[4 + i];
             }
             if (known && k < AG_XROUNDS) {
@@ -567,10 +578,10 @@ struct AgPass
                 for (int i = 0; i < 8; ++i) {
                     float x = v[i];
                     if (MODE == AG_MODE_DD) {
-                        neg |= in[i] ? dd_neg(x) : 0u;
+                        neg |= dd_neg(x);
                         x = fabsf(x);
                     }
-                    const float x0 = in[i] ? __fmul_rn(x, sc) : 0.0f;
+                    const float x0 = __fmul_rn(x, sc);
                     /* one binade up: half the units (exact, or a value far
                      * below one unit either way) */
                     const float x1 = __fmul_rn(x0, 0.5f);
@@ -589,9 +600,12 @@ struct AgPass
             } else if (MODE == AG_MODE_DD) {
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
-                    neg |= in[i] ? dd_neg(v[i]) : 0u;
+                    neg |= dd_neg(v[i]);
             }
-            cur = nx;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                v[i] = vn[i];
+            nxt = nn;
         }
         if (!known && lane < AG_XROUNDS)
             words[2 * lane] = words[2 * lane + 1] = AG_XNOT;
