@@ -138,7 +138,7 @@ __device__ __forceinline__ uint32_t ag_warp_sum_u(uint32_t v)
 }
 
 /* ------------------------------------------------------------- kernel */
-template <int MODE, int PREC, bool EXACT>
+template <int MODE, int PREC, bool EXACT, bool LOW = false>
 struct AgPass
 {
     const AgPullParams &p;
@@ -147,7 +147,10 @@ struct AgPass
     const uint16_t *c_in16;
     float *c_out32;
     uint16_t *c_out16;
-    uint32_t read_low, write_low;
+    /* this pass reads 16-bit contributions (fixed per kernel body, so that
+     * the 16-bit and 32-bit passes each get their own loads and registers) */
+    static constexpr bool read_low = PREC != 0 && LOW;
+    uint32_t write_low;
     double eps;
     double my_err;
     uint32_t my_active;
@@ -165,7 +168,7 @@ struct AgPass
         pol_last = ag_policy_evict_last();
         my_err = 0.0;
         my_active = 0;
-        read_low = write_low = 0;
+        write_low = 0;
         eps = 0.0;
         c_in32 = nullptr;
         c_in16 = nullptr;
@@ -175,10 +178,8 @@ struct AgPass
         if (MODE != AG_MODE_SPMV) {
             const uint32_t pass = p.ctl->iter;
             eps = p.ctl->eps;
-            if (PREC != 0) {
-                read_low = p.ctl->mode_read;
+            if (PREC != 0)
                 write_low = p.ctl->mode_write;
-            }
             const bool odd = (pass & 1u) != 0;
             c_in32 = odd ? p.c32_1 : p.c32_0;
             c_out32 = odd ? p.c32_0 : p.c32_1;
@@ -843,19 +844,12 @@ static __device__ __forceinline__ uint32_t ag_steal_next(uint32_t *steal, AgStea
     return ntasks;
 }
 
-template <int MODE, int PREC, bool EXACT>
-__global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const AgPullParams p)
+/* one pull pass on this CTA; LOW: the pass reads 16-bit contributions */
+template <int MODE, int PREC, bool EXACT, bool LOW>
+__device__ __forceinline__ void ag_pull_body(const AgPullParams &p, double *s_redd, uint32_t *s_redu,
+                                             uint32_t &s_last, uint64_t &s_bar)
 {
-    __shared__ double s_redd[AG_WARPS];
-    __shared__ uint32_t s_redu[AG_WARPS];
-    __shared__ uint32_t s_last;
-    __shared__ __align__(8) uint64_t s_bar;
-
-    /* stream launches (profiling) run a fixed number of kernels: the ones
-     * after the loop has ended return at once */
-    if ((MODE != AG_MODE_SPMV || p.honor_stop) && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
-        return;
-    AgPass<MODE, PREC, EXACT> ps(p);
+    AgPass<MODE, PREC, EXACT, LOW> ps(p);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float *vals = reinterpret_cast<float *>(ag_dsmem) + warp * AG_WCAP;
     unsigned char *hot = ag_dsmem + AG_STAGE_BYTES;
@@ -893,7 +887,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
      * gathered, reduced and written, so it is in flight meanwhile */
     uint32_t t = blockIdx.x * AG_WARPS + warp;
     uint4 task = t < p.ntasks ? p.tasks[t] : make_uint4(0, 0, 0, 0);
-    typename AgPass<MODE, PREC, EXACT>::Pair pf = ps.prefetch(task.z, task.w, lane);
+    typename AgPass<MODE, PREC, EXACT, LOW>::Pair pf = ps.prefetch(task.z, task.w, lane);
     AgSteal steal;
     while (t < p.ntasks) {
         uint32_t tn = t + nwarps;
@@ -939,7 +933,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 rp = ag_ld_rank(p.rank + r);
                 od = ag_ld_row_u32(p.outdeg + r);
             }
-            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            const typename AgPass<MODE, PREC, EXACT, LOW>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
             ps.stage(vals, eb, ee, lane, pf);
             __syncwarp();
             o0 -= eb;
@@ -1004,7 +998,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                     od = ag_ld_row_u32(p.outdeg + r);
                 }
             }
-            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            const typename AgPass<MODE, PREC, EXACT, LOW>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
             ps.stage(vals, eb, ee, lane, pf);
             __syncwarp();
             o0 -= eb;
@@ -1054,7 +1048,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                 rp = p.rank[r0];
                 od = p.outdeg[r0];
             }
-            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            const typename AgPass<MODE, PREC, EXACT, LOW>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
             float s;
             uint32_t neg = 0;
             if (EXACT) {
@@ -1080,7 +1074,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             const uint32_t pbase = task.y & AG_SLOT_MASK, chunk = task.y >> AG_SLOT_BITS;
             const uint32_t o0 = eb - chunk * p.whub;
             float *row_vals = p.hub_vals + (size_t)pbase * p.whub;
-            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            const typename AgPass<MODE, PREC, EXACT, LOW>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
             if (chunk == 0) {
                 uint32_t neg0 = 0;
                 const float s0 = ps.ordered_sum(vals, eb, ee, lane, pf, neg0);
@@ -1115,7 +1109,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
                         steal.donor = (int)d;
                     }
                 }
-                const typename AgPass<MODE, PREC, EXACT>::XSum xs = AgPass<MODE, PREC, EXACT>::hub_compose(
+                const typename AgPass<MODE, PREC, EXACT, LOW>::XSum xs = AgPass<MODE, PREC, EXACT, LOW>::hub_compose(
                     reinterpret_cast<const uint32_t *>(p.hub_part), p.hub_t, p.hub_pred, row_vals, p.ids, ps.c_in32,
                     vals, p.whub, o0, deg, pbase, nch, lane);
                 const float tot = xs.s;
@@ -1142,7 +1136,7 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
             uint32_t deg = 0;
             if (lane == 0)
                 deg = p.row_off[r0 + 1] - p.row_off[r0];
-            const typename AgPass<MODE, PREC, EXACT>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
+            const typename AgPass<MODE, PREC, EXACT, LOW>::Pair pn = ps.prefetch(task_n.z, task_n.w, lane);
             /* data-driven: each chunk's partial carries the sign of a change
              * among its in-neighbours; the last chunk ORs them */
             uint32_t neg = 0;
@@ -1331,6 +1325,28 @@ __global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const A
         if (p.use_cond)
             cudaGraphSetConditional(p.cond, cont ? 1u : 0u);
     }
+}
+
+template <int MODE, int PREC, bool EXACT>
+__global__ void __launch_bounds__(AG_BLK, AG_CTAS_PER_SM) ag_pull_kernel(const AgPullParams p)
+{
+    __shared__ double s_redd[AG_WARPS];
+    __shared__ uint32_t s_redu[AG_WARPS];
+    __shared__ uint32_t s_last;
+    __shared__ __align__(8) uint64_t s_bar;
+
+    /* stream launches (profiling) run a fixed number of kernels: the ones
+     * after the loop has ended return at once */
+    if ((MODE != AG_MODE_SPMV || p.honor_stop) && !p.use_cond && *((volatile uint32_t *)&p.ctl->stop))
+        return;
+    if constexpr (PREC != 0) {
+        /* the storage this pass reads, set by the pass before */
+        if (*((volatile uint32_t *)&p.ctl->mode_read)) {
+            ag_pull_body<MODE, PREC, EXACT, true>(p, s_redd, s_redu, s_last, s_bar);
+            return;
+        }
+    }
+    ag_pull_body<MODE, PREC, EXACT, false>(p, s_redd, s_redu, s_last, s_bar);
 }
 
 /* init: r = base (or the warm start), first contributions, control reset */
