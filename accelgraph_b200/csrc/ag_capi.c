@@ -13,6 +13,7 @@
  * accelerator calls do (capienv.c:113-131); the *_ex forms return the status.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -37,6 +38,12 @@ static int env_keep(void)
     const char *k = getenv("AG_KEEP_GRAPH");
     return k && k[0] && k[0] != '0';
 }
+
+/* The CSR entry points run one at a time: callers in several host threads
+ * are serialised here, as one context per process with one stream expects
+ * (the reference is not re-entrant either, capienv.c:35-36).  The kept
+ * uploads below are only touched under this lock. */
+static pthread_mutex_t g_csr_lock = PTHREAD_MUTEX_INITIALIZER;
 
 /* ------------------------------------------------ uploads kept between calls */
 /* A caller that solves on one unchanged GraphCSR several times pays the
@@ -133,12 +140,14 @@ ag_status_t ag_graph_forget(const struct GraphCSR *graph)
 {
     int i;
     ag_clear_error();
+    pthread_mutex_lock(&g_csr_lock);
     for (i = 0; i < AG_KEEP_SLOTS; i++) {
         if (g_keep[i].g && (!graph || g_keep[i].graph == graph)) {
             ag_graph_release(g_keep[i].g);
             memset(&g_keep[i], 0, sizeof(g_keep[i]));
         }
     }
+    pthread_mutex_unlock(&g_csr_lock);
     return AG_OK;
 }
 
@@ -182,8 +191,21 @@ void freePageRankStats(struct PageRankStats *stats)
     }
 }
 
+static ag_status_t pagerank_pull_locked(const struct Arguments *arguments, const struct GraphCSR *graph,
+                                        const ag_pr_opts *opts, struct PageRankStats **out);
+
 ag_status_t ag_pagerank_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph,
                                 const ag_pr_opts *opts, struct PageRankStats **out)
+{
+    ag_status_t st;
+    pthread_mutex_lock(&g_csr_lock);
+    st = pagerank_pull_locked(arguments, graph, opts, out);
+    pthread_mutex_unlock(&g_csr_lock);
+    return st;
+}
+
+static ag_status_t pagerank_pull_locked(const struct Arguments *arguments, const struct GraphCSR *graph,
+                                        const ag_pr_opts *opts, struct PageRankStats **out)
 {
     ag_pr_opts o;
     ag_pr_result res;
@@ -454,8 +476,21 @@ void freeSPMVStats(struct SPMVStats *stats)
     }
 }
 
+static ag_status_t spmv_pull_locked(const struct Arguments *arguments, const struct GraphCSR *graph, int quiet,
+                                    struct SPMVStats **out);
+
 ag_status_t ag_spmv_pull_ex(const struct Arguments *arguments, const struct GraphCSR *graph, int quiet,
                             struct SPMVStats **out)
+{
+    ag_status_t st;
+    pthread_mutex_lock(&g_csr_lock);
+    st = spmv_pull_locked(arguments, graph, quiet, out);
+    pthread_mutex_unlock(&g_csr_lock);
+    return st;
+}
+
+static ag_status_t spmv_pull_locked(const struct Arguments *arguments, const struct GraphCSR *graph, int quiet,
+                                    struct SPMVStats **out)
 {
     ag_graph_t g = NULL;
     int kept = 0;

@@ -50,8 +50,14 @@ static AgContext g_ctx = {0, -1, 0, nullptr};
 
 static ag_status_t ctx_ensure(int want_device)
 {
-    if (g_ctx.ready && (want_device < 0 || want_device == g_ctx.device))
+    if (g_ctx.ready && (want_device < 0 || want_device == g_ctx.device)) {
+        /* a call from another host thread: make the library's device the
+         * current one there too */
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != g_ctx.device)
+            AG_CUDA(cudaSetDevice(g_ctx.device));
         return AG_OK;
+    }
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || n == 0) {

@@ -15,8 +15,11 @@
  *     checkout, so these restate its documented behaviour (-k: drop self loops
  *     and duplicates and sort, accel-graph.c:142-145,336-337).
  * All pointers are plain host or device pointers; no library types from any
- * framework appear in the signatures.  Every call is made from one host
- * thread at a time (the reference is not re-entrant either, capienv.c:35-36).
+ * framework appear in the signatures.  The CSR entry points (pageRank.h,
+ * SPMV.h, ag_pagerank_pull_ex, ag_spmv_pull_ex, ag_graph_forget) serialise
+ * callers from several host threads behind one lock; the handle API below is
+ * called from one host thread at a time (the reference is not re-entrant
+ * either, capienv.c:35-36).
  */
 #ifndef ACCELGRAPH_B200_H
 #define ACCELGRAPH_B200_H

@@ -11,9 +11,9 @@ EXACT order sums every row in the reference loop's stream order: ranks,
 iteration count and the number of vertices still moving by eps or more in
 every pass equal the oracle's (the restatement of pageRank.c:942-1109 and the
 sequential binary32 gather of the compute units) bit for bit.  FAST order
-stays within 1e-5 relative L1 of the oracle's ranks, the north star's
-tolerance for binary32 results; its iteration count may differ by a few
-passes at eps 1e-6.  The SpMV product follows SPMV.c:1200-1224.
+stays within 1e-5 relative L1 of the oracle's ranks, the tolerance asked of
+binary32 results; its iteration count may differ by a few passes at eps
+1e-6.  The SpMV product follows SPMV.c:1200-1224.
 """
 import numpy as np
 import pytest

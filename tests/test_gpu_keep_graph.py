@@ -101,3 +101,34 @@ def test_spmv_keeps_its_upload_under_the_environment_switch(gpu, oracle, monkeyp
         assert np.abs(ys[0].astype(np.float64) - yo).sum() <= 1e-5 * np.abs(yo.astype(np.float64)).sum()
     finally:
         ag.check(ag.lib.ag_graph_forget(None), "ag_graph_forget")
+
+
+def test_csr_entry_points_serialise_concurrent_callers(gpu, oracle):
+    """Four host threads call ag_pagerank_pull_ex (the entry under
+    pageRankPullGraphCSR) at once; ctypes releases the GIL, so the library's
+    lock is what keeps them apart.  Each gets the oracle's ranks bit for
+    bit."""
+    import threading
+
+    ag = gpu
+    gs = [ag.Graph.rmat(12, 16, seed=40 + i) for i in range(4)]
+    want = [_oracle(oracle, g, 40, 1e-7) for g in gs]
+    got = [None] * 4
+
+    def run(i):
+        args = ag.default_arguments(40, 1e-7)
+        opts = ag.make_opts(order=ag.AG_ORDER_EXACT, quiet=True)
+        out = C.POINTER(ag.PageRankStats)()
+        st = ag.lib.ag_pagerank_pull_ex(C.byref(args), gs[i].ptr, C.byref(opts), C.byref(out))
+        if st == 0:
+            got[i] = (ag.stats_ranks(out), out.contents.iterations)
+            ag.lib.freePageRankStats(out)
+
+    ts = [threading.Thread(target=run, args=(i,)) for i in range(4)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=300)
+    for i in range(4):
+        assert got[i] is not None
+        assert np.array_equal(got[i][0], want[i]["ranks"]) and got[i][1] == want[i]["iterations"]
