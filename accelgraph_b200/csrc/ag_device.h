@@ -61,11 +61,17 @@ static inline unsigned ag_sm_grid(unsigned per_sm)
 #error "AG_WHUB must be a multiple of 32 (EXACT-order hub rows are read in 16-byte groups)"
 #endif
 #ifndef AG_STEAL_MIN
-#define AG_STEAL_MIN 32768 /* EXACT order: the warp that sums a hub row of at
-                              least this many in-edges gives the rest of its
-                              work list away to warps that run out of work */
+#define AG_STEAL_MIN 4096  /* EXACT order: the warp that composes a hub row of
+                              at least this many in-edges gives the rest of
+                              its work list away to warps that run out of
+                              work (measured best of 2049 .. 32768 at R-MAT
+                              s22 and s24, with AG_STEAL_CAP 4096)          */
 #endif
-#define AG_STEAL_CAP 256  /* donors per pass                                 */
+#ifndef AG_STEAL_CAP
+#define AG_STEAL_CAP 4096 /* donors per pass: above the number of rows of
+                             AG_STEAL_MIN in-edges or more at R-MAT s24,
+                             whose composers all give their lists away    */
+#endif
 #define AG_XWORDS 64      /* EXACT order: words per hub chunk of integer step
                              totals (two per 256-value round, the last word
                              the chunk's data-driven sign tag)              */

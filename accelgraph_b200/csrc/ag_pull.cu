@@ -1196,15 +1196,24 @@ __device__ __forceinline__ void ag_pull_body(const AgPullParams &p, double *s_re
         t = tn;
     }
 
-    if (EXACT && lane == 0) {
-        /* the last warp out clears the donor table for the next pass */
-        __threadfence();
-        if (atomicAdd(p.steal + 1, 1u) == nwarps - 1) {
+    if (EXACT) {
+        /* the last warp out clears the donor table for the next pass, its
+         * lanes taking every 32nd entry */
+        uint32_t out = 0;
+        if (lane == 0) {
+            __threadfence();
+            out = atomicAdd(p.steal + 1, 1u) == nwarps - 1 ? 1u : 0u;
+        }
+        if (__shfl_sync(0xffffffffu, out, 0)) {
+            __threadfence();
             const uint32_t n = min(*((volatile uint32_t *)p.steal), (uint32_t)AG_STEAL_CAP);
-            for (uint32_t d = 0; d < n; ++d)
+            for (uint32_t d = lane; d < n; d += 32)
                 p.steal[2 + 2 * d] = 0;
-            p.steal[0] = 0;
-            p.steal[1] = 0;
+            __syncwarp();
+            if (lane == 0) {
+                p.steal[0] = 0;
+                p.steal[1] = 0;
+            }
             __threadfence();
         }
     }
