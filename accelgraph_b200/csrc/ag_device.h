@@ -79,7 +79,9 @@ static inline unsigned ag_sm_grid(unsigned per_sm)
 #define AG_XNOT 0x80000000u /* a round's total that does not apply          */
 #define AG_XFELL 0x100u   /* hub_pred: the chunk had a round summed one value
                              after another in the pass before              */
+#ifndef AG_STEAL_PROBES
 #define AG_STEAL_PROBES 8 /* donor entries a warp out of work tries          */
+#endif
 #define AG_STEAL_WORDS (2 + 2 * AG_STEAL_CAP)
 #define AG_STAGE_BYTES (AG_WARPS * AG_WCAP * 4)
 #if AG_CTAS_PER_SM == 1
