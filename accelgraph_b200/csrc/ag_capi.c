@@ -212,7 +212,7 @@ static ag_status_t pagerank_pull_locked(const struct Arguments *arguments, const
     ag_graph_t g = NULL;
     int kept = 0;
     ag_status_t st;
-    struct PageRankStats *stats;
+    struct PageRankStats *stats = NULL;
     uint32_t *h_active = NULL;
     double *h_err = NULL, *h_sec = NULL;
     uint32_t cap, i;
@@ -227,10 +227,6 @@ static ag_status_t pagerank_pull_locked(const struct Arguments *arguments, const
     if (opts)
         memcpy(&o, opts, opts->struct_size && opts->struct_size < sizeof(o) ? opts->struct_size : sizeof(o));
     quiet = o.quiet || env_quiet();
-
-    stats = newPageRankStatsGraphCSR((struct GraphCSR *)graph);
-    if (!stats)
-        return ag_set_error(AG_ERR_OOM, "stats allocation failed");
 
     if (!quiet) {
         printf(" -----------------------------------------------------\n");
@@ -275,6 +271,13 @@ static ag_status_t pagerank_pull_locked(const struct Arguments *arguments, const
     st = ag_pagerank_launch(g, arguments->iterations, arguments->epsilon, &o);
     if (st != AG_OK)
         goto fail;
+    /* the host allocates and first-touches the stats object while the
+     * device solves */
+    stats = newPageRankStatsGraphCSR((struct GraphCSR *)graph);
+    if (!stats) {
+        st = ag_set_error(AG_ERR_OOM, "stats allocation failed");
+        goto fail;
+    }
     cap = arguments->iterations ? arguments->iterations : 1;
     h_active = (uint32_t *)calloc(cap, sizeof(uint32_t));
     h_err = (double *)calloc(cap, sizeof(double));
