@@ -537,7 +537,10 @@ static ag_status_t spmv_pull_locked(const struct Arguments *arguments, const str
         st = ag_set_error(AG_ERR_OOM, "allocation failed");
         goto fail;
     }
-    st = ag_spmv_run_host(g, stats->vector_input, stats->vector_output, iters, AG_SPMV_GRAPH_WEIGHTS, sec);
+    /* rows summed in stream order: the reference's sequential binary32 sums
+     * (cu_sum_kernel_control.sv), bit for bit */
+    st = ag_spmv_run_host(g, stats->vector_input, stats->vector_output, iters, AG_SPMV_GRAPH_WEIGHTS | AG_SPMV_EXACT,
+                          sec);
     if (st != AG_OK)
         goto fail;
     stats->iterations = iters;
