@@ -539,28 +539,10 @@ struct AgPass
         const bool known = (e >= 24u) & (e <= 253u);
         const float sc = known ? exact_scale(e) : 0.0f;
         uint32_t neg = 0;
-        /* two rounds of gathers in flight, as in strided_partial: round k's
-         * steps are summed while round k + 1's values travel and round
-         * k + 2's ids load.  Values outside [eb, ee) gather as +0, whose
-         * step is 0. */
-        uint32_t q0 = eb >> 2;
-        float v[8];
-        {
-            bool in[8];
-            gather8(first, q0 + lane, eb, ee, v, in);
-        }
-        Pair nxt = load_pair(q0 + lane + 64, q1);
-        /* the loop runs on the round's first quad, the same in every lane:
-         * the warp reductions below need all 32 lanes (lanes past the range
-         * load and gather nothing) */
-        for (uint32_t k = 0; q0 < q1; ++k, q0 += 64) {
-            const uint32_t qa = q0 + lane;
-            const Pair nn = load_pair(qa + 128, q1);
-            float vn[8];
-            {
-                bool in[8];
-                gather8(nxt, qa + 64, eb, ee, vn, in);
-            }
+        /* round k's values v (quads qa and qa + 32): staged when asked, and
+         * their integer steps summed.  Values outside [eb, ee) gather as +0,
+         * whose step is 0. */
+        auto round = [&](uint32_t k, uint32_t qa, const float *v) {
             if (stage) {
                 const uint32_t ja = qa << 2, jb = (qa + 32) << 2;
 #pragma unroll
@@ -603,10 +585,47 @@ struct AgPass
                 for (int i = 0; i < 8; ++i)
                     neg |= dd_neg(v[i]);
             }
+        };
+        /* the loop runs on the round's first quad, the same in every lane:
+         * the warp reductions need all 32 lanes (lanes past the range load
+         * and gather nothing) */
+        uint32_t q0 = eb >> 2;
+        if (MODE == AG_MODE_SPMV) {
+            /* weighted pairs take twice the registers: one round in flight */
+            Pair cur = first;
+            for (uint32_t k = 0; q0 < q1; ++k, q0 += 64) {
+                const uint32_t qa = q0 + lane;
+                const Pair nx = load_pair(qa + 64, q1);
+                float v[8];
+                bool in[8];
+                gather8(cur, qa, eb, ee, v, in);
+                round(k, qa, v);
+                cur = nx;
+            }
+        } else {
+            /* two rounds of gathers in flight, as in strided_partial: round
+             * k's steps are summed while round k + 1's values travel and
+             * round k + 2's ids load */
+            float v[8];
+            {
+                bool in[8];
+                gather8(first, q0 + lane, eb, ee, v, in);
+            }
+            Pair nxt = load_pair(q0 + lane + 64, q1);
+            for (uint32_t k = 0; q0 < q1; ++k, q0 += 64) {
+                const uint32_t qa = q0 + lane;
+                const Pair nn = load_pair(qa + 128, q1);
+                float vn[8];
+                {
+                    bool in[8];
+                    gather8(nxt, qa + 64, eb, ee, vn, in);
+                }
+                round(k, qa, v);
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                v[i] = vn[i];
-            nxt = nn;
+                for (int i = 0; i < 8; ++i)
+                    v[i] = vn[i];
+                nxt = nn;
+            }
         }
         if (!known && lane < AG_XROUNDS)
             words[2 * lane] = words[2 * lane + 1] = AG_XNOT;
