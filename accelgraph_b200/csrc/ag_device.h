@@ -265,6 +265,9 @@ typedef struct AgGraphView
     const uint32_t *row_off, *ids, *outdeg, *perm, *inv;
     uint32_t N, E;
     cudaStream_t stream;
+    const uint4 *tasks;  /* the pull kernel's FAST-order work list           */
+    uint32_t ntasks;
+    uint32_t hub_slots;  /* hub chunks in it (slot indexes of HUB items)     */
 } AgGraphView;
 
 /* device planner of the work lists (ag_plan.cu): hub chunks, long rows not

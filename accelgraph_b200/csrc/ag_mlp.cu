@@ -72,79 +72,183 @@ __global__ void ag_deg2_kernel(AgGraphView gv, uint2 *deg2)
         deg2[v] = make_uint2(gv.row_off[v + 1] - gv.row_off[v], gv.outdeg[v]);
 }
 
-/* the eight features of a vertex, written in caller order */
+/* Per-row statistics of the in-neighbours u, all integers so that they
+ * come out the same in any order and on any split of the row: sums of u's
+ * in- and out-degree, the sum of 1/out-degree(u) in fixed point (2^40 units,
+ * one binary32 reciprocal per edge), and the extremes of the degrees. */
+struct AgFeatAcc
+{
+    unsigned long long s_in, s_out, s_c;
+    uint32_t mx_in, mx_out, mn_out;
+};
+
+#define AG_FEAT_FIX 1099511627776.0 /* 2^40 */
+
+__device__ __forceinline__ AgFeatAcc ag_feat_zero()
+{
+    AgFeatAcc a;
+    a.s_in = a.s_out = a.s_c = 0ull;
+    a.mx_in = a.mx_out = 0u;
+    a.mn_out = 0xFFFFFFFFu;
+    return a;
+}
+
+__device__ __forceinline__ void ag_feat_edge(uint2 d, AgFeatAcc &a)
+{
+    a.s_in += d.x;
+    a.s_out += d.y;
+    a.s_c += d.y ? __double2ull_rn((double)__frcp_rn((float)d.y) * AG_FEAT_FIX) : 0ull;
+    a.mx_in = max(a.mx_in, d.x);
+    a.mx_out = max(a.mx_out, d.y);
+    a.mn_out = min(a.mn_out, d.y);
+}
+
+__device__ __forceinline__ AgFeatAcc ag_feat_warp(AgFeatAcc a)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a.s_in += __shfl_xor_sync(0xffffffffu, a.s_in, o);
+        a.s_out += __shfl_xor_sync(0xffffffffu, a.s_out, o);
+        a.s_c += __shfl_xor_sync(0xffffffffu, a.s_c, o);
+    }
+    a.mx_in = __reduce_max_sync(0xffffffffu, a.mx_in);
+    a.mx_out = __reduce_max_sync(0xffffffffu, a.mx_out);
+    a.mn_out = __reduce_min_sync(0xffffffffu, a.mn_out);
+    return a;
+}
+
+/* the warp's lane-strided pass over in-edges [b, e) */
+__device__ __forceinline__ AgFeatAcc ag_feat_range(const AgGraphView &gv, const uint2 *deg2, uint32_t b, uint32_t e,
+                                                   uint32_t lane)
+{
+    AgFeatAcc a = ag_feat_zero();
+    uint32_t j = b + lane;
+    for (; j + 96 < e; j += 128) {
+        const uint32_t u0 = __ldg(gv.ids + j), u1 = __ldg(gv.ids + j + 32), u2 = __ldg(gv.ids + j + 64),
+                       u3 = __ldg(gv.ids + j + 96);
+        const uint2 d0 = __ldg(deg2 + u0), d1 = __ldg(deg2 + u1), d2 = __ldg(deg2 + u2), d3 = __ldg(deg2 + u3);
+        ag_feat_edge(d0, a);
+        ag_feat_edge(d1, a);
+        ag_feat_edge(d2, a);
+        ag_feat_edge(d3, a);
+    }
+    for (; j < e; j += 32)
+        ag_feat_edge(__ldg(deg2 + __ldg(gv.ids + j)), a);
+    return ag_feat_warp(a);
+}
+
+/* the eight features of a vertex, written in caller order (two 16-byte
+ * stores when the output is 16-byte aligned) */
 __device__ __forceinline__ void ag_features_store(const AgGraphView &gv, float *X, uint32_t v, uint32_t deg,
-                                                  float s_in, float s_out, float s_c, float mn_out, float mx_out,
-                                                  float mx_in)
+                                                  const AgFeatAcc &a, bool vec)
 {
     const uint32_t dst = gv.perm ? gv.perm[v] : v;
     float *x = X + (size_t)dst * AG_MLP_IN;
-    x[0] = log1pf((float)deg);
-    x[1] = log1pf((float)gv.outdeg[v]);
-    x[2] = log1pf(s_in);
-    x[3] = log1pf(s_out);
-    x[4] = log1pf(deg ? mn_out : 0.0f);
-    x[5] = log1pf(mx_out);
-    x[6] = log1pf(s_c);
-    x[7] = log1pf(mx_in);
-}
-
-/* Vertices of at most 32 in-edges, one per lane.  Degree sums are sums of
- * integers below 2^24, exact in any order. */
-__global__ void ag_features_kernel(AgGraphView gv, const uint2 *deg2, float *X)
-{
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < gv.N; v += gridDim.x * blockDim.x) {
-        const uint32_t b = gv.row_off[v], e = gv.row_off[v + 1];
-        if (e - b > 32)
-            continue;
-        float s_in = 0.f, s_out = 0.f, s_c = 0.f, mx_in = 0.f, mx_out = 0.f, mn_out = 3.0e38f;
-        for (uint32_t j = b; j < e; ++j) {
-            const uint2 d = __ldg(deg2 + __ldg(gv.ids + j));
-            const float din = (float)d.x, dout = (float)d.y;
-            s_in += din;
-            s_out += dout;
-            s_c += d.y ? 1.0f / dout : 0.0f;
-            mx_in = fmaxf(mx_in, din);
-            mx_out = fmaxf(mx_out, dout);
-            mn_out = fminf(mn_out, dout);
-        }
-        ag_features_store(gv, X, v, e - b, s_in, s_out, s_c, mn_out, mx_out, mx_in);
+    const float4 lo = make_float4(log1pf((float)deg), log1pf((float)gv.outdeg[v]), log1pf((float)a.s_in),
+                                  log1pf((float)a.s_out));
+    const float4 hi = make_float4(log1pf(deg ? (float)a.mn_out : 0.0f), log1pf((float)a.mx_out),
+                                  log1pf((float)((double)a.s_c * (1.0 / AG_FEAT_FIX))), log1pf((float)a.mx_in));
+    if (vec) {
+        reinterpret_cast<float4 *>(x)[0] = lo;
+        reinterpret_cast<float4 *>(x)[1] = hi;
+    } else {
+        x[0] = lo.x;
+        x[1] = lo.y;
+        x[2] = lo.z;
+        x[3] = lo.w;
+        x[4] = hi.x;
+        x[5] = hi.y;
+        x[6] = hi.z;
+        x[7] = hi.w;
     }
 }
 
-/* Vertices of more than 32 in-edges, one warp each (lane-strided partials,
- * xor tree), so that the long rows, which the relabelling puts side by side,
- * spread over all warps. */
-__global__ void ag_features_long_kernel(AgGraphView gv, const uint2 *deg2, float *X)
+/* All features in one pass over the pull kernel's work list, so that the
+ * gathers are balanced as the pull's are (a warp per item):
+ *  - row items: one row per lane; rows of up to 32 in-edges by their lane
+ *    (four gathers in flight), longer ones by the whole warp;
+ *  - long rows: the whole warp;
+ *  - hub chunks: the whole warp, then integer atomics into the row's slot
+ *    (acc: three sums, ext: two maxima, the complemented minimum, and the
+ *    in-edges seen); the chunk that completes the row writes it. */
+__global__ void __launch_bounds__(256) ag_features_items_kernel(AgGraphView gv, const uint2 *deg2,
+                                                                unsigned long long *acc, uint32_t *ext, float *X)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < gv.N; v += nw) {
-        const uint32_t b = gv.row_off[v], e = gv.row_off[v + 1];
-        if (e - b <= 32)
-            continue;
-        float a_in = 0.f, a_out = 0.f, a_c = 0.f, x_in = 0.f, x_out = 0.f, n_out = 3.0e38f;
-        for (uint32_t j = b + lane; j < e; j += 32) {
-            const uint2 d = __ldg(deg2 + __ldg(gv.ids + j));
-            const float din = (float)d.x, dout = (float)d.y;
-            a_in += din;
-            a_out += dout;
-            a_c += d.y ? 1.0f / dout : 0.0f;
-            x_in = fmaxf(x_in, din);
-            x_out = fmaxf(x_out, dout);
-            n_out = fminf(n_out, dout);
+    const bool vec = (reinterpret_cast<uintptr_t>(X) & 15u) == 0;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < gv.ntasks; t += nw) {
+        const uint4 task = gv.tasks[t];
+        const uint32_t kind = task.x >> 30, r0 = task.x & AG_ROW_MASK;
+        if (kind == AG_T_ROWS) {
+            const uint32_t r = r0 + lane;
+            const bool live = r < task.y;
+            uint32_t b = 0, e = 0;
+            if (live) {
+                b = gv.row_off[r];
+                e = gv.row_off[r + 1];
+            }
+            AgFeatAcc a = ag_feat_zero();
+            const bool mine = live && e - b <= 32;
+            if (mine) {
+                uint32_t j = b;
+                for (; j + 4 <= e; j += 4) {
+                    const uint32_t u0 = __ldg(gv.ids + j), u1 = __ldg(gv.ids + j + 1), u2 = __ldg(gv.ids + j + 2),
+                                   u3 = __ldg(gv.ids + j + 3);
+                    const uint2 d0 = __ldg(deg2 + u0), d1 = __ldg(deg2 + u1), d2 = __ldg(deg2 + u2),
+                                d3 = __ldg(deg2 + u3);
+                    ag_feat_edge(d0, a);
+                    ag_feat_edge(d1, a);
+                    ag_feat_edge(d2, a);
+                    ag_feat_edge(d3, a);
+                }
+                for (; j < e; ++j)
+                    ag_feat_edge(__ldg(deg2 + __ldg(gv.ids + j)), a);
+            }
+            unsigned m = __ballot_sync(0xffffffffu, live && !mine);
+            while (m) {
+                const int src = __ffs(m) - 1;
+                m &= m - 1;
+                const AgFeatAcc w =
+                    ag_feat_range(gv, deg2, __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, e, src), lane);
+                if ((int)lane == src)
+                    a = w;
+            }
+            if (live)
+                ag_features_store(gv, X, r, e - b, a, vec);
+        } else if (kind == AG_T_LONG) {
+            const AgFeatAcc w = ag_feat_range(gv, deg2, task.z, task.w, lane);
+            if (lane == 0)
+                ag_features_store(gv, X, r0, task.w - task.z, w, vec);
+        } else {
+            const AgFeatAcc w = ag_feat_range(gv, deg2, task.z, task.w, lane);
+            if (lane == 0) {
+                const uint32_t slot = task.y & AG_SLOT_MASK;
+                unsigned long long *ac = acc + (size_t)slot * 3;
+                uint32_t *ex = ext + (size_t)slot * 4;
+                atomicAdd(ac, w.s_in);
+                atomicAdd(ac + 1, w.s_out);
+                atomicAdd(ac + 2, w.s_c);
+                atomicMax(ex, w.mx_in);
+                atomicMax(ex + 1, w.mx_out);
+                atomicMax(ex + 2, 0xFFFFFFFFu - w.mn_out);
+                __threadfence();
+                const uint32_t deg = gv.row_off[r0 + 1] - gv.row_off[r0];
+                const uint32_t seen = atomicAdd(ex + 3, task.w - task.z) + (task.w - task.z);
+                if (seen == deg) {
+                    /* every chunk of the row is in: the row's totals */
+                    __threadfence();
+                    AgFeatAcc a;
+                    a.s_in = __ldcg(ac);
+                    a.s_out = __ldcg(ac + 1);
+                    a.s_c = __ldcg(ac + 2);
+                    a.mx_in = __ldcg(ex);
+                    a.mx_out = __ldcg(ex + 1);
+                    a.mn_out = 0xFFFFFFFFu - __ldcg(ex + 2);
+                    ag_features_store(gv, X, r0, deg, a, vec);
+                }
+            }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a_in += __shfl_xor_sync(0xffffffffu, a_in, o);
-            a_out += __shfl_xor_sync(0xffffffffu, a_out, o);
-            a_c += __shfl_xor_sync(0xffffffffu, a_c, o);
-            x_in = fmaxf(x_in, __shfl_xor_sync(0xffffffffu, x_in, o));
-            x_out = fmaxf(x_out, __shfl_xor_sync(0xffffffffu, x_out, o));
-            n_out = fminf(n_out, __shfl_xor_sync(0xffffffffu, n_out, o));
-        }
-        if (lane == 0)
-            ag_features_store(gv, X, v, e - b, a_in, a_out, a_c, n_out, x_out, x_in);
     }
 }
 
@@ -587,16 +691,33 @@ extern "C" ag_status_t ag_features(ag_graph_t g, float *features)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_features: NULL output");
     if (gv.N == 0)
         return AG_OK;
-    uint2 *deg2 = nullptr;
-    MCHK(cudaMallocAsync((void **)&deg2, (size_t)gv.N * sizeof(uint2), gv.stream));
-    uint64_t blocks = ((uint64_t)gv.N + 255) / 256;
-    if (blocks > ag_sm_grid(16))
-        blocks = ag_sm_grid(16);
-    ag_deg2_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2);
-    ag_features_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2, features);
-    ag_features_long_kernel<<<ag_sm_grid(16), 256, 0, gv.stream>>>(gv, deg2, features);
-    const cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(deg2, gv.stream);
+    if (!gv.tasks)
+        return ag_set_error(AG_ERR_INVALID_ARG, "ag_features: the graph has no work list");
+    /* deg2, then the hub rows' slots: three 64-bit sums and four words each */
+    const size_t deg2_bytes = ((size_t)gv.N * sizeof(uint2) + 255) & ~(size_t)255;
+    const size_t acc_bytes = (size_t)gv.hub_slots * 3 * sizeof(unsigned long long);
+    const size_t ext_bytes = (size_t)gv.hub_slots * 4 * sizeof(uint32_t);
+    unsigned char *buf = nullptr;
+    MCHK(cudaMallocAsync((void **)&buf, deg2_bytes + acc_bytes + ext_bytes + 16, gv.stream));
+    uint2 *deg2 = reinterpret_cast<uint2 *>(buf);
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(buf + deg2_bytes);
+    uint32_t *ext = reinterpret_cast<uint32_t *>(buf + deg2_bytes + acc_bytes);
+    cudaError_t e = cudaSuccess;
+    if (acc_bytes)
+        e = cudaMemsetAsync(acc, 0, acc_bytes + ext_bytes, gv.stream);
+    if (e == cudaSuccess) {
+        uint64_t blocks = ((uint64_t)gv.N + 255) / 256;
+        if (blocks > ag_sm_grid(16))
+            blocks = ag_sm_grid(16);
+        ag_deg2_kernel<<<(unsigned)blocks, 256, 0, gv.stream>>>(gv, deg2);
+        uint64_t iblocks = ((uint64_t)gv.ntasks * 32 + 255) / 256;
+        if (iblocks > ag_sm_grid(8))
+            iblocks = ag_sm_grid(8);
+        if (iblocks)
+            ag_features_items_kernel<<<(unsigned)iblocks, 256, 0, gv.stream>>>(gv, deg2, acc, ext, features);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(buf, gv.stream);
     MCHK(e);
     return AG_OK;
 }

@@ -1889,6 +1889,9 @@ extern "C" ag_status_t ag_rt_graph_view(ag_graph_t g, AgGraphView *v)
     v->N = g->N;
     v->E = g->E;
     v->stream = g_ctx.stream;
+    v->tasks = g->tasks_fast;
+    v->ntasks = g->ntasks_fast;
+    v->hub_slots = g->nparts;
     return AG_OK;
 }
 
