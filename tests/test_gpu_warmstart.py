@@ -38,6 +38,38 @@ def test_features_match_numpy(gpu):
     np.testing.assert_allclose(X, _np_features(g), rtol=2e-6, atol=2e-6)
 
 
+@pytest.mark.parametrize("tiles", [None, (64, 128)])
+def test_features_of_split_rows_and_unaligned_output(gpu, tiles):
+    """Rows of every kind the work list has (short, up to 256, up to the hub
+    chunk, split into chunks), with the default tiles and with 128-edge hub
+    chunks that split every row above 128 in-edges; the output written once
+    16-byte aligned and once 4 bytes off."""
+    import ctypes as C
+
+    import torch
+
+    ag = gpu
+    rng = np.random.default_rng(11)
+    n = 6000
+    src = [rng.integers(0, n, 40000)]
+    dst = [rng.integers(0, n, 40000)]
+    for v, d in zip((5, 17, 300, 4001, 5999), (100, 700, 2500, 5000, 5999)):
+        src.append(rng.choice(n, size=d, replace=False))
+        dst.append(np.full(d, v))
+    g = ag.Graph.from_edges(n, np.concatenate(src), np.concatenate(dst), flags=ag.AG_BUILD_DEDUPE)
+    assert int(g.in_degree().max()) > 2048
+    dg = ag.DeviceGraph(g)
+    if tiles:
+        dg.set_tiles(tiles[0], tiles[1])
+    want = _np_features(g)
+    buf = torch.empty(n * 8 + 4, dtype=torch.float32, device="cuda")
+    for off in (0, 1):
+        ag.check(ag.lib.ag_features(dg.h, buf.data_ptr() + 4 * off), "ag_features")
+        torch.cuda.synchronize()
+        X = buf[off:off + n * 8].cpu().numpy().reshape(n, 8)
+        np.testing.assert_allclose(X, want, rtol=2e-6, atol=2e-6)
+
+
 def test_mlp_forward_and_gradients_match_oracle(gpu):
     ag = gpu
     import torch
