@@ -1881,6 +1881,9 @@ extern "C" ag_status_t ag_rt_graph_view(ag_graph_t g, AgGraphView *v)
 {
     if (!g || !v)
         return ag_set_error(AG_ERR_INVALID_ARG, "NULL graph");
+    if (g->norm_n)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "a row-partitioned graph names other ranks' rows by global id; this "
+                            "entry needs a whole graph");
     v->row_off = g->row_off;
     v->ids = g->ids;
     v->outdeg = g->outdeg;

@@ -37,3 +37,29 @@ def test_rows_partition_single_rank_matches_oracle(gpu, oracle):
         assert np.abs(ranks.astype(np.float64) - ref["ranks"]).sum() / ref["ranks"].sum() <= 1e-5
     finally:
         dist.destroy_process_group()
+
+
+def test_whole_graph_entries_refuse_a_row_partition(gpu):
+    """A rank's row upload names the other ranks' rows by padded global id,
+    so the entries that need a whole graph (features, warm start, PPR)
+    refuse it instead of reading past their per-vertex arrays."""
+    import ctypes as C
+
+    import torch
+
+    ag = gpu
+    g = ag.Graph.rmat(10, 8)
+    n = g.num_vertices
+    bounds = np.array([0, n // 2, n], np.uint32)
+    h = C.c_void_p()
+    ag.check(ag.lib.ag_graph_upload_rows(g.ptr, bounds.ctypes.data_as(C.POINTER(C.c_uint32)), 2, 1, n, 0,
+                                         C.byref(h)), "ag_graph_upload_rows")
+    try:
+        X = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+        assert ag.lib.ag_features(h, X.data_ptr()) == ag.AG_ERR_UNSUPPORTED
+        src = np.array([0], np.uint32)
+        out = np.empty(n, np.float32)
+        assert ag.lib.ag_ppr_spmm(h, src.ctypes.data_as(C.POINTER(C.c_uint32)), 1, 3, C.c_double(1e-4),
+                                  out.ctypes.data_as(ag.f32p), None) == ag.AG_ERR_UNSUPPORTED
+    finally:
+        ag.lib.ag_graph_release(h)
