@@ -1581,12 +1581,24 @@ extern "C" void ag_pr_opts_init(ag_pr_opts *o)
     o->switch_residual = 1e-4;
 }
 
+/* a row-partitioned upload names other ranks' rows by padded global id and
+ * writes its contributions at its slice of a full-length vector: only the
+ * ag_partition_* entries run on it */
+static ag_status_t whole_graph(const ag_graph_s *g, const char *what)
+{
+    if (g->norm_n)
+        return ag_set_error(AG_ERR_UNSUPPORTED, "%s: a row-partitioned graph runs through ag_partition_step", what);
+    return AG_OK;
+}
+
 extern "C" ag_status_t ag_pagerank_launch(ag_graph_t g, uint32_t max_iterations, double epsilon,
                                           const ag_pr_opts *opts)
 {
     ag_clear_error();
     if (!g)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_launch: NULL graph");
+    if (whole_graph(g, "ag_pagerank_launch") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     ag_pr_opts o;
     ag_pr_opts_init(&o);
     if (opts)
@@ -1739,6 +1751,8 @@ extern "C" ag_status_t ag_spmv_pull_device(ag_graph_t g, const float *x, float *
     ag_clear_error();
     if (!g || (g->N && (!x || !y)))
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull_device: NULL argument");
+    if (whole_graph(g, "ag_spmv_pull_device") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     if (g->N == 0)
         return AG_OK;
     cudaStream_t s = g_ctx.stream;
@@ -1775,6 +1789,8 @@ extern "C" ag_status_t ag_spmv_pull(ag_graph_t g, const float *x, float *y, uint
     ag_clear_error();
     if (!g || (g->N && (!x || !y)))
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_pull: NULL argument");
+    if (whole_graph(g, "ag_spmv_pull") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     if (g->N == 0)
         return AG_OK;
     ag_status_t st = AG_OK;
@@ -1799,6 +1815,8 @@ extern "C" ag_status_t ag_pagerank_f64(ag_graph_t g, uint32_t max_iterations, do
     ag_clear_error();
     if (!g || !ranks)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_pagerank_f64: NULL argument");
+    if (whole_graph(g, "ag_pagerank_f64") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     cudaStream_t s = g_ctx.stream;
     double *r = nullptr, *r2 = nullptr, *c = nullptr, *md = nullptr;
     const size_t nb = (size_t)g->N * 8 + 16;
@@ -1838,6 +1856,8 @@ extern "C" ag_status_t ag_spmv_run_host(ag_graph_t g, const float *x, float *y, 
 {
     if (!g || (g->N && (!x || !y)))
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_spmv_run_host: NULL argument");
+    if (whole_graph(g, "ag_spmv_run_host") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     if (g->N == 0)
         return AG_OK;
     cudaStream_t s = g_ctx.stream;
@@ -2060,6 +2080,8 @@ extern "C" ag_status_t ag_autotune(ag_graph_t g, uint32_t passes, ag_tile_config
     ag_clear_error();
     if (!g)
         return ag_set_error(AG_ERR_INVALID_ARG, "ag_autotune: NULL graph");
+    if (whole_graph(g, "ag_autotune") != AG_OK)
+        return AG_ERR_UNSUPPORTED;
     if (passes == 0)
         passes = 8;
     char dev_name[256] = "unknown";

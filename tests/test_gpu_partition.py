@@ -41,8 +41,9 @@ def test_rows_partition_single_rank_matches_oracle(gpu, oracle):
 
 def test_whole_graph_entries_refuse_a_row_partition(gpu):
     """A rank's row upload names the other ranks' rows by padded global id,
-    so the entries that need a whole graph (features, warm start, PPR)
-    refuse it instead of reading past their per-vertex arrays."""
+    so the entries that need a whole graph (features, warm start, PPR, the
+    solves and products) refuse it instead of reading or writing past their
+    per-vertex arrays."""
     import ctypes as C
 
     import torch
@@ -61,5 +62,15 @@ def test_whole_graph_entries_refuse_a_row_partition(gpu):
         out = np.empty(n, np.float32)
         assert ag.lib.ag_ppr_spmm(h, src.ctypes.data_as(C.POINTER(C.c_uint32)), 1, 3, C.c_double(1e-4),
                                   out.ctypes.data_as(ag.f32p), None) == ag.AG_ERR_UNSUPPORTED
+        # the whole-graph solves and products too: only ag_partition_* run on it
+        opts = ag.make_opts(order=ag.AG_ORDER_EXACT)
+        assert ag.lib.ag_pagerank_launch(h, 5, C.c_double(1e-4), C.byref(opts)) == ag.AG_ERR_UNSUPPORTED
+        x = np.ones(n, np.float32)
+        assert ag.lib.ag_spmv_pull(h, x.ctypes.data_as(ag.f32p), out.ctypes.data_as(ag.f32p), 0) == \
+            ag.AG_ERR_UNSUPPORTED
+        r64 = np.empty(n, np.float64)
+        p = C.c_uint32()
+        assert ag.lib.ag_pagerank_f64(h, 5, C.c_double(1e-9), r64.ctypes.data_as(ag.f64p), C.byref(p)) == \
+            ag.AG_ERR_UNSUPPORTED
     finally:
         ag.lib.ag_graph_release(h)
