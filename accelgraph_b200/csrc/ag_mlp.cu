@@ -59,6 +59,8 @@ struct ag_mlp_s
     float *m, *v;    /* Adam moments                  */
     float *buf;      /* per-sample training signals   */
     uint32_t buf_cap;
+    float *part;     /* per-chunk gradient sums       */
+    uint32_t part_cap; /* chunks                      */
     float *loss;     /* device scalar                 */
     uint32_t step;
 };
@@ -511,8 +513,10 @@ __global__ void __launch_bounds__(AG_MLP_BLK) ag_mlp_k1(const __nv_bfloat16 *wb,
     }
 }
 
-/* chunk sums of the weight gradients over AG_MLP_CHUNK samples */
-__global__ void __launch_bounds__(256) ag_mlp_k2(const float *buf, uint32_t n, float *grad)
+/* chunk sums of the weight gradients over AG_MLP_CHUNK samples, one row of
+ * part per chunk (added in chunk order by ag_mlp_k3, so that a gradient
+ * does not depend on which chunk finishes first) */
+__global__ void __launch_bounds__(256) ag_mlp_k2(const float *buf, uint32_t n, float *part)
 {
     extern __shared__ float sm[]; /* AG_MLP_CHUNK x AG_MLP_REC */
     const uint32_t s0 = blockIdx.x * AG_MLP_CHUNK;
@@ -547,7 +551,18 @@ __global__ void __launch_bounds__(256) ag_mlp_k2(const float *buf, uint32_t n, f
             for (uint32_t s = 0; s < cnt; ++s)
                 a += sm[s * AG_MLP_REC + AG_MLP_IN + 4 * AG_MLP_H];
         }
-        atomicAdd(grad + o, a);
+        part[(size_t)blockIdx.x * AG_MLP_NPARAM + o] = a;
+    }
+}
+
+/* the gradient: the chunk sums added in chunk order */
+__global__ void ag_mlp_k3(const float *part, uint32_t nchunks, float *grad)
+{
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < AG_MLP_NPARAM; o += gridDim.x * blockDim.x) {
+        float a = 0.0f;
+        for (uint32_t c = 0; c < nchunks; ++c)
+            a += part[(size_t)c * AG_MLP_NPARAM + o];
+        grad[o] = a;
     }
 }
 
@@ -651,6 +666,7 @@ extern "C" ag_status_t ag_mlp_release(ag_mlp_t m)
     cudaFree(m->m);
     cudaFree(m->v);
     cudaFree(m->buf);
+    cudaFree(m->part);
     cudaFree(m->loss);
     delete m;
     return AG_OK;
@@ -752,13 +768,21 @@ extern "C" ag_status_t ag_mlp_predict(ag_mlp_t m, const float *X, uint32_t n, fl
 
 static ag_status_t mlp_ensure_buf(ag_mlp_t m, uint32_t n)
 {
-    if (m->buf_cap >= n)
-        return AG_OK;
-    cudaFree(m->buf);
-    m->buf = nullptr;
-    m->buf_cap = 0;
-    MCHK(cudaMalloc((void **)&m->buf, (size_t)n * AG_MLP_REC * sizeof(float)));
-    m->buf_cap = n;
+    if (m->buf_cap < n) {
+        cudaFree(m->buf);
+        m->buf = nullptr;
+        m->buf_cap = 0;
+        MCHK(cudaMalloc((void **)&m->buf, (size_t)n * AG_MLP_REC * sizeof(float)));
+        m->buf_cap = n;
+    }
+    const uint32_t chunks = (n + AG_MLP_CHUNK - 1) / AG_MLP_CHUNK;
+    if (m->part_cap < chunks) {
+        cudaFree(m->part);
+        m->part = nullptr;
+        m->part_cap = 0;
+        MCHK(cudaMalloc((void **)&m->part, (size_t)chunks * AG_MLP_NPARAM * sizeof(float)));
+        m->part_cap = chunks;
+    }
     return AG_OK;
 }
 
@@ -769,7 +793,6 @@ static ag_status_t mlp_grad(ag_mlp_t m, const float *X, const float *T, uint32_t
     if (st != AG_OK)
         return st;
     cudaStream_t s = mlp_stream();
-    MCHK(cudaMemsetAsync(m->g, 0, AG_MLP_NPARAM * sizeof(float), s));
     MCHK(cudaMemsetAsync(m->loss, 0, sizeof(float), s));
     uint64_t blocks = (n + AG_MLP_BLK - 1) / AG_MLP_BLK;
     if (blocks > ag_sm_grid(16))
@@ -778,7 +801,9 @@ static ag_status_t mlp_grad(ag_mlp_t m, const float *X, const float *T, uint32_t
     MCHK(cudaGetLastError());
     const size_t smem = AG_MLP_CHUNK * AG_MLP_REC * sizeof(float);
     MCHK(cudaFuncSetAttribute(ag_mlp_k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ag_mlp_k2<<<(n + AG_MLP_CHUNK - 1) / AG_MLP_CHUNK, 256, smem, s>>>(m->buf, n, m->g);
+    const uint32_t chunks = (n + AG_MLP_CHUNK - 1) / AG_MLP_CHUNK;
+    ag_mlp_k2<<<chunks, 256, smem, s>>>(m->buf, n, m->part);
+    ag_mlp_k3<<<(AG_MLP_NPARAM + 255) / 256, 256, 0, s>>>(m->part, chunks, m->g);
     MCHK(cudaGetLastError());
     if (loss) {
         float h = 0.0f;

@@ -96,6 +96,26 @@ def test_mlp_forward_and_gradients_match_oracle(gpu):
         assert np.linalg.norm(g[a:b] - g_ref[a:b]) <= 1e-3 * np.linalg.norm(g_ref[a:b]) + 1e-7
 
 
+def test_training_is_deterministic(gpu):
+    """Two networks from the same seed, trained on the same samples, end with
+    the same parameters bit for bit: the gradient's chunk sums are added in
+    chunk order, not in the order the chunks finish."""
+    ag = gpu
+    import torch
+
+    from accelgraph_b200 import warmstart as ws
+    rng = np.random.default_rng(4)
+    X = torch.from_numpy(rng.normal(size=(20_000, 8)).astype(np.float32)).cuda()
+    T = torch.from_numpy(rng.normal(size=20_000).astype(np.float32)).cuda()
+    params = []
+    for _ in range(2):
+        m = ws.MLP(seed=3)
+        m.train(X, T, epochs=2, batch=4096, lr=2e-3)
+        params.append(m.params.view(np.uint32))
+        m.release()
+    assert np.array_equal(params[0], params[1])
+
+
 def test_tensor_core_prediction_matches_forward(gpu):
     """The warm start's prediction (mma.sync with bfloat16 head and tail of
     every feature and activation, binary32 accumulation) agrees with the
