@@ -71,64 +71,113 @@ def solve(init_fn, pass_fn, allgather_fn, allreduce_fn, close_fn, stopped_fn, re
     return its, passes, converged, err
 
 
+class RowPartition:
+    """This rank's rows of `graph` (an accelgraph_b200.Graph every rank has
+    built) resident on its GPU, over the initialised torch.distributed NCCL
+    group: the row upload and the contribution buffers are made once, and
+    `solve` runs the partitioned loop on them as often as asked."""
+
+    def __init__(self, graph):
+        import ctypes as C
+
+        import torch
+        import torch.distributed as dist
+
+        from . import check, lib
+
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.bounds, self.slice = partition_bounds(graph.in_degree(), self.world)
+        self.num_vertices = graph.num_vertices
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        # one stream for the library's kernels and torch's collectives and
+        # copies, so that they run in order.  It is a stream of its own: the
+        # legacy default stream (handle 0) would read as "the library's own
+        # stream", which does not wait for work on the default stream.
+        self.stream = torch.cuda.Stream(self.dev)
+        check(lib.ag_set_stream(C.c_void_p(self.stream.cuda_stream)), "ag_set_stream")
+        self.h = C.c_void_p()
+        check(lib.ag_graph_upload_rows(graph.ptr, self.bounds.ctypes.data_as(C.POINTER(C.c_uint32)), self.world,
+                                       self.rank, self.slice, 0, C.byref(self.h)), "ag_graph_upload_rows")
+        with torch.cuda.stream(self.stream):
+            self.full = [torch.zeros(self.world * self.slice, dtype=torch.float32, device=self.dev)
+                         for _ in range(2)]
+            self.stats = torch.zeros(2, dtype=torch.float64, device=self.dev)
+            self.state = torch.zeros(3, dtype=torch.int32, device=self.dev)  # stop, passes, converged
+            self.err = torch.zeros(1, dtype=torch.float64, device=self.dev)
+
+    def solve(self, iterations=20, epsilon=1e-4, exact=True):
+        """One partitioned solve; returns (iterations, passes, converged,
+        error_total) of the reference's semantics."""
+        import torch
+        import torch.distributed as dist
+
+        from . import AG_ORDER_EXACT, AG_ORDER_FAST, check, lib
+
+        order = AG_ORDER_EXACT if exact else AG_ORDER_FAST
+        h, full, stats, state, err, rank, sl = self.h, self.full, self.stats, self.state, self.err, self.rank, self.slice
+
+        def init_fn():
+            check(lib.ag_partition_init(h, full[0].data_ptr()), "ag_partition_init")
+            return full
+
+        def pass_fn(c_in, c_out, eps):
+            check(lib.ag_partition_step(h, c_in.data_ptr(), c_out.data_ptr(), eps, order, stats.data_ptr(),
+                                        state.data_ptr()), "ag_partition_step")
+            return stats
+
+        def allgather_fn(c):
+            # in place: this rank's input is its own slice of the output
+            dist.all_gather_into_tensor(c, c[rank * sl:(rank + 1) * sl])
+
+        def allreduce_fn(st):
+            dist.all_reduce(st)
+
+        def close_fn(st):
+            check(lib.ag_partition_close(st.data_ptr(), state.data_ptr(), err.data_ptr()), "ag_partition_close")
+
+        def stopped_fn():
+            return bool(state[0].item())
+
+        def result_fn():
+            s = state.tolist()
+            return int(s[1]), bool(s[2]), float(err.item())
+
+        with torch.cuda.stream(self.stream):
+            state.zero_()
+            err.zero_()
+            stats.zero_()
+            its, passes, conv, err_sum = solve(init_fn, pass_fn, allgather_fn, allreduce_fn, close_fn, stopped_fn,
+                                               result_fn, iterations, epsilon)
+        return its, passes, conv, err_sum / self.num_vertices
+
+    def ranks(self):
+        """This rank's normalised ranks and its row range."""
+        from . import check, f32p, lib
+
+        n_local = int(self.bounds[self.rank + 1] - self.bounds[self.rank])
+        local = np.empty(n_local, np.float32)
+        check(lib.ag_partition_fetch(self.h, local.ctypes.data_as(f32p)), "ag_partition_fetch")
+        return local, (int(self.bounds[self.rank]), int(self.bounds[self.rank + 1]))
+
+    def release(self):
+        from . import check, lib
+
+        if self.h:
+            self.stream.synchronize()
+            lib.ag_graph_release(self.h)
+            self.h = None
+            check(lib.ag_set_stream(None), "ag_set_stream")
+
+
 def pagerank_rows_gpu(graph, iterations=20, epsilon=1e-4, exact=True):
     """Partitioned solve of `graph` (an accelgraph_b200.Graph every rank has
     built) over the initialised torch.distributed NCCL group, in EXACT order
     (or FAST with exact=False).  Returns this rank's normalised ranks, its row
     range and the solve statistics."""
-    import ctypes as C
-
-    import torch
-    import torch.distributed as dist
-
-    from . import AG_ORDER_EXACT, AG_ORDER_FAST, check, f32p, lib
-
-    rank, world = dist.get_rank(), dist.get_world_size()
-    bounds, slice_ = partition_bounds(graph.in_degree(), world)
-    dev = torch.device("cuda", torch.cuda.current_device())
-    check(lib.ag_set_stream(C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)), "ag_set_stream")
-    h = C.c_void_p()
-    check(lib.ag_graph_upload_rows(graph.ptr, bounds.ctypes.data_as(C.POINTER(C.c_uint32)), world, rank, slice_,
-                                   0, C.byref(h)), "ag_graph_upload_rows")
-    full = [torch.zeros(world * slice_, dtype=torch.float32, device=dev) for _ in range(2)]
-    stats = torch.zeros(2, dtype=torch.float64, device=dev)
-    state = torch.zeros(3, dtype=torch.int32, device=dev)  # stop, passes, converged
-    err = torch.zeros(1, dtype=torch.float64, device=dev)
-    order = AG_ORDER_EXACT if exact else AG_ORDER_FAST
-
-    def init_fn():
-        check(lib.ag_partition_init(h, full[0].data_ptr()), "ag_partition_init")
-        return full
-
-    def pass_fn(c_in, c_out, eps):
-        check(lib.ag_partition_step(h, c_in.data_ptr(), c_out.data_ptr(), eps, order, stats.data_ptr(),
-                                    state.data_ptr()), "ag_partition_step")
-        return stats
-
-    def allgather_fn(c):
-        # in place: this rank's input is its own slice of the output
-        dist.all_gather_into_tensor(c, c[rank * slice_:(rank + 1) * slice_])
-
-    def allreduce_fn(st):
-        dist.all_reduce(st)
-
-    def close_fn(st):
-        check(lib.ag_partition_close(st.data_ptr(), state.data_ptr(), err.data_ptr()), "ag_partition_close")
-
-    def stopped_fn():
-        return bool(state[0].item())
-
-    def result_fn():
-        s = state.tolist()
-        return int(s[1]), bool(s[2]), float(err.item())
-
-    its, passes, conv, err_sum = solve(init_fn, pass_fn, allgather_fn, allreduce_fn, close_fn, stopped_fn, result_fn,
-                                       iterations, epsilon)
-    n_local = int(bounds[rank + 1] - bounds[rank])
-    local = np.empty(n_local, np.float32)
-    check(lib.ag_partition_fetch(h, local.ctypes.data_as(f32p)), "ag_partition_fetch")
-    lib.ag_graph_release(h)
-    check(lib.ag_set_stream(None), "ag_set_stream")
-    return local, (int(bounds[rank]), int(bounds[rank + 1])), {"iterations": its, "passes": passes,
-                                                             "converged": conv, "error_total":
-                                                             err_sum / graph.num_vertices}
+    part = RowPartition(graph)
+    try:
+        its, passes, conv, err = part.solve(iterations, epsilon, exact)
+        local, rows = part.ranks()
+    finally:
+        part.release()
+    return local, rows, {"iterations": its, "passes": passes, "converged": conv, "error_total": err}

@@ -39,6 +39,42 @@ def test_rows_partition_single_rank_matches_oracle(gpu, oracle):
         dist.destroy_process_group()
 
 
+def test_rows_partition_at_scale_22_repeats_the_single_gpu_solve(gpu):
+    """RMAT s22 to 1e-6 (126 iterations): the partitioned loop, run twice on
+    one upload, stops on the same pass as the one-GPU EXACT solve with the
+    same ranks bit for bit.  The library's kernels and torch's collectives
+    share one stream; on unordered streams the statistics were read before
+    the pass that made them had finished."""
+    ag = gpu
+    import torch
+    import torch.distributed as dist
+
+    from accelgraph_b200 import distributed as agd
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        g = ag.Graph.rmat(22, 16, seed=27491095)
+        dg = ag.DeviceGraph(g)
+        want, res, _ = dg.pagerank(300, 1e-6, order=ag.AG_ORDER_EXACT)
+        dg.release()
+        part = agd.RowPartition(g)
+        try:
+            for _ in range(2):
+                its, passes, conv, _ = part.solve(300, 1e-6, True)
+                assert (its, passes, conv) == (res.iterations, res.passes, True)
+                ranks, _ = part.ranks()
+                assert np.array_equal(ranks.view(np.uint32), want.view(np.uint32))
+        finally:
+            part.release()
+    finally:
+        dist.destroy_process_group()
+
+
 def test_whole_graph_entries_refuse_a_row_partition(gpu):
     """A rank's row upload names the other ranks' rows by padded global id,
     so the entries that need a whole graph (features, warm start, PPR, the
