@@ -64,7 +64,10 @@ ag_status_t ag_init(int device);
 /* The cudaStream_t (as void*) every launch of this library goes to. */
 void *ag_stream(void);
 /* Make every later launch of this library go to the caller's stream (NULL:
- * back to the library's own); waits for work already queued. */
+ * back to the library's own); waits for work already queued.  The library's
+ * own stream is non-blocking: it does not wait for work on the legacy
+ * default stream, whose handle is also NULL, so a caller that orders its
+ * own work against the library's passes a stream it created. */
 ag_status_t ag_set_stream(void *stream);
 /* Wait for the library stream, polling with a deadline (seconds; <=0 means
  * the AG_WAIT_TIMEOUT_S environment variable, default 600).  Returns
