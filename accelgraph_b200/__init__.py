@@ -5,6 +5,12 @@ libaccelgraph_b200.so (hand-written CUDA for sm_100a behind a C ABI); this
 module only binds it with ctypes and offers numpy conveniences.  Importing it
 fails loudly when the library has not been built: there is no CPU fallback.
 
+Summation order: the reference entry points and ag_pr_opts_init (the C
+defaults) use EXACT order, the reference loop's bits.  The numpy conveniences
+here (DeviceGraph.launch / pagerank, MultiGraph.pagerank, make_opts) default
+to FAST order, the faster tree sums for rows over 32 in-edges; pass
+order=AG_ORDER_EXACT for the reference's bits.
+
 Reference interface mirrored (AccelGraph, 02_capi_graph):
   struct Arguments            include/config/graphConfig.h:11-52
   struct PageRankStats        include/algorithms/capi/pageRank.h:19-30
