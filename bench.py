@@ -248,8 +248,8 @@ def run_reference(a):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(a, 1),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{per_step} passes per step of the C/OpenMP restatement of "
-                                   f"pageRankPullGraphCSR on RMAT s{a.scale} ef{a.edge_factor}"},
+                         "sample": f"up to {per_step} passes per step (a step stops at epsilon) of the C/OpenMP "
+                                   f"restatement of pageRankPullGraphCSR on RMAT s{a.scale} ef{a.edge_factor}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "num_vertices": 1 << a.scale, "num_edges": E,
     }
