@@ -49,8 +49,8 @@ static pthread_mutex_t g_csr_lock = PTHREAD_MUTEX_INITIALIZER;
 /* A caller that solves on one unchanged GraphCSR several times pays the
  * upload once when it asks for it.  An entry matches on the GraphCSR
  * address, its vertex and edge counts, the addresses of every array the
- * upload reads and the upload flags.  The library is called from one host
- * thread at a time, so the table has no lock. */
+ * upload reads and the upload flags.  The table is only read and written
+ * under g_csr_lock. */
 #define AG_KEEP_SLOTS 8
 
 typedef struct keep_slot
