@@ -153,3 +153,21 @@ def test_partition_bounds_balance():
     w = np.add.reduceat(deg + 1, b[:-1].astype(np.int64))
     assert w.max() <= 1.6 * w.mean()
     assert s % 64 == 0 and s >= np.diff(b).max()
+
+
+def test_partition_bounds_edge_cases():
+    """One rank owns everything; more ranks than rows leaves some ranks
+    empty, and every row still has exactly one owner."""
+    import numpy as np
+
+    from accelgraph_b200 import distributed as agd
+    b, s = agd.partition_bounds(np.array([5, 0, 7]), 1)
+    assert list(b) == [0, 3] and s == 64
+    b, s = agd.partition_bounds(np.array([5, 0, 7]), 8)
+    assert b[0] == 0 and b[-1] == 3 and len(b) == 9 and np.all(np.diff(b.astype(np.int64)) >= 0)
+    owners = np.zeros(3, np.int64)
+    for r in range(8):
+        owners[b[r]:b[r + 1]] += 1
+    assert np.all(owners == 1) and s == 64
+    b, s = agd.partition_bounds(np.zeros(0, np.int64), 2)
+    assert list(b) == [0, 0, 0] and s == 64
